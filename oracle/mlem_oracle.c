@@ -1,0 +1,241 @@
+/*
+ * mlem_oracle.c -- CPU restatement of the reference MLEM hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY (the parity checker).  See mlem_oracle.h for the
+ * contract; every function cites the reference function it restates.
+ * Build with -ffp-contract=off so no multiply-add is fused: the reference is
+ * compiled for x86-64 without FMA, and bit-exact agreement depends on that.
+ */
+#include "mlem_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#if defined(__x86_64__) || defined(__i386__)
+#include <xmmintrin.h>
+#define ORACLE_HAVE_MXCSR 1
+#endif
+
+static inline uint64_t row_begin(const uint64_t* row_end, uint32_t r) {
+    /* helper_files_common/csr4matrix.hpp:138-140: row r starts at row_end[r-1]. */
+    return r == 0 ? 0 : row_end[r - 1];
+}
+
+void oracle_column_sums(uint32_t R, uint32_t C, const uint64_t* row_end,
+                        const oracle_elem* e, float* norm) {
+    /* seqcsr4mlem.cpp:41 zero-fill, then :44-47 scatter-add in row order. */
+    memset(norm, 0, (size_t)C * sizeof(float));
+    for (uint32_t r = 0; r < R; ++r)
+        for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+            norm[e[k].index] += e[k].value;
+}
+
+float oracle_init_value(uint32_t C, const float* norm, uint64_t S, const int32_t* sino,
+                        double* sumnorm_out, double* sumin_out) {
+    /* seqcsr4mlem.cpp:55-60 */
+    double sumnorm = 0.0;
+    for (uint32_t i = 0; i < C; ++i) sumnorm += norm[i];
+    double sumin = 0.0;
+    for (uint64_t i = 0; i < S; ++i) sumin += sino[i];
+    if (sumnorm_out) *sumnorm_out = sumnorm;
+    if (sumin_out) *sumin_out = sumin;
+    return (float)(sumin / sumnorm);
+}
+
+void oracle_fwproj(uint32_t R, const uint64_t* row_end, const oracle_elem* e,
+                   const float* x, float* f) {
+    /* seqcsr4mlem.cpp:76-90: float accumulator, multiply then add. */
+    for (uint32_t r = 0; r < R; ++r) {
+        float res = 0.0f;
+        for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+            res += e[k].value * x[e[k].index];
+        f[r] = res;
+    }
+}
+
+void oracle_correl(uint64_t R, const float* f, const int32_t* s, float* c) {
+    /* seqcsr4mlem.cpp:98-99: the int count is converted to float before the divide. */
+    for (uint64_t i = 0; i < R; ++i)
+        c[i] = (f[i] != 0.0) ? ((float)s[i] / f[i]) : 0.0f;
+}
+
+void oracle_bkproj(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_elem* e,
+                   const float* c, float* u) {
+    /* seqcsr4mlem.cpp:113 zero-fill, :116-119 scatter in row order. */
+    memset(u, 0, (size_t)C * sizeof(float));
+    for (uint32_t r = 0; r < R; ++r)
+        for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+            u[e[k].index] += e[k].value * c[r];
+}
+
+void oracle_update(uint32_t C, const float* u, const float* norm, float* x) {
+    /* seqcsr4mlem.cpp:127-128 */
+    for (uint32_t i = 0; i < C; ++i)
+        x[i] *= (norm[i] != 0.0) ? (u[i] / norm[i]) : u[i];
+}
+
+int oracle_mlem(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_elem* e,
+                const int32_t* sino, uint64_t S, int n_iter, int ftz,
+                const float* start_image, float* image, float* image_sums) {
+    if (S != R) return -1; /* seqcsr4mlem.cpp:96 asserts fwproj.size() == input.size() */
+#ifdef ORACLE_HAVE_MXCSR
+    unsigned int saved = _mm_getcsr();
+    if (ftz) _MM_SET_FLUSH_ZERO_MODE(_MM_FLUSH_ZERO_ON); /* seqcsr4mlem.cpp:194 */
+#else
+    (void)ftz;
+#endif
+    float* fw = (float*)malloc((size_t)R * sizeof(float) + 1);
+    float* cr = (float*)malloc((size_t)R * sizeof(float) + 1);
+    float* up = (float*)malloc((size_t)C * sizeof(float) + 1);
+    float* norm = (float*)malloc((size_t)C * sizeof(float) + 1);
+    int rc = 0;
+    if (!fw || !cr || !up || !norm) { rc = -2; goto done; }
+
+    oracle_column_sums(R, C, row_end, e, norm);
+    if (start_image) {
+        memcpy(image, start_image, (size_t)C * sizeof(float));
+    } else {
+        float init = oracle_init_value(C, norm, S, sino, NULL, NULL);
+        for (uint32_t i = 0; i < C; ++i) image[i] = init;
+    }
+    for (int it = 0; it < n_iter; ++it) {
+        oracle_fwproj(R, row_end, e, image, fw);
+        oracle_correl(R, fw, sino, cr);
+        oracle_bkproj(R, C, row_end, e, cr, up);
+        oracle_update(C, up, norm, image);
+        if (image_sums) {
+            float s = 0.0f; /* seqcsr4mlem.cpp:174-176 */
+            for (uint32_t i = 0; i < C; ++i) s += image[i];
+            image_sums[it] = s;
+        }
+    }
+done:
+    free(fw); free(cr); free(up); free(norm);
+#ifdef ORACLE_HAVE_MXCSR
+    _mm_setcsr(saved);
+#endif
+    return rc;
+}
+
+int oracle_mlem_f64(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_elem* e,
+                    const int32_t* sino, uint64_t S, int n_iter, double* image) {
+    if (S != R) return -1;
+    double* fw = (double*)malloc((size_t)R * sizeof(double) + 1);
+    double* up = (double*)malloc((size_t)C * sizeof(double) + 1);
+    double* norm = (double*)calloc((size_t)C + 1, sizeof(double));
+    if (!fw || !up || !norm) { free(fw); free(up); free(norm); return -2; }
+    for (uint32_t r = 0; r < R; ++r)
+        for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+            norm[e[k].index] += (double)e[k].value;
+    double sumnorm = 0.0, sumin = 0.0;
+    for (uint32_t i = 0; i < C; ++i) sumnorm += norm[i];
+    for (uint64_t i = 0; i < S; ++i) sumin += sino[i];
+    for (uint32_t i = 0; i < C; ++i) image[i] = sumin / sumnorm;
+    for (int it = 0; it < n_iter; ++it) {
+        for (uint32_t r = 0; r < R; ++r) {
+            double res = 0.0;
+            for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+                res += (double)e[k].value * image[e[k].index];
+            fw[r] = (res != 0.0) ? (double)sino[r] / res : 0.0;
+        }
+        memset(up, 0, (size_t)C * sizeof(double));
+        for (uint32_t r = 0; r < R; ++r)
+            for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+                up[e[k].index] += (double)e[k].value * fw[r];
+        for (uint32_t i = 0; i < C; ++i)
+            image[i] *= (norm[i] != 0.0) ? (up[i] / norm[i]) : up[i];
+    }
+    free(fw); free(up); free(norm);
+    return 0;
+}
+
+void oracle_mlem_relaxed_f64(uint32_t R, uint32_t C, const uint64_t* row_end,
+                             const oracle_elem* e, const int32_t* sino, const double* x0,
+                             const double* omega, int K, double* xK) {
+    double* fw = (double*)malloc((size_t)R * sizeof(double) + 1);
+    double* up = (double*)malloc((size_t)C * sizeof(double) + 1);
+    double* norm = (double*)calloc((size_t)C + 1, sizeof(double));
+    for (uint32_t r = 0; r < R; ++r)
+        for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+            norm[e[k].index] += (double)e[k].value;
+    memcpy(xK, x0, (size_t)C * sizeof(double));
+    for (int it = 0; it < K; ++it) {
+        for (uint32_t r = 0; r < R; ++r) {
+            double res = 0.0;
+            for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+                res += (double)e[k].value * xK[e[k].index];
+            fw[r] = (res != 0.0) ? (double)sino[r] / res : 0.0;
+        }
+        memset(up, 0, (size_t)C * sizeof(double));
+        for (uint32_t r = 0; r < R; ++r)
+            for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+                up[e[k].index] += (double)e[k].value * fw[r];
+        for (uint32_t i = 0; i < C; ++i) {
+            double ratio = (norm[i] != 0.0) ? (up[i] / norm[i]) : up[i];
+            xK[i] *= (ratio > 0.0) ? pow(ratio, omega[it]) : 0.0;
+        }
+    }
+    free(fw); free(up); free(norm);
+}
+
+void oracle_project_f64(uint32_t R, const uint64_t* row_end, const oracle_elem* e,
+                        const float* x, double* out) {
+    for (uint32_t r = 0; r < R; ++r) {
+        double s = 0.0;
+        for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+            s += (double)e[k].value * (double)x[e[k].index];
+        out[r] = s;
+    }
+}
+
+void oracle_poisson_grad_f64(uint32_t R, uint32_t C, const uint64_t* row_end,
+                             const oracle_elem* e, const int32_t* s, const double* x,
+                             double* grad) {
+    memset(grad, 0, (size_t)C * sizeof(double));
+    for (uint32_t r = 0; r < R; ++r) {
+        double ax = 0.0;
+        for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+            ax += (double)e[k].value * x[e[k].index];
+        /* d/dx [Ax - s log Ax] = A^T (1 - s / Ax); rows with Ax == 0 contribute A^T 1. */
+        double w = (ax != 0.0) ? 1.0 - (double)s[r] / ax : 1.0;
+        for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+            grad[e[k].index] += (double)e[k].value * w;
+    }
+}
+
+void oracle_transpose(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_elem* e,
+                      uint64_t* col_ptr, oracle_elem* ce) {
+    memset(col_ptr, 0, ((size_t)C + 1) * sizeof(uint64_t));
+    uint64_t Z = R ? row_end[R - 1] : 0;
+    for (uint64_t k = 0; k < Z; ++k) col_ptr[e[k].index + 1] += 1;
+    for (uint32_t c = 0; c < C; ++c) col_ptr[c + 1] += col_ptr[c];
+    uint64_t* cursor = (uint64_t*)malloc(((size_t)C + 1) * sizeof(uint64_t));
+    memcpy(cursor, col_ptr, ((size_t)C + 1) * sizeof(uint64_t));
+    for (uint32_t r = 0; r < R; ++r)
+        for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k) {
+            uint64_t slot = cursor[e[k].index]++;
+            ce[slot].index = r;
+            ce[slot].value = e[k].value;
+        }
+    free(cursor);
+}
+
+void oracle_partition(uint32_t R, const uint64_t* row_end, int n_ranks,
+                      uint32_t* starts, uint32_t* ends) {
+    /* mpicsr4mlem.cpp:206-224, including its float comparison of the running sum. */
+    uint64_t Z = R ? row_end[R - 1] : 0;
+    float avg = (float)Z / (float)n_ranks;
+    int idx = 0;
+    uint64_t sum = 0;
+    for (int i = 0; i < n_ranks; ++i) { starts[i] = 0; ends[i] = 0; }
+    starts[0] = 0;
+    for (uint32_t r = 0; r < R; ++r) {
+        sum += row_end[r] - row_begin(row_end, r);
+        if ((float)sum > avg * (float)(idx + 1) && idx + 1 < n_ranks) {
+            ends[idx] = r + 1;
+            idx += 1;
+            starts[idx] = r + 1;
+        }
+    }
+    ends[n_ranks - 1] = R;
+}
