@@ -1,0 +1,431 @@
+#!/usr/bin/env python3
+"""MLEM benchmark: iterations/s and HBM GB/s on the plain-full workload.
+
+Workload ("plain-full"): a synthetic Siddon system matrix of 4,194,304 LORs
+x 1,048,576 voxels (128x128x64 grid, 150-250 elements per row, ~0.78e9
+elements, 6.2 GB CSR4 plus a 6.2 GB device CSC copy), one int32 Poisson
+sinogram of an 8-ellipsoid phantom at 1e9 counts, float32.  A step is one
+MLEM iteration (forward projection + correlation + back projection + update,
+plus the per-iteration image-sum census the reference prints).  The matrix
+(6.2 GB) is larger than the 126 MB L2, so no L2 flush is needed between
+steps.  The batched line ("batched-b16") runs 16 sinograms over the same
+matrix in one pass per iteration.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints ONE JSON line (rank 0).  --impl reference times the reference's own
+OpenMP implementation (openmpcsr4mlem, compiled from its sources into
+oracle/_ref) on this host's cores on the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import re
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MLEM iterations/s and HBM GB/s, plain vs batched B=16, at rel L2 err <=1e-4"
+UNIT = "iterations/s"
+REF_MESSUNG = os.path.join(ROOT, "oracle", "_ref", "openmpcsr4mlem_messung")
+PHASES = ("project", "backproject", "update", "stats")
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--mode", choices=["auto", "csc", "atomic", "fused"], default="auto",
+                    help="back-projection method; auto = autotuned")
+    ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-iters", type=int, default=3)
+    return ap.parse_args()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,utilization.gpu,"
+              "clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self.thread = None
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.proc = subprocess.Popen(
+            ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+             "-lms", "100", "-i", str(self.gpu)],
+            stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, smax, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 10:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = max(smax, float(f[2]))
+            except ValueError:
+                continue
+            for name, v in zip(names, f[6:10]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def committed_traffic():
+    """Per-launch DRAM bytes of the dominant kernels from the committed ncu
+    summary (profiles/traffic.json), keyed by kernel name; {} if absent."""
+    p = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the reference's openmpcsr4mlem on this host
+# ---------------------------------------------------------------------------
+def write_inputs(tmpdir, row_end, elems, n_rows, n_cols, grid, sino):
+    from mlem_b200 import formats
+    mp = os.path.join(tmpdir, "matrix.csr4")
+    sp = os.path.join(tmpdir, "sino.bin")
+    formats.write_csr4(mp, n_rows, n_cols, row_end, elems, grid=grid)
+    formats.write_vector(sp, sino, "int32")
+    return mp, sp
+
+
+def scratch_dir(need_bytes):
+    for d in ("/dev/shm", tempfile.gettempdir()):
+        try:
+            if shutil.disk_usage(d).free > need_bytes * 1.2:
+                return tempfile.mkdtemp(prefix="mlem_bench_", dir=d)
+        except OSError:
+            continue
+    return None
+
+
+def run_reference_binary(matrix_path, sino_path, iters, threads, timeout=900):
+    """Per-iteration seconds printed by openmpcsr4mlem -DMESSUNG (iter,elapsed)."""
+    out = os.path.join(os.path.dirname(matrix_path), "image.out")
+    env = dict(os.environ, OMP_NUM_THREADS=str(threads))
+    t0 = time.time()
+    p = subprocess.run([REF_MESSUNG, matrix_path, sino_path, out, str(iters)], env=env,
+                       capture_output=True, text=True, timeout=timeout,
+                       cwd=os.path.dirname(matrix_path))
+    if p.returncode != 0:
+        raise RuntimeError(f"openmpcsr4mlem failed: {p.stderr[-500:]}")
+    secs = [float(m.group(2)) for m in re.finditer(r"^(\d+),([0-9.eE+-]+)$", p.stdout, re.M)]
+    return secs, time.time() - t0
+
+
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# ---------------------------------------------------------------------------
+# our implementation
+# ---------------------------------------------------------------------------
+def run_ours(a, rank, world, local_rank):
+    import numpy as np
+    import torch
+
+    from mlem_b200 import api, synth
+
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    w = synth.WORKLOADS["plain-full"]
+    g = w.geometry
+    if world > 1:  # weak scaling: every rank reconstructs its own full-size LOR set
+        g = synth.Geometry(g.nx, g.ny, g.nz, g.n_rows, g.min_count, g.max_count, seed=g.seed + 100 * rank)
+    t_setup = time.time()
+    ctx = api.Context.siddon(g, device=local_rank)
+    t_matrix = time.time() - t_setup
+    frames = synth.make_frames(w, ctx.project_f64)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    ctx.set_sinograms(frames.sinograms)
+    ctx.init_images()
+
+    mode_map = {"csc": api.BK_CSC, "atomic": api.BK_ATOMIC, "fused": api.BK_FUSED}
+    if a.mode == "auto":
+        tuning = ctx.autotune()
+    else:
+        ctx.set_tuning(bk_mode=mode_map[a.mode], group=32, frame_tile=1, blocks_per_sm=8)
+        tuning = ctx.tuning()
+    ctx.init_images()
+    ctx.iterate(a.warmup, stats=False)
+    kernels_per_iter = ctx.kernels_per_iteration()
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    # --- timed region: K iterations, device events on the context's stream ---
+    clocks = ClockSampler(local_rank) if rank == 0 else None
+    barrier()
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    ctx.iterate(a.steps, stats=False)
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1)
+    # per-phase events (a second pass, same kernels)
+    ph_ms, ph_bytes, ph_launch = ctx.profile_phases(max(10, min(a.steps, 50)))
+    clk = clocks.stop() if clocks else None
+    if dist is not None:
+        t = torch.tensor([ms], device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / a.steps
+    value = world * a.steps / (ms / 1e3)
+
+    # parity of this run's image against the FP64 projection of its phantom is
+    # covered by the tests; report the image sum as a sanity figure
+    img = ctx.get_images()[0]
+    image_sum = float(img.astype(np.float64).sum())
+
+    # --- end to end through the C ABI: pinned host sinogram + image in, image out ---
+    sino_h = torch.from_numpy(frames.sinograms[0].copy()).pin_memory()
+    img_h = torch.from_numpy(img.copy()).pin_memory()
+    k_e2e = max(5, min(a.steps, 50))
+    ctx.step_host_ptr(sino_h.data_ptr(), img_h.data_ptr(), 1)  # warm (captures the 1-step graph)
+    barrier()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(k_e2e):
+        ctx.step_host_ptr(sino_h.data_ptr(), img_h.data_ptr(), 1)
+    f1.record(stream)
+    barrier()
+    e2e_ms = f0.elapsed_time(f1) / k_e2e
+    e2e = {"value": world * 1e3 / e2e_ms, "unit": UNIT,
+           "h2d_bytes_per_step": int(4 * ctx.n_rows + 4 * ctx.n_cols),
+           "d2h_bytes_per_step": int(4 * ctx.n_cols),
+           "call": "mlem_step_host (pinned host sinogram + image)"}
+
+    peak, peak_kind = measured_peak()
+    total_bytes = float(ph_bytes.sum())
+    dom = int(ph_ms[:3].argmax())
+    kernel_names = {
+        api.BK_CSC: ("k_fwproj", "k_bkproj_csc", "-", "k_stats"),
+        api.BK_ATOMIC: ("k_fwproj", "k_bkproj_scatter", "k_apply_update", "k_stats"),
+        api.BK_FUSED: ("k_fused_row", "-", "k_apply_update", "k_stats"),
+    }[tuning["bk_mode"]]
+    traffic = committed_traffic().get(kernel_names[dom])
+    achieved = ph_bytes[dom] / (ph_ms[dom] / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": kernel_names[dom], "achieved": round(achieved, 1),
+                "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                "traffic": traffic, "peak_kind": peak_kind,
+                "algorithmic_bytes_per_launch": ph_bytes[dom] / max(1, ph_launch[dom]),
+                "ms_per_launch": ph_ms[dom] / max(1, ph_launch[dom])}
+    phases = {PHASES[p]: {"ms": round(float(ph_ms[p]), 4), "GB": round(ph_bytes[p] / 1e9, 4),
+                          "GB/s": round(ph_bytes[p] / (ph_ms[p] / 1e3) / 1e9, 1) if ph_ms[p] > 0 else None,
+                          "kernel": kernel_names[p], "launches": int(ph_launch[p])}
+              for p in range(4)}
+
+    line = {
+        "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
+        "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_per_step, 4),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded Siddon matrix, ellipsoid phantom, Poisson sinogram)",
+        "config": {"workload": "plain-full", "grid": [g.nx, g.ny, g.nz], "n_rows": ctx.n_rows,
+                   "n_cols": ctx.n_cols, "nnz": int(ctx.nnz), "frames": 1,
+                   "bk_mode": api.BK_NAMES[tuning["bk_mode"]], "group": tuning["group"],
+                   "frame_tile": tuning["frame_tile"], "blocks_per_sm": tuning["blocks_per_sm"],
+                   "l2": "inputs larger than L2 (6.2 GB matrix), no flush",
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "hbm_gbs": round(total_bytes / (ms_per_step / 1e3) / 1e9, 1),
+        "iteration_roofline_frac": round(total_bytes / (ms_per_step / 1e3) / 1e9 / peak, 4),
+        "bytes_per_iteration": total_bytes,
+        "roofline": roofline, "phases": phases, "e2e": e2e,
+        "gpu_launches": int(kernels_per_iter * a.steps),
+        "clocks": clk, "image_sum": image_sum, "setup_s": {"matrix": round(t_matrix, 2)},
+    }
+
+    # --- batched: 16 sinograms in one pass over the matrix per iteration ---
+    if not a.no_batched:
+        wb = synth.WORKLOADS["batched-b16"]
+        fb = synth.make_frames(wb, ctx.project_f64)
+        ctx.set_sinograms(fb.sinograms)
+        ctx.init_images()
+        tb = ctx.autotune()
+        ctx.init_images()
+        ctx.iterate(a.warmup, stats=False)
+        kb = max(10, a.steps // 4)
+        barrier()
+        e0.record(stream)
+        ctx.iterate(kb, stats=False)
+        e1.record(stream)
+        barrier()
+        bms = e0.elapsed_time(e1) / kb
+        bph_ms, bph_bytes, _ = ctx.profile_phases(10)
+        line["batched"] = {
+            "workload": "batched-b16", "frames": 16, "ms_per_iteration": round(bms, 4),
+            "frame_iterations_per_s": round(16 * 1e3 / bms, 2),
+            "per_frame_speedup_vs_plain": round((16 / bms) / (1 / ms_per_step), 3),
+            "hbm_gbs": round(float(bph_bytes.sum()) / (bms / 1e3) / 1e9, 1),
+            "bk_mode": api.BK_NAMES[tb["bk_mode"]], "group": tb["group"],
+            "frame_tile": tb["frame_tile"],
+            "phases_ms": [round(float(x), 4) for x in bph_ms],
+        }
+
+    # --- CPU baseline: the reference's openmpcsr4mlem on this host (rank 0, N=1) ---
+    if rank == 0 and world == 1 and not a.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_from_ctx(ctx, frames.sinograms[0], g, a.cpu_iters)
+
+    ctx.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return line
+
+
+def cpu_baseline_from_ctx(ctx, sino, g, iters):
+    if not os.path.exists(REF_MESSUNG):
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/openmpcsr4mlem_messung not built"}
+    need = 8 * ctx.nnz + 8 * ctx.n_rows + 4 * ctx.n_rows
+    d = scratch_dir(need)
+    if d is None:
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "unavailable: no scratch space for the CSR4 file"}
+    try:
+        row_end, elems = ctx.csr()
+        mp, sp = write_inputs(d, row_end, elems, ctx.n_rows, ctx.n_cols, (g.nx, g.ny, g.nz), sino)
+        del row_end, elems
+        threads = host_threads()
+        secs, wall = run_reference_binary(mp, sp, iters, threads)
+        per = statistics.mean(secs[1:]) if len(secs) > 1 else secs[0]
+        return {"value": round(1.0 / per, 4), "unit": UNIT, "cores": threads, "kind": "reference",
+                "sample": f"{iters} full iterations of openmpcsr4mlem (reference source, -O3 -fopenmp "
+                          f"-DMESSUNG) on the same plain-full CSR4 file; mean of iterations 2..{iters}; "
+                          f"wall {wall:.1f} s incl. load and serial column sums",
+                "iteration_seconds": secs}
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+# ---------------------------------------------------------------------------
+def run_reference(a, rank, world):
+    if rank != 0:
+        return None
+    import numpy as np
+
+    from mlem_b200 import synth
+
+    if not os.path.exists(REF_MESSUNG):
+        return {"impl": "reference", "unavailable": "oracle/_ref/openmpcsr4mlem_messung is not built"}
+    w = synth.WORKLOADS["plain-full"]
+    g = w.geometry
+    m = synth.host_matrix(g)  # host generator (CPU); bit-identical to the GPU arm's matrix
+    frames = synth.make_frames(w, lambda x: synth.project_f64(m, x))
+    need = 8 * m.nnz + 8 * m.n_rows
+    d = scratch_dir(need)
+    if d is None:
+        return {"impl": "reference", "unavailable": "no scratch space for the 6 GB CSR4 file"}
+    try:
+        mp, sp = write_inputs(d, m.row_end, m.elems, m.n_rows, m.n_cols, (g.nx, g.ny, g.nz),
+                              frames.sinograms[0])
+        del m
+        threads = host_threads()
+        k = max(1, min(a.steps, 20))
+        wu = max(1, min(a.warmup, 2))
+        secs, wall = run_reference_binary(mp, sp, wu + k, threads)
+        timed = secs[wu:]
+        per = statistics.mean(timed)
+        value = 1.0 / per
+        return {
+            "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
+            "n_gpus": world, "steps": len(timed), "warmup": wu, "ms_per_step": round(per * 1e3, 2),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded Siddon matrix, ellipsoid phantom, Poisson sinogram)",
+            "config": {"workload": "plain-full", "grid": [g.nx, g.ny, g.nz], "n_rows": g.n_rows,
+                       "n_cols": g.n_cols, "frames": 1},
+            "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads,
+                             "kind": "reference",
+                             "sample": f"{len(timed)} timed iterations (of the {a.steps} requested; "
+                                       f"capped at 20 to bound the run) of openmpcsr4mlem after "
+                                       f"{wu} warm-up iterations; wall {wall:.1f} s"},
+            "e2e": {"value": round(value, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0},
+        }
+    finally:
+        shutil.rmtree(d, ignore_errors=True)
+
+
+def main():
+    a = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        line = run_reference(a, rank, world)
+    else:
+        line = run_ours(a, rank, world, local_rank)
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

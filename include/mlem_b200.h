@@ -1,0 +1,255 @@
+/*
+ * mlem_b200.h -- C ABI of the B200-native MLEM reconstructor.
+ *
+ * Drop-in boundary for the hot path of the reference tools seqcsr4mlem /
+ * openmpcsr4mlem (gupta-apoorva/mlem):
+ *   calcColumnSums once, then per iteration calcFwProj -> calcCorrel ->
+ *   calcBkProj -> calcUpdate (mlem_seq/seqcsr4mlem.cpp:37-189),
+ * over the CSR4 system matrix of helper_files_common/csr4matrix.cpp:32-157.
+ *
+ * Conventions
+ *   - Every function returns an int status (MLEM_OK == 0); no C++ exception
+ *     crosses the ABI.  Where the reference throws std::runtime_error
+ *     (csr4matrix.cpp:41-136, vector.hpp:35-44) or asserts on a size
+ *     mismatch (seqcsr4mlem.cpp:39,73,96,110,125) these functions return
+ *     MLEM_ERR_FORMAT / MLEM_ERR_IO / MLEM_ERR_INVALID and record a message,
+ *     readable with mlem_last_error(ctx) (or mlem_global_error() when no
+ *     context exists yet).
+ *   - A context owns one matrix on one GPU: the CSR copy, the CSC copy built
+ *     once on the device, the column sums, and the state of B frames
+ *     (sinograms and images).  A context is not thread-safe.
+ *   - Host pointers are caller-owned and only read (or written) during the
+ *     call.  Host frame arrays are frame-major: sinograms [B][R], images
+ *     [B][C].
+ *   - The *_d functions take caller-owned DEVICE pointers and a cudaStream_t
+ *     (passed as void*) and only enqueue work; their frame layout is
+ *     interleaved: x[C][B], y[R][B].
+ *   - Element layout (CSR4 and the device copies): 8 bytes {uint32 index,
+ *     float32 value}, little-endian (helper_files_common/matrixelement.hpp
+ *     :37-46).  Row offsets: the R uint64 row END offsets of the file
+ *     (no leading zero).
+ */
+#ifndef MLEM_B200_H
+#define MLEM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MLEM_B200_VERSION 1
+
+/* ---- status codes ----------------------------------------------------- */
+#define MLEM_OK 0
+#define MLEM_ERR_INVALID 1   /* bad argument or size mismatch */
+#define MLEM_ERR_CUDA 2      /* CUDA runtime error (message has the name) */
+#define MLEM_ERR_IO 3        /* cannot open / read / write a file */
+#define MLEM_ERR_FORMAT 4    /* not a valid CSR4 file or vector file */
+#define MLEM_ERR_NOMEM 5     /* device or host allocation failed */
+#define MLEM_ERR_STATE 6     /* call out of order (e.g. iterate before sinograms) */
+#define MLEM_ERR_MATRIX 7    /* matrix content invalid (column >= C, offsets decreasing) */
+#define MLEM_NO_CHECKPOINT 8 /* mlem_checkpoint_read: no complete checkpoint present */
+
+/* ---- context flags ------------------------------------------------------ */
+#define MLEM_FLAG_EXACT 0x1u    /* bit-exact kernels: the float operation order of seqcsr4mlem */
+#define MLEM_FLAG_NO_CSC 0x2u   /* do not build the CSC copy (atomic back projection only) */
+#define MLEM_FLAG_CHECKED 0x4u  /* validate offsets and column indices on the device at create */
+
+/* ---- back-projection strategies ---------------------------------------- */
+#define MLEM_BK_AUTO 0    /* the autotuner's choice (CSC when not tuned) */
+#define MLEM_BK_CSC 1     /* gather over the device CSC copy, fused with calcUpdate (deterministic) */
+#define MLEM_BK_ATOMIC 2  /* atomic scatter over the CSR (reference GPU drivers' method) */
+#define MLEM_BK_FUSED 3   /* one pass per row: fwproj, correl and atomic scatter together */
+
+typedef struct mlem_ctx mlem_ctx;
+
+typedef struct {
+    uint32_t n_rows;      /* LORs */
+    uint32_t n_cols;      /* voxels */
+    uint64_t nnz;
+    uint32_t n_frames;    /* B of the current sinograms (0 before mlem_set_sinograms) */
+    uint32_t flags;
+    int device;
+    int has_csc;
+    uint32_t max_col_len;
+    uint32_t max_row_len;
+    uint64_t device_bytes; /* device memory held by the context */
+} mlem_info;
+
+/* Launch configuration chosen by the autotuner (or set by the caller). */
+typedef struct {
+    int bk_mode;        /* MLEM_BK_CSC, MLEM_BK_ATOMIC or MLEM_BK_FUSED */
+    int group;          /* lanes per row/column: 4, 8, 16 or 32 */
+    int frame_tile;     /* frames per pass over the matrix: 1, 2, 4, 8 or 16 */
+    int blocks_per_sm;  /* 1..8 blocks of 256 threads per SM */
+    double ms_per_iter; /* measured by mlem_autotune; 0 when set by hand */
+} mlem_tuning;
+
+/* ---- errors ------------------------------------------------------------- */
+const char* mlem_last_error(const mlem_ctx* ctx);
+const char* mlem_global_error(void);
+const char* mlem_status_string(int status);
+int mlem_version(void);
+
+/* ---- context lifecycle -------------------------------------------------- */
+/* Replaces Csr4Matrix + mapRows (csr4matrix.cpp:32-224): uploads the CSR4
+ * arrays (row_end = the file's R row END offsets) to `device`, builds the
+ * CSC copy (unless MLEM_FLAG_NO_CSC) and computes the column sums. */
+int mlem_create(mlem_ctx** out, const uint64_t* row_end, const void* elems, uint32_t n_rows,
+                uint32_t n_cols, uint64_t nnz, uint32_t flags, int device);
+
+/* Same, from a CSR4 file (the command-line driver's path). */
+int mlem_create_from_file(mlem_ctx** out, const char* csr4_path, uint32_t flags, int device);
+
+/* Synthetic Siddon matrix generated on the device (bit-identical to the host
+ * generator of mlem_b200/gen); the reference relies on an external generator. */
+int mlem_create_siddon(mlem_ctx** out, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t n_rows,
+                       uint32_t min_count, uint32_t max_count, double radius_scale,
+                       double min_len, uint64_t seed, uint32_t flags, int device);
+
+void mlem_destroy(mlem_ctx* ctx);
+int mlem_get_info(const mlem_ctx* ctx, mlem_info* out);
+/* Enqueue the context's work on `stream` (a cudaStream_t of the context's
+ * device; NULL restores the context's own stream).  Lets a caller order the
+ * reconstruction with its own work and time it with its own events. */
+int mlem_set_stream(mlem_ctx* ctx, void* stream);
+/* Number of kernels one iteration launches with the current tuning and
+ * frame count (the iteration, plus the two image-statistics kernels). */
+int mlem_kernels_per_iteration(const mlem_ctx* ctx, int* n);
+
+/* Copy the device CSR back: row_end[R] (END offsets), elems[Z]. */
+int mlem_get_csr(mlem_ctx* ctx, uint64_t* row_end, void* elems);
+/* Copy the device CSC: col_ptr[C+1] (leading 0), elems[Z] {row, value}. */
+int mlem_get_csc(mlem_ctx* ctx, uint64_t* col_ptr, void* elems);
+
+/* ---- the reference's five functions, on host buffers ------------------ */
+/* seqcsr4mlem.cpp:37-49 calcColumnSums -> norm[C] (bit-exact). */
+int mlem_calc_column_sums(mlem_ctx* ctx, float* norm);
+/* seqcsr4mlem.cpp:52-66 initImage: float(sum_double(sino) / sum_double(norm)). */
+int mlem_init_value(mlem_ctx* ctx, const int32_t* sino, uint64_t sino_len, float* initial);
+/* seqcsr4mlem.cpp:69-91 calcFwProj: fwproj[R] = A image[C]. */
+int mlem_calc_fwproj(mlem_ctx* ctx, const float* image, float* fwproj);
+/* seqcsr4mlem.cpp:94-105 calcCorrel: correl[R] = fwproj != 0 ? sino / fwproj : 0. */
+int mlem_calc_correl(mlem_ctx* ctx, const float* fwproj, const int32_t* sino, uint64_t sino_len,
+                     float* correl);
+/* seqcsr4mlem.cpp:108-120 calcBkProj: update[C] = A^T correl[R]. */
+int mlem_calc_bkproj(mlem_ctx* ctx, const float* correl, float* update);
+/* seqcsr4mlem.cpp:123-134 calcUpdate: image *= norm != 0 ? update / norm : update. */
+int mlem_calc_update(mlem_ctx* ctx, const float* update, const float* norm, float* image);
+
+/* ---- device-resident reconstruction (seqcsr4mlem.cpp:137-189 mlem) ------ */
+/* Upload B sinograms [B][R] (int32).  Each must have exactly R entries
+ * (the reference asserts this in calcCorrel, seqcsr4mlem.cpp:96). */
+int mlem_set_sinograms(mlem_ctx* ctx, const int32_t* sino, uint32_t n_frames);
+/* initImage for every frame (seqcsr4mlem.cpp:52-66); `initial` (nullable)
+ * receives the B initial values. */
+int mlem_init_images(mlem_ctx* ctx, float* initial);
+/* Set the B images [B][C] (restart from a checkpoint, mpicsr4mlem.cpp:536-553). */
+int mlem_set_images(mlem_ctx* ctx, const float* images);
+/* Run n iterations.  image_sums (nullable) receives [n][B] double image
+ * sums after each iteration; zeros / subnormals (nullable) the per-iteration
+ * zero and subnormal counts [n][B] that seqcsr4mlem prints (:172-185).
+ * The iteration is replayed from a captured CUDA graph. */
+int mlem_iterate(mlem_ctx* ctx, int n_iter, double* image_sums, uint64_t* zeros,
+                 uint64_t* subnormals);
+/* Download the B images [B][C]. */
+int mlem_get_images(mlem_ctx* ctx, float* images);
+/* One iteration end to end on host buffers: upload the B sinograms and the B
+ * images, iterate once on the device, download the images. */
+int mlem_step_host(mlem_ctx* ctx, const int32_t* sino, float* images_inout, uint32_t n_frames);
+
+/* Phases of one iteration, as timed by mlem_profile_phases. */
+#define MLEM_PHASE_PROJECT 0     /* forward projection + calcCorrel (or the one-pass kernel) */
+#define MLEM_PHASE_BACKPROJECT 1 /* back projection (+ calcUpdate for the CSC method) */
+#define MLEM_PHASE_UPDATE 2      /* calcUpdate for the scatter methods */
+#define MLEM_PHASE_STATS 3       /* per-iteration image sum / zero / subnormal census */
+#define MLEM_N_PHASES 4
+
+/* Run n iterations with CUDA events around every phase on the context's
+ * stream.  ms[p]: average device time of phase p per iteration; bytes[p]:
+ * the algorithmic bytes phase p moves per iteration (each matrix element,
+ * offset and vector entry counted once per pass); launches[p]: kernels per
+ * iteration.  Changes the images like mlem_iterate. */
+int mlem_profile_phases(mlem_ctx* ctx, int n_iter, double* ms, double* bytes, int* launches);
+
+/* ---- tuning --------------------------------------------------------------- */
+int mlem_get_tuning(const mlem_ctx* ctx, mlem_tuning* out);
+int mlem_set_tuning(mlem_ctx* ctx, const mlem_tuning* t);
+/* Time every valid configuration for the current B on the device and keep
+ * the fastest (deterministic_only != 0 restricts to MLEM_BK_CSC).  The
+ * image state is restored afterwards. */
+int mlem_autotune(mlem_ctx* ctx, int deterministic_only, mlem_tuning* best);
+
+/* ---- device-pointer entry points (torch extension, custom drivers) ------ */
+/* y[R][B] = A x[C][B]. */
+int mlem_fwproj_d(mlem_ctx* ctx, const float* x, float* y, uint32_t n_frames, void* stream);
+/* x[C][B] = A^T y[R][B]. */
+int mlem_bkproj_d(mlem_ctx* ctx, const float* y, float* x, uint32_t n_frames, void* stream);
+/* correl[R][B] = calcCorrel(sino[R][B], A x[C][B])  (fused). */
+int mlem_fwproj_correl_d(mlem_ctx* ctx, const float* x, const int32_t* sino, float* correl,
+                         uint32_t n_frames, void* stream);
+/* x[C][B] *= calcUpdate factor(A^T correl[R][B], norm)  (fused, CSC). */
+int mlem_bkproj_update_d(mlem_ctx* ctx, const float* correl, float* x, uint32_t n_frames,
+                         void* stream);
+/* x[C][B] *= calcUpdate factor(update[C][B], norm): the update step of a
+ * row-sharded reconstruction after the update vectors of all shards have
+ * been summed (the single exchange of mlem_mpi/fusedmpimlem.cpp:227). */
+int mlem_apply_update_d(mlem_ctx* ctx, const float* update, float* x, uint32_t n_frames,
+                        void* stream);
+/* Device pointer of the context's column sums (float[C]). */
+int mlem_norm_d(mlem_ctx* ctx, const float** norm);
+/* Replace the column sums with norm[C] (device pointer): a row shard uses the
+ * column sums of the whole matrix (mlem_mpi/mpicsr4mlem.cpp:266). */
+int mlem_set_norm_d(mlem_ctx* ctx, const float* norm, void* stream);
+/* Sequential double projection out[R] = A x (bit-identical to the host
+ * generator's; used for synthetic sinogram means).  Host buffers. */
+int mlem_project_f64(mlem_ctx* ctx, const float* x, double* out);
+
+/* ---- host IO: the reference's file formats ------------------------------ */
+typedef struct {
+    uint32_t n_rows, n_cols;
+    uint64_t nnz;
+    uint8_t version, flags;
+    uint32_t scan_config_bytes;
+    uint32_t grid[3];
+    float voxel_size[3];
+    uint64_t file_size;
+    uint64_t data_offset; /* byte offset of the row END offsets */
+} mlem_csr4_header;
+
+/* Parse and validate a CSR4 header like csr4matrix.cpp:32-138, with 64-bit
+ * size arithmetic. */
+int mlem_csr4_read_header(const char* path, mlem_csr4_header* out);
+/* Read the row END offsets [R] and elements [Z] of a CSR4 file. */
+int mlem_csr4_read(const char* path, uint64_t* row_end, void* elems);
+/* Write a CSR4 file with the minimal 60-byte scanner block. */
+int mlem_csr4_write(const char* path, const uint64_t* row_end, const void* elems,
+                    uint32_t n_rows, uint32_t n_cols, const uint32_t grid[3]);
+/* vector.hpp:33-53: element count = file size / elem_size (error if not a
+ * multiple).  Call with buf == NULL to query the count. */
+int mlem_vector_read(const char* path, uint32_t elem_size, void* buf, uint64_t capacity,
+                     uint64_t* count);
+/* vector.hpp:77-87 writeToFile, or :102-114 writeToFileSync when sync != 0. */
+int mlem_vector_write(const char* path, const void* buf, uint32_t elem_size, uint64_t count,
+                      int sync);
+/* mpicsr4mlem.cpp:95-122 checkPointNow: img.chkpt (float32[C], fsync'd) and
+ * iter.chkpt (int32 next iteration) in `dir`. */
+int mlem_checkpoint_write(const char* dir, const float* image, uint32_t n_cols, int32_t next_iter);
+/* mpicsr4mlem.cpp:133-154 restore + :536-550: MLEM_NO_CHECKPOINT unless both
+ * files exist; the image must have exactly n_cols floats. */
+int mlem_checkpoint_read(const char* dir, float* image, uint32_t n_cols, int32_t* next_iter);
+/* mpicsr4mlem.cpp:656-660: remove both checkpoint files. */
+int mlem_checkpoint_remove(const char* dir);
+
+/* mpicsr4mlem.cpp:202-234 partition(): nnz-balanced contiguous row ranges
+ * for n_ranks (starts/ends: n_ranks entries each). */
+int mlem_partition_rows(const uint64_t* row_end, uint32_t n_rows, int n_ranks, uint32_t* starts,
+                        uint32_t* ends);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MLEM_B200_H */

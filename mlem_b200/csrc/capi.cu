@@ -1,0 +1,1081 @@
+// capi.cu -- the mlem_ctx device context behind include/mlem_b200.h.
+//
+// One context = one CSR4 matrix resident on one GPU (CSR copy, CSC copy,
+// column sums) plus the state of B frames.  The iteration of
+// mlem_seq/seqcsr4mlem.cpp:163-167 is enqueued by enqueue_iteration() and
+// replayed from a captured CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <type_traits>
+#include <vector>
+
+#include "host/errors.hpp"
+#include "kernels.h"
+#include "mlem_b200.h"
+
+using namespace mlem;
+
+struct mlem_ctx {
+    int device = 0;
+    int n_sm = 148;
+    uint32_t R = 0, C = 0;
+    uint64_t Z = 0;
+    uint32_t flags = 0;
+    cudaStream_t stream = nullptr;      // where work is enqueued
+    cudaStream_t own_stream = nullptr;  // created with the context
+    uint64_t device_bytes = 0;
+
+    // matrix
+    uint64_t* row_ptr = nullptr;
+    uint2* elems = nullptr;
+    uint64_t* col_ptr = nullptr;
+    uint2* celems = nullptr;
+    bool has_csc = false;
+    uint32_t max_col_len = 0, max_row_len = 0;
+    float* norm = nullptr;
+    std::vector<float> norm_host;
+    double sumnorm = 0.0;
+
+    // frames
+    uint32_t B = 0, Bp = 0;
+    std::vector<double> sumin;
+    int32_t* sino = nullptr;
+    float* x = nullptr;
+    float* correl = nullptr;
+    float* update = nullptr;
+    void* stage = nullptr;  // staging for frame-major <-> interleaved copies
+    size_t stage_bytes = 0;
+    bool images_ready = false;
+
+    // statistics history
+    void* stats_scratch = nullptr;
+    unsigned int* stats_slot = nullptr;
+    double* hist_sums = nullptr;
+    unsigned long long* hist_zeros = nullptr;
+    unsigned long long* hist_subn = nullptr;
+    int hist_cap = 0;
+
+    // scratch for the host-buffer reference functions
+    float* tmp_r[2] = {nullptr, nullptr};
+    float* tmp_c[3] = {nullptr, nullptr, nullptr};
+    int32_t* tmp_sino = nullptr;
+    double* tmp_d = nullptr;
+    float* inits_dev = nullptr;
+
+    mlem_tuning tuning{};
+    cudaGraphExec_t graph = nullptr;
+    int graph_iters = 0;
+    bool graph_dirty = true;
+
+    std::string err;
+};
+
+namespace {
+
+int fail(mlem_ctx* ctx, int status, const char* fmt, ...) __attribute__((format(printf, 3, 4)));
+int fail(mlem_ctx* ctx, int status, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    return set_error(ctx ? &ctx->err : nullptr, status, "%s", buf);
+}
+
+#define CK(ctx, call)                                                                       \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return fail((ctx), e_ == cudaErrorMemoryAllocation ? MLEM_ERR_NOMEM : MLEM_ERR_CUDA, \
+                        "%s: %s (%s:%d)", cudaGetErrorName(e_), cudaGetErrorString(e_),    \
+                        __FILE__, __LINE__);                                                \
+    } while (0)
+
+#define TRY(call)                         \
+    do {                                  \
+        int s_ = (call);                  \
+        if (s_ != MLEM_OK) return s_;     \
+    } while (0)
+
+int dev_alloc(mlem_ctx* c, void** p, size_t bytes) {
+    if (bytes == 0) bytes = 256;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return fail(c, MLEM_ERR_NOMEM, "cudaMalloc of %zu bytes failed: %s", bytes,
+                    cudaGetErrorString(e));
+    }
+    c->device_bytes += bytes;
+    return MLEM_OK;
+}
+
+template <typename T>
+int dev_alloc(mlem_ctx* c, T** p, size_t count) {
+    return dev_alloc(c, reinterpret_cast<void**>(p), count * sizeof(T));
+}
+
+void dev_free(void* p) {
+    if (p) cudaFree(p);
+}
+
+SparseView csr_view(const mlem_ctx* c) {
+    return SparseView{c->row_ptr, reinterpret_cast<const uint4*>(c->elems), c->R, c->Z};
+}
+SparseView csc_view(const mlem_ctx* c) {
+    return SparseView{c->col_ptr, reinterpret_cast<const uint4*>(c->celems), c->C, c->Z};
+}
+
+int sm_count(int device) {
+    int n = 0;
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) n = 148;
+    return n > 0 ? n : 148;
+}
+
+LaunchCfg cfg_of(const mlem_ctx* c, const mlem_tuning& t) {
+    LaunchCfg cfg;
+    cfg.group = t.group;
+    cfg.frame_tile = t.frame_tile;
+    cfg.blocks_per_sm = t.blocks_per_sm;
+    cfg.sm_count = c->n_sm;
+    return cfg;
+}
+
+// Interleave stride for B frames: every frame tile 1..16 that fits divides it.
+uint32_t padded_frames(uint32_t B) {
+    for (uint32_t p : {1u, 2u, 4u, 8u, 16u, 32u, 48u, 64u})
+        if (B <= p) return p;
+    return 0;
+}
+
+// Widest frame tile (<= 16) that divides Bp.
+int default_tile(uint32_t Bp) {
+    for (int t : {16, 8, 4, 2})
+        if (Bp % t == 0) return t;
+    return 1;
+}
+
+int set_device(mlem_ctx* c) {
+    CK(c, cudaSetDevice(c->device));
+    return MLEM_OK;
+}
+
+void default_tuning(mlem_ctx* c) {
+    c->tuning.bk_mode = c->has_csc ? MLEM_BK_CSC : MLEM_BK_ATOMIC;
+    c->tuning.group = 32;
+    c->tuning.frame_tile = c->Bp ? std::min(default_tile(c->Bp), 16) : 1;
+    c->tuning.blocks_per_sm = 8;
+    c->tuning.ms_per_iter = 0.0;
+}
+
+// ---------------------------------------------------------------------------
+// Setup common to all create paths: validate, CSC, column sums.
+// ---------------------------------------------------------------------------
+int finish_create(mlem_ctx* c) {
+    // device-side validation: offsets non-decreasing, last offset == Z, columns < C
+    unsigned int* bad = nullptr;
+    TRY(dev_alloc(c, &bad, 1));
+    CK(c, validate_csr(csr_view(c), c->C, bad, c->stream));
+    unsigned int hbad = 0;
+    CK(c, cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    cudaFree(bad);
+    c->device_bytes -= sizeof(unsigned int);
+    if (hbad & 1u) return fail(c, MLEM_ERR_MATRIX, "row offsets decrease");
+    if (hbad & 2u) return fail(c, MLEM_ERR_MATRIX, "last row offset differs from nnz");
+    if (hbad & 4u) return fail(c, MLEM_ERR_MATRIX, "a column index is >= the number of columns");
+
+    if (!(c->flags & MLEM_FLAG_NO_CSC)) {
+        TRY(dev_alloc(c, &c->col_ptr, (size_t)c->C + 1));
+        TRY(dev_alloc(c, &c->celems, c->Z + 2));
+        CK(c, cudaMemsetAsync(c->celems + c->Z, 0, 2 * sizeof(uint2), c->stream));
+        void* scratch = nullptr;
+        const size_t sb = transpose_scratch_bytes(c->C);
+        TRY(dev_alloc(c, &scratch, sb));
+        cudaError_t e = transpose(csr_view(c), c->C, c->col_ptr, c->celems, scratch,
+                                  &c->max_col_len, c->stream);
+        cudaFree(scratch);
+        c->device_bytes -= sb;
+        CK(c, e);
+        c->has_csc = true;
+        CK(c, column_sums_exact(csc_view(c), c->norm, c->stream));
+    } else {
+        CK(c, column_sums_atomic(csr_view(c), c->C, c->norm, c->stream));
+    }
+    c->norm_host.resize(c->C);
+    if (c->C)
+        CK(c, cudaMemcpyAsync(c->norm_host.data(), c->norm, (size_t)c->C * 4,
+                              cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    // initImage's sum (seqcsr4mlem.cpp:55-56): sequential double sum of the norm.
+    double s = 0.0;
+    for (uint32_t i = 0; i < c->C; ++i) s += c->norm_host[i];
+    c->sumnorm = s;
+    default_tuning(c);
+    return MLEM_OK;
+}
+
+int alloc_matrix(mlem_ctx* c) {
+    TRY(dev_alloc(c, &c->row_ptr, (size_t)c->R + 1));
+    TRY(dev_alloc(c, &c->elems, c->Z + 2));  // even element count + one spare pair word
+    TRY(dev_alloc(c, &c->norm, (size_t)std::max<uint32_t>(c->C, 1)));
+    CK(c, cudaMemsetAsync(c->row_ptr, 0, 8, c->stream));
+    CK(c, cudaMemsetAsync(c->elems + c->Z, 0, 2 * sizeof(uint2), c->stream));
+    return MLEM_OK;
+}
+
+int new_ctx(mlem_ctx** out, uint32_t R, uint32_t C, uint64_t Z, uint32_t flags, int device) {
+    *out = nullptr;
+    int n_dev = 0;
+    cudaError_t e = cudaGetDeviceCount(&n_dev);
+    if (e != cudaSuccess || n_dev == 0)
+        return fail(nullptr, MLEM_ERR_CUDA, "no CUDA device available (%s)",
+                    e != cudaSuccess ? cudaGetErrorString(e) : "0 devices");
+    if (device < 0 || device >= n_dev)
+        return fail(nullptr, MLEM_ERR_INVALID, "device %d out of range (%d devices)", device, n_dev);
+    if (flags & ~(MLEM_FLAG_EXACT | MLEM_FLAG_NO_CSC | MLEM_FLAG_CHECKED))
+        return fail(nullptr, MLEM_ERR_INVALID, "unknown flags 0x%x", flags);
+    if ((flags & MLEM_FLAG_EXACT) && (flags & MLEM_FLAG_NO_CSC))
+        return fail(nullptr, MLEM_ERR_INVALID, "MLEM_FLAG_EXACT needs the CSC copy");
+    mlem_ctx* c = new mlem_ctx();
+    c->device = device;
+    c->R = R;
+    c->C = C;
+    c->Z = Z;
+    c->flags = flags;
+    int s = set_device(c);
+    c->n_sm = sm_count(device);
+    if (s == MLEM_OK) {
+        cudaError_t e2 = cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking);
+        if (e2 != cudaSuccess) s = fail(c, MLEM_ERR_CUDA, "stream: %s", cudaGetErrorString(e2));
+        c->stream = c->own_stream;
+    }
+    if (s != MLEM_OK) {
+        global_error() = c->err;
+        mlem_destroy(c);
+        return s;
+    }
+    *out = c;
+    return MLEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Frames.
+// ---------------------------------------------------------------------------
+int ensure_stage(mlem_ctx* c, size_t bytes) {
+    if (c->stage_bytes >= bytes) return MLEM_OK;
+    if (c->stage) { cudaFree(c->stage); c->device_bytes -= c->stage_bytes; }
+    c->stage = nullptr;
+    c->stage_bytes = 0;
+    TRY(dev_alloc(c, &c->stage, bytes));
+    c->stage_bytes = bytes;
+    return MLEM_OK;
+}
+
+void free_frames(mlem_ctx* c) {
+    for (void* p : {(void*)c->sino, (void*)c->x, (void*)c->correl, (void*)c->update,
+                    (void*)c->stats_scratch, (void*)c->inits_dev})
+        dev_free(p);
+    c->sino = nullptr; c->x = nullptr; c->correl = nullptr; c->update = nullptr;
+    c->stats_scratch = nullptr; c->inits_dev = nullptr;
+    c->B = c->Bp = 0;
+    c->images_ready = false;
+}
+
+int alloc_frames(mlem_ctx* c, uint32_t B) {
+    const uint32_t Bp = padded_frames(B);
+    if (B == 0 || Bp == 0) return fail(c, MLEM_ERR_INVALID, "n_frames must be 1..64 (got %u)", B);
+    if (c->B == B && c->sino) return MLEM_OK;
+    free_frames(c);
+    c->B = B;
+    c->Bp = Bp;
+    TRY(dev_alloc(c, &c->sino, (size_t)c->R * Bp));
+    TRY(dev_alloc(c, &c->x, (size_t)c->C * Bp));
+    TRY(dev_alloc(c, &c->correl, (size_t)c->R * Bp));
+    TRY(dev_alloc(c, &c->update, (size_t)c->C * Bp));
+    TRY(dev_alloc(c, &c->stats_scratch, stats_scratch_bytes(Bp)));
+    TRY(dev_alloc(c, &c->inits_dev, Bp));
+    CK(c, cudaMemsetAsync(c->sino, 0, (size_t)c->R * Bp * 4, c->stream));
+    CK(c, cudaMemsetAsync(c->x, 0, (size_t)c->C * Bp * 4, c->stream));
+    CK(c, cudaMemsetAsync(c->correl, 0, (size_t)c->R * Bp * 4, c->stream));
+    CK(c, cudaMemsetAsync(c->update, 0, (size_t)c->C * Bp * 4, c->stream));
+    c->tuning.frame_tile = std::min(c->tuning.frame_tile > 0 ? c->tuning.frame_tile : 16,
+                                    default_tile(Bp));
+    if (c->tuning.frame_tile > c->tuning.group) c->tuning.frame_tile = c->tuning.group;
+    c->graph_dirty = true;
+    return MLEM_OK;
+}
+
+// Frame-major host [B][n] -> interleaved device [n][Bp] (pad frames untouched).
+template <typename T>
+int upload_frames(mlem_ctx* c, const T* host, T* dev, uint64_t n) {
+    if (c->Bp == 1) {
+        CK(c, cudaMemcpyAsync(dev, host, n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+        return MLEM_OK;
+    }
+    TRY(ensure_stage(c, n * c->B * sizeof(T)));
+    CK(c, cudaMemcpyAsync(c->stage, host, n * c->B * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+    if (std::is_same<T, int32_t>::value)
+        CK(c, interleave_i32(reinterpret_cast<const int32_t*>(c->stage),
+                             reinterpret_cast<int32_t*>(dev), n, c->B, c->Bp, c->stream));
+    else
+        CK(c, interleave_f32(reinterpret_cast<const float*>(c->stage),
+                             reinterpret_cast<float*>(dev), n, c->B, c->Bp, c->stream));
+    return MLEM_OK;
+}
+
+int download_images(mlem_ctx* c, float* host) {
+    if (c->Bp == 1) {
+        CK(c, cudaMemcpyAsync(host, c->x, (size_t)c->C * 4, cudaMemcpyDeviceToHost, c->stream));
+        return MLEM_OK;
+    }
+    TRY(ensure_stage(c, (size_t)c->C * c->B * 4));
+    float* st = static_cast<float*>(c->stage);
+    CK(c, deinterleave_f32(c->x, st, c->C, c->B, c->Bp, c->stream));
+    CK(c, cudaMemcpyAsync(host, st, (size_t)c->C * c->B * 4, cudaMemcpyDeviceToHost, c->stream));
+    return MLEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// One MLEM iteration (seqcsr4mlem.cpp:164-167) plus the image statistics.
+// ---------------------------------------------------------------------------
+// Events recorded at the phase boundaries of one iteration (profiling only).
+struct PhaseEvents {
+    cudaEvent_t ev[MLEM_N_PHASES + 1];
+};
+
+int mark(mlem_ctx* c, const PhaseEvents* pe, int i) {
+    if (pe) CK(c, cudaEventRecord(pe->ev[i], c->stream));
+    return MLEM_OK;
+}
+
+int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
+                      const PhaseEvents* pe = nullptr) {
+    const SparseView csr = csr_view(c);
+    const uint32_t Bp = c->Bp;
+    cudaStream_t st = c->stream;
+    TRY(mark(c, pe, 0));
+    if (c->flags & MLEM_FLAG_EXACT) {
+        CK(c, fwproj_exact(csr, c->x, Bp, c->sino, c->correl, nullptr, st));
+        TRY(mark(c, pe, 1));
+        CK(c, bkproj_exact(csc_view(c), c->correl, Bp, c->norm, c->x, nullptr, st));
+        TRY(mark(c, pe, 2));
+    } else {
+        const LaunchCfg cfg = cfg_of(c, t);
+        const uint32_t T = (uint32_t)t.frame_tile;
+        switch (t.bk_mode) {
+            case MLEM_BK_CSC:
+                if (!c->has_csc) return fail(c, MLEM_ERR_STATE, "no CSC copy (MLEM_FLAG_NO_CSC)");
+                for (uint32_t f0 = 0; f0 < Bp; f0 += T)
+                    CK(c, fwproj(csr, c->x, Bp, f0, c->sino, c->correl, nullptr, cfg, st));
+                TRY(mark(c, pe, 1));
+                for (uint32_t f0 = 0; f0 < Bp; f0 += T)
+                    CK(c, bkproj_csc(csc_view(c), c->correl, Bp, f0, c->norm, c->x, nullptr, cfg, st));
+                TRY(mark(c, pe, 2));
+                break;
+            case MLEM_BK_ATOMIC:
+                for (uint32_t f0 = 0; f0 < Bp; f0 += T)
+                    CK(c, fwproj(csr, c->x, Bp, f0, c->sino, c->correl, nullptr, cfg, st));
+                TRY(mark(c, pe, 1));
+                for (uint32_t f0 = 0; f0 < Bp; f0 += T)
+                    CK(c, bkproj_scatter(csr, c->correl, Bp, f0, c->update, cfg, st));
+                TRY(mark(c, pe, 2));
+                CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
+                break;
+            case MLEM_BK_FUSED:
+                for (uint32_t f0 = 0; f0 < Bp; f0 += T)
+                    CK(c, fused_row(csr, c->x, Bp, f0, c->sino, c->update, cfg, st));
+                TRY(mark(c, pe, 1));
+                TRY(mark(c, pe, 2));
+                CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
+                break;
+            default:
+                return fail(c, MLEM_ERR_INVALID, "unknown back-projection mode %d", t.bk_mode);
+        }
+    }
+    TRY(mark(c, pe, 3));
+    if (stats)
+        CK(c, image_stats(c->x, c->C, Bp, c->B, c->stats_scratch, c->stats_slot, c->hist_sums,
+                          c->hist_zeros, c->hist_subn, st));
+    TRY(mark(c, pe, 4));
+    return MLEM_OK;
+}
+
+// Algorithmic bytes of each phase per iteration: every matrix element and
+// offset once per pass over the matrix (one pass per frame tile), every
+// vector entry once per read or write, for the B real frames.
+void phase_bytes(const mlem_ctx* c, double* bytes, int* launches) {
+    const double R = c->R, C = c->C, Z = (double)c->Z, B = c->B;
+    const bool exact = (c->flags & MLEM_FLAG_EXACT) != 0;
+    const int mode = exact ? MLEM_BK_CSC : c->tuning.bk_mode;
+    const double tiles = exact ? 1.0 : (double)(c->Bp / (uint32_t)c->tuning.frame_tile);
+    const double csr_pass = 8.0 * (R + 1) + 8.0 * Z;
+    const double csc_pass = 8.0 * (C + 1) + 8.0 * Z;
+    for (int p = 0; p < MLEM_N_PHASES; ++p) { bytes[p] = 0.0; launches[p] = 0; }
+    const int nt = (int)tiles;
+    if (mode == MLEM_BK_FUSED) {
+        bytes[0] = tiles * csr_pass + B * (4.0 * C + 4.0 * R + 4.0 * C);  // x, sino, update
+        launches[0] = nt;
+    } else {
+        bytes[0] = tiles * csr_pass + B * (4.0 * C + 4.0 * R + 4.0 * R);  // x, sino, correl
+        launches[0] = exact ? 1 : nt;
+    }
+    if (mode == MLEM_BK_CSC) {
+        bytes[1] = tiles * (csc_pass + 4.0 * C) + B * (4.0 * R + 8.0 * C);  // norm, correl, x r/w
+        launches[1] = exact ? 1 : nt;
+    } else if (mode == MLEM_BK_ATOMIC) {
+        bytes[1] = tiles * csr_pass + B * (4.0 * R + 4.0 * C);  // correl, update
+        launches[1] = nt;
+    }
+    if (mode != MLEM_BK_CSC) {
+        bytes[2] = 4.0 * C + B * (4.0 * C + 8.0 * C + 4.0 * C);  // norm, update, x r/w, zeroing
+        launches[2] = 1;
+    }
+    bytes[3] = 4.0 * C * B;
+    launches[3] = 2;
+}
+
+int ensure_history(mlem_ctx* c, int n) {
+    if (!c->stats_slot) TRY(dev_alloc(c, &c->stats_slot, 1));
+    if (c->hist_cap >= n && c->hist_sums) return MLEM_OK;
+    dev_free(c->hist_sums); dev_free(c->hist_zeros); dev_free(c->hist_subn);
+    c->hist_sums = nullptr; c->hist_zeros = nullptr; c->hist_subn = nullptr;
+    const int cap = std::max(n, 64);
+    TRY(dev_alloc(c, &c->hist_sums, (size_t)cap * 64));
+    TRY(dev_alloc(c, &c->hist_zeros, (size_t)cap * 64));
+    TRY(dev_alloc(c, &c->hist_subn, (size_t)cap * 64));
+    c->hist_cap = cap;
+    c->graph_dirty = true;  // graphs hold the history pointers
+    return MLEM_OK;
+}
+
+void drop_graph(mlem_ctx* c) {
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    c->graph = nullptr;
+    c->graph_iters = 0;
+}
+
+// Capture `n` iterations (slot reset + n x (iteration + statistics)) as one graph.
+int capture(mlem_ctx* c, int n) {
+    drop_graph(c);
+    CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    int s = MLEM_OK;
+    cudaError_t e = cudaMemsetAsync(c->stats_slot, 0, sizeof(unsigned int), c->stream);
+    if (e != cudaSuccess) s = fail(c, MLEM_ERR_CUDA, "capture memset: %s", cudaGetErrorString(e));
+    for (int i = 0; i < n && s == MLEM_OK; ++i) s = enqueue_iteration(c, c->tuning, true);
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+    if (s != MLEM_OK) { if (g) cudaGraphDestroy(g); return s; }
+    if (e2 != cudaSuccess) return fail(c, MLEM_ERR_CUDA, "end capture: %s", cudaGetErrorString(e2));
+    e2 = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) return fail(c, MLEM_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e2));
+    c->graph_iters = n;
+    c->graph_dirty = false;
+    return MLEM_OK;
+}
+
+int ensure_tmp(mlem_ctx* c) {
+    if (c->tmp_r[0]) return MLEM_OK;
+    for (auto& p : c->tmp_r) TRY(dev_alloc(c, &p, std::max<uint32_t>(c->R, 1)));
+    for (auto& p : c->tmp_c) TRY(dev_alloc(c, &p, std::max<uint32_t>(c->C, 1)));
+    TRY(dev_alloc(c, &c->tmp_sino, std::max<uint32_t>(c->R, 1)));
+    return MLEM_OK;
+}
+
+LaunchCfg cfg_for_frames(const mlem_ctx* c, uint32_t B) {
+    LaunchCfg cfg = cfg_of(c, c->tuning);
+    int t = 1;
+    for (int v : {16, 8, 4, 2})
+        if (B % v == 0) { t = v; break; }
+    cfg.frame_tile = t;
+    if (cfg.group < t) cfg.group = t;
+    return cfg;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+extern "C" {
+
+const char* mlem_last_error(const mlem_ctx* ctx) {
+    return ctx ? ctx->err.c_str() : global_error().c_str();
+}
+const char* mlem_global_error(void) { return global_error().c_str(); }
+int mlem_version(void) { return MLEM_B200_VERSION; }
+
+const char* mlem_status_string(int s) {
+    switch (s) {
+        case MLEM_OK: return "ok";
+        case MLEM_ERR_INVALID: return "invalid argument";
+        case MLEM_ERR_CUDA: return "CUDA error";
+        case MLEM_ERR_IO: return "I/O error";
+        case MLEM_ERR_FORMAT: return "bad file format";
+        case MLEM_ERR_NOMEM: return "out of memory";
+        case MLEM_ERR_STATE: return "call out of order";
+        case MLEM_ERR_MATRIX: return "invalid matrix";
+        case MLEM_NO_CHECKPOINT: return "no checkpoint";
+        default: return "unknown status";
+    }
+}
+
+int mlem_create(mlem_ctx** out, const uint64_t* row_end, const void* elems, uint32_t n_rows,
+                uint32_t n_cols, uint64_t nnz, uint32_t flags, int device) {
+    if (!out) return fail(nullptr, MLEM_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if ((n_rows && !row_end) || (nnz && !elems))
+        return fail(nullptr, MLEM_ERR_INVALID, "null matrix arrays");
+    // host checks of the offsets (cheap, R values)
+    uint64_t prev = 0, max_row = 0;
+    for (uint32_t r = 0; r < n_rows; ++r) {
+        if (row_end[r] < prev) return fail(nullptr, MLEM_ERR_MATRIX, "row offsets decrease at row %u", r);
+        max_row = std::max(max_row, row_end[r] - prev);
+        prev = row_end[r];
+    }
+    if (prev != nnz)
+        return fail(nullptr, MLEM_ERR_MATRIX, "last row END offset %llu differs from nnz %llu",
+                    (unsigned long long)prev, (unsigned long long)nnz);
+    mlem_ctx* c = nullptr;
+    TRY(new_ctx(&c, n_rows, n_cols, nnz, flags, device));
+    c->max_row_len = (uint32_t)std::min<uint64_t>(max_row, 0xffffffffu);
+    int s = alloc_matrix(c);
+    if (s == MLEM_OK && n_rows) {
+        cudaError_t e = cudaMemcpyAsync(c->row_ptr + 1, row_end, (size_t)n_rows * 8,
+                                        cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess && nnz)
+            e = cudaMemcpyAsync(c->elems, elems, nnz * 8, cudaMemcpyHostToDevice, c->stream);
+        if (e != cudaSuccess) s = fail(c, MLEM_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
+    }
+    if (s == MLEM_OK) s = finish_create(c);
+    if (s != MLEM_OK) {
+        global_error() = c->err;
+        mlem_destroy(c);
+        return s;
+    }
+    *out = c;
+    return MLEM_OK;
+}
+
+int mlem_create_siddon(mlem_ctx** out, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t n_rows,
+                       uint32_t min_count, uint32_t max_count, double radius_scale,
+                       double min_len, uint64_t seed, uint32_t flags, int device) {
+    if (!out) return fail(nullptr, MLEM_ERR_INVALID, "out is null");
+    *out = nullptr;
+    if (nx == 0 || ny == 0 || nz == 0) return fail(nullptr, MLEM_ERR_INVALID, "empty voxel grid");
+    const uint64_t C64 = (uint64_t)nx * ny * nz;
+    if (C64 > 0xffffffffull) return fail(nullptr, MLEM_ERR_INVALID, "grid has more than 2^32 voxels");
+    if (!(min_len > 0.0)) return fail(nullptr, MLEM_ERR_INVALID, "min_len must be > 0");
+    mlem_ctx* c = nullptr;
+    TRY(new_ctx(&c, n_rows, (uint32_t)C64, 0, flags, device));
+    SiddonSpec spec{nx, ny, nz, n_rows, min_count, max_count, radius_scale, min_len, seed};
+    int s = MLEM_OK;
+    uint64_t* counts = nullptr;
+    void* scratch = nullptr;
+    const size_t sb = scan_scratch_bytes(n_rows);
+    do {
+        if ((s = dev_alloc(c, &c->row_ptr, (size_t)n_rows + 1)) != MLEM_OK) break;
+        if ((s = dev_alloc(c, &counts, std::max<uint32_t>(n_rows, 1))) != MLEM_OK) break;
+        if ((s = dev_alloc(c, &scratch, sb)) != MLEM_OK) break;
+        cudaError_t e = siddon_counts(spec, counts, c->stream);
+        if (e == cudaSuccess) e = exclusive_scan_u64(counts, c->row_ptr, n_rows, scratch, c->stream);
+        uint64_t Z = 0;
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(&Z, c->row_ptr + n_rows, 8, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) { s = fail(c, MLEM_ERR_CUDA, "generator: %s", cudaGetErrorString(e)); break; }
+        c->Z = Z;
+        if ((s = dev_alloc(c, &c->elems, Z + 2)) != MLEM_OK) break;
+        if ((s = dev_alloc(c, &c->norm, std::max<uint32_t>(c->C, 1))) != MLEM_OK) break;
+        e = cudaMemsetAsync(c->elems + Z, 0, 2 * sizeof(uint2), c->stream);
+        if (e == cudaSuccess) e = siddon_fill(spec, c->row_ptr, c->elems, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) { s = fail(c, MLEM_ERR_CUDA, "generator fill: %s", cudaGetErrorString(e)); break; }
+        // longest row, for the info block
+        std::vector<uint64_t> rp((size_t)n_rows + 1);
+        e = cudaMemcpy(rp.data(), c->row_ptr, rp.size() * 8, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) { s = fail(c, MLEM_ERR_CUDA, "%s", cudaGetErrorString(e)); break; }
+        uint64_t mr = 0;
+        for (uint32_t r = 0; r < n_rows; ++r) mr = std::max(mr, rp[r + 1] - rp[r]);
+        c->max_row_len = (uint32_t)mr;
+    } while (0);
+    dev_free(counts);
+    dev_free(scratch);
+    if (s == MLEM_OK) s = finish_create(c);
+    if (s != MLEM_OK) {
+        global_error() = c->err;
+        mlem_destroy(c);
+        return s;
+    }
+    *out = c;
+    return MLEM_OK;
+}
+
+void mlem_destroy(mlem_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    drop_graph(c);
+    free_frames(c);
+    for (void* p : {(void*)c->row_ptr, (void*)c->elems, (void*)c->col_ptr, (void*)c->celems,
+                    (void*)c->norm, c->stage, (void*)c->stats_slot, (void*)c->hist_sums,
+                    (void*)c->hist_zeros, (void*)c->hist_subn, (void*)c->tmp_r[0],
+                    (void*)c->tmp_r[1], (void*)c->tmp_c[0], (void*)c->tmp_c[1], (void*)c->tmp_c[2],
+                    (void*)c->tmp_sino, (void*)c->tmp_d})
+        dev_free(p);
+    if (c->own_stream) cudaStreamSynchronize(c->own_stream);
+    if (c->own_stream) cudaStreamDestroy(c->own_stream);
+    delete c;
+}
+
+int mlem_get_info(const mlem_ctx* c, mlem_info* out) {
+    if (!c || !out) return fail(nullptr, MLEM_ERR_INVALID, "null argument");
+    out->n_rows = c->R;
+    out->n_cols = c->C;
+    out->nnz = c->Z;
+    out->n_frames = c->B;
+    out->flags = c->flags;
+    out->device = c->device;
+    out->has_csc = c->has_csc ? 1 : 0;
+    out->max_col_len = c->max_col_len;
+    out->max_row_len = c->max_row_len;
+    out->device_bytes = c->device_bytes;
+    return MLEM_OK;
+}
+
+int mlem_set_stream(mlem_ctx* c, void* stream) {
+    if (!c) return fail(nullptr, MLEM_ERR_INVALID, "null context");
+    TRY(set_device(c));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+    c->graph_dirty = true;
+    return MLEM_OK;
+}
+
+int mlem_kernels_per_iteration(const mlem_ctx* c, int* n) {
+    if (!c || !n) return fail(nullptr, MLEM_ERR_INVALID, "null argument");
+    if (!c->Bp) return fail(const_cast<mlem_ctx*>(c), MLEM_ERR_STATE, "no frames");
+    const int tiles = (int)(c->Bp / (uint32_t)c->tuning.frame_tile);
+    int k = 2;  // image statistics
+    if (c->flags & MLEM_FLAG_EXACT) k += 2;
+    else if (c->tuning.bk_mode == MLEM_BK_CSC) k += 2 * tiles;
+    else if (c->tuning.bk_mode == MLEM_BK_ATOMIC) k += 2 * tiles + 1;
+    else k += tiles + 1;
+    *n = k;
+    return MLEM_OK;
+}
+
+int mlem_get_csr(mlem_ctx* c, uint64_t* row_end, void* elems) {
+    if (!c) return fail(nullptr, MLEM_ERR_INVALID, "null context");
+    TRY(set_device(c));
+    if (row_end && c->R)
+        CK(c, cudaMemcpy(row_end, c->row_ptr + 1, (size_t)c->R * 8, cudaMemcpyDeviceToHost));
+    if (elems && c->Z) CK(c, cudaMemcpy(elems, c->elems, c->Z * 8, cudaMemcpyDeviceToHost));
+    return MLEM_OK;
+}
+
+int mlem_get_csc(mlem_ctx* c, uint64_t* col_ptr, void* elems) {
+    if (!c) return fail(nullptr, MLEM_ERR_INVALID, "null context");
+    if (!c->has_csc) return fail(c, MLEM_ERR_STATE, "context has no CSC copy");
+    TRY(set_device(c));
+    if (col_ptr) CK(c, cudaMemcpy(col_ptr, c->col_ptr, ((size_t)c->C + 1) * 8, cudaMemcpyDeviceToHost));
+    if (elems && c->Z) CK(c, cudaMemcpy(elems, c->celems, c->Z * 8, cudaMemcpyDeviceToHost));
+    return MLEM_OK;
+}
+
+// ---- the five reference functions on host buffers ---------------------------
+int mlem_calc_column_sums(mlem_ctx* c, float* norm) {
+    if (!c || !norm) return fail(c, MLEM_ERR_INVALID, "null argument");
+    std::memcpy(norm, c->norm_host.data(), (size_t)c->C * 4);
+    return MLEM_OK;
+}
+
+int mlem_init_value(mlem_ctx* c, const int32_t* sino, uint64_t len, float* initial) {
+    if (!c || !initial || (len && !sino)) return fail(c, MLEM_ERR_INVALID, "null argument");
+    double sumin = 0.0;
+    for (uint64_t i = 0; i < len; ++i) sumin += sino[i];
+    *initial = (float)(sumin / c->sumnorm);
+    return MLEM_OK;
+}
+
+int mlem_calc_fwproj(mlem_ctx* c, const float* image, float* out) {
+    if (!c || !image || !out) return fail(c, MLEM_ERR_INVALID, "null argument");
+    TRY(set_device(c));
+    TRY(ensure_tmp(c));
+    CK(c, cudaMemcpyAsync(c->tmp_c[0], image, (size_t)c->C * 4, cudaMemcpyHostToDevice, c->stream));
+    if (c->flags & MLEM_FLAG_EXACT)
+        CK(c, fwproj_exact(csr_view(c), c->tmp_c[0], 1, nullptr, nullptr, c->tmp_r[0], c->stream));
+    else
+        CK(c, fwproj(csr_view(c), c->tmp_c[0], 1, 0, nullptr, nullptr, c->tmp_r[0],
+                     cfg_for_frames(c, 1), c->stream));
+    CK(c, cudaMemcpyAsync(out, c->tmp_r[0], (size_t)c->R * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return MLEM_OK;
+}
+
+int mlem_calc_correl(mlem_ctx* c, const float* f, const int32_t* sino, uint64_t len, float* out) {
+    if (!c || !f || !sino || !out) return fail(c, MLEM_ERR_INVALID, "null argument");
+    if (len != c->R)
+        return fail(c, MLEM_ERR_INVALID, "sinogram has %llu entries, matrix has %u rows",
+                    (unsigned long long)len, c->R);
+    TRY(set_device(c));
+    TRY(ensure_tmp(c));
+    CK(c, cudaMemcpyAsync(c->tmp_r[0], f, (size_t)c->R * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemcpyAsync(c->tmp_sino, sino, (size_t)c->R * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(c, correl_elementwise(c->tmp_r[0], c->tmp_sino, c->tmp_r[1], c->R, c->stream));
+    CK(c, cudaMemcpyAsync(out, c->tmp_r[1], (size_t)c->R * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return MLEM_OK;
+}
+
+int mlem_calc_bkproj(mlem_ctx* c, const float* correl, float* update) {
+    if (!c || !correl || !update) return fail(c, MLEM_ERR_INVALID, "null argument");
+    TRY(set_device(c));
+    TRY(ensure_tmp(c));
+    CK(c, cudaMemcpyAsync(c->tmp_r[0], correl, (size_t)c->R * 4, cudaMemcpyHostToDevice, c->stream));
+    if (c->flags & MLEM_FLAG_EXACT) {
+        CK(c, bkproj_exact(csc_view(c), c->tmp_r[0], 1, nullptr, nullptr, c->tmp_c[0], c->stream));
+    } else if (c->has_csc) {
+        CK(c, bkproj_csc(csc_view(c), c->tmp_r[0], 1, 0, nullptr, nullptr, c->tmp_c[0],
+                         cfg_for_frames(c, 1), c->stream));
+    } else {
+        CK(c, cudaMemsetAsync(c->tmp_c[0], 0, (size_t)c->C * 4, c->stream));
+        CK(c, bkproj_scatter(csr_view(c), c->tmp_r[0], 1, 0, c->tmp_c[0], cfg_for_frames(c, 1),
+                             c->stream));
+    }
+    CK(c, cudaMemcpyAsync(update, c->tmp_c[0], (size_t)c->C * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return MLEM_OK;
+}
+
+int mlem_calc_update(mlem_ctx* c, const float* update, const float* norm, float* image) {
+    if (!c || !update || !norm || !image) return fail(c, MLEM_ERR_INVALID, "null argument");
+    TRY(set_device(c));
+    TRY(ensure_tmp(c));
+    const size_t nb = (size_t)c->C * 4;
+    CK(c, cudaMemcpyAsync(c->tmp_c[0], update, nb, cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemcpyAsync(c->tmp_c[1], norm, nb, cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaMemcpyAsync(c->tmp_c[2], image, nb, cudaMemcpyHostToDevice, c->stream));
+    CK(c, apply_update(c->tmp_c[2], c->tmp_c[0], c->tmp_c[1], c->C, 1, false, c->stream));
+    CK(c, cudaMemcpyAsync(image, c->tmp_c[2], nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return MLEM_OK;
+}
+
+// ---- device-resident reconstruction -----------------------------------------
+int mlem_set_sinograms(mlem_ctx* c, const int32_t* sino, uint32_t B) {
+    if (!c || !sino) return fail(c, MLEM_ERR_INVALID, "null argument");
+    TRY(set_device(c));
+    TRY(alloc_frames(c, B));
+    c->sumin.assign(B, 0.0);
+    for (uint32_t b = 0; b < B; ++b) {
+        double s = 0.0;  // seqcsr4mlem.cpp:57-58
+        const int32_t* p = sino + (size_t)b * c->R;
+        for (uint32_t i = 0; i < c->R; ++i) s += p[i];
+        c->sumin[b] = s;
+    }
+    TRY(upload_frames<int32_t>(c, sino, c->sino, c->R));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->images_ready = false;
+    return MLEM_OK;
+}
+
+int mlem_init_images(mlem_ctx* c, float* initial) {
+    if (!c) return fail(nullptr, MLEM_ERR_INVALID, "null context");
+    if (!c->B) return fail(c, MLEM_ERR_STATE, "mlem_set_sinograms must come first");
+    TRY(set_device(c));
+    std::vector<float> init(c->Bp, 0.0f);
+    for (uint32_t b = 0; b < c->B; ++b) init[b] = (float)(c->sumin[b] / c->sumnorm);
+    CK(c, cudaMemcpyAsync(c->inits_dev, init.data(), c->Bp * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(c, fill_frames(c->x, c->C, c->Bp, c->B, c->inits_dev, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    if (initial) std::memcpy(initial, init.data(), c->B * 4);
+    c->images_ready = true;
+    return MLEM_OK;
+}
+
+int mlem_set_images(mlem_ctx* c, const float* images) {
+    if (!c || !images) return fail(c, MLEM_ERR_INVALID, "null argument");
+    if (!c->B) return fail(c, MLEM_ERR_STATE, "mlem_set_sinograms must come first");
+    TRY(set_device(c));
+    TRY(upload_frames<float>(c, images, c->x, c->C));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->images_ready = true;
+    return MLEM_OK;
+}
+
+int mlem_iterate(mlem_ctx* c, int n, double* sums, uint64_t* zeros, uint64_t* subn) {
+    if (!c) return fail(nullptr, MLEM_ERR_INVALID, "null context");
+    if (n < 0) return fail(c, MLEM_ERR_INVALID, "negative iteration count");
+    if (!c->images_ready) return fail(c, MLEM_ERR_STATE, "images not initialised");
+    if (n == 0) return MLEM_OK;
+    TRY(set_device(c));
+    // Chunks of up to 64 iterations, each one graph launch.
+    const int chunk = std::min(n, 64);
+    TRY(ensure_history(c, chunk));
+    if (c->graph_dirty || !c->graph || c->graph_iters != chunk) TRY(capture(c, chunk));
+    int done = 0;
+    while (done < n) {
+        const int k = std::min(chunk, n - done);
+        if (k == chunk) {
+            CK(c, cudaGraphLaunch(c->graph, c->stream));
+        } else {
+            CK(c, cudaMemsetAsync(c->stats_slot, 0, 4, c->stream));
+            for (int i = 0; i < k; ++i) TRY(enqueue_iteration(c, c->tuning, true));
+        }
+        const size_t cnt = (size_t)k * c->B;
+        if (sums) CK(c, cudaMemcpyAsync(sums + (size_t)done * c->B, c->hist_sums, cnt * 8,
+                                        cudaMemcpyDeviceToHost, c->stream));
+        if (zeros) CK(c, cudaMemcpyAsync(zeros + (size_t)done * c->B, c->hist_zeros, cnt * 8,
+                                         cudaMemcpyDeviceToHost, c->stream));
+        if (subn) CK(c, cudaMemcpyAsync(subn + (size_t)done * c->B, c->hist_subn, cnt * 8,
+                                        cudaMemcpyDeviceToHost, c->stream));
+        if (sums || zeros || subn) CK(c, cudaStreamSynchronize(c->stream));
+        done += k;
+    }
+    CK(c, cudaStreamSynchronize(c->stream));
+    return MLEM_OK;
+}
+
+int mlem_get_images(mlem_ctx* c, float* images) {
+    if (!c || !images) return fail(c, MLEM_ERR_INVALID, "null argument");
+    if (!c->B) return fail(c, MLEM_ERR_STATE, "no frames");
+    TRY(set_device(c));
+    TRY(download_images(c, images));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return MLEM_OK;
+}
+
+int mlem_step_host(mlem_ctx* c, const int32_t* sino, float* images, uint32_t B) {
+    if (!c || !sino || !images) return fail(c, MLEM_ERR_INVALID, "null argument");
+    TRY(set_device(c));
+    if (c->B != B) TRY(alloc_frames(c, B));
+    TRY(upload_frames<int32_t>(c, sino, c->sino, c->R));
+    TRY(upload_frames<float>(c, images, c->x, c->C));
+    c->images_ready = true;
+    if (c->graph_dirty || !c->graph || c->graph_iters != 1) {
+        TRY(ensure_history(c, 1));
+        TRY(capture(c, 1));
+    }
+    CK(c, cudaGraphLaunch(c->graph, c->stream));
+    TRY(download_images(c, images));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return MLEM_OK;
+}
+
+int mlem_profile_phases(mlem_ctx* c, int n, double* ms, double* bytes, int* launches) {
+    if (!c || n <= 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
+    if (!c->images_ready) return fail(c, MLEM_ERR_STATE, "images not initialised");
+    TRY(set_device(c));
+    TRY(ensure_history(c, 1));
+    std::vector<PhaseEvents> evs((size_t)n);
+    for (auto& pe : evs)
+        for (auto& e : pe.ev) CK(c, cudaEventCreate(&e));
+    int s = MLEM_OK;
+    for (int i = 0; i < n && s == MLEM_OK; ++i) {
+        if (cudaMemsetAsync(c->stats_slot, 0, 4, c->stream) != cudaSuccess)
+            s = fail(c, MLEM_ERR_CUDA, "memset");
+        else
+            s = enqueue_iteration(c, c->tuning, true, &evs[(size_t)i]);
+    }
+    if (s == MLEM_OK && cudaStreamSynchronize(c->stream) != cudaSuccess)
+        s = fail(c, MLEM_ERR_CUDA, "synchronize");
+    double acc[MLEM_N_PHASES] = {0, 0, 0, 0};
+    for (auto& pe : evs)
+        for (int p = 0; p < MLEM_N_PHASES && s == MLEM_OK; ++p) {
+            float t = 0.0f;
+            if (cudaEventElapsedTime(&t, pe.ev[p], pe.ev[p + 1]) != cudaSuccess)
+                s = fail(c, MLEM_ERR_CUDA, "event timing");
+            acc[p] += t;
+        }
+    for (auto& pe : evs)
+        for (auto& e : pe.ev) cudaEventDestroy(e);
+    if (s != MLEM_OK) return s;
+    double b[MLEM_N_PHASES];
+    int l[MLEM_N_PHASES];
+    phase_bytes(c, b, l);
+    for (int p = 0; p < MLEM_N_PHASES; ++p) {
+        if (ms) ms[p] = acc[p] / n;
+        if (bytes) bytes[p] = b[p];
+        if (launches) launches[p] = l[p];
+    }
+    return MLEM_OK;
+}
+
+// ---- tuning -------------------------------------------------------------------
+int mlem_get_tuning(const mlem_ctx* c, mlem_tuning* out) {
+    if (!c || !out) return fail(nullptr, MLEM_ERR_INVALID, "null argument");
+    *out = c->tuning;
+    return MLEM_OK;
+}
+
+int mlem_set_tuning(mlem_ctx* c, const mlem_tuning* t) {
+    if (!c || !t) return fail(c, MLEM_ERR_INVALID, "null argument");
+    mlem_tuning n = *t;
+    if (n.bk_mode == MLEM_BK_AUTO) n.bk_mode = c->has_csc ? MLEM_BK_CSC : MLEM_BK_ATOMIC;
+    if (n.bk_mode == MLEM_BK_CSC && !c->has_csc)
+        return fail(c, MLEM_ERR_INVALID, "MLEM_BK_CSC needs the CSC copy");
+    if (n.bk_mode < MLEM_BK_CSC || n.bk_mode > MLEM_BK_FUSED)
+        return fail(c, MLEM_ERR_INVALID, "unknown back-projection mode %d", n.bk_mode);
+    LaunchCfg cfg;
+    cfg.group = n.group;
+    cfg.frame_tile = n.frame_tile;
+    cfg.blocks_per_sm = n.blocks_per_sm;
+    if (!cfg_valid(cfg))
+        return fail(c, MLEM_ERR_INVALID, "invalid launch configuration (group %d, tile %d, blocks %d)",
+                    n.group, n.frame_tile, n.blocks_per_sm);
+    if (c->Bp && (c->Bp % (uint32_t)n.frame_tile))
+        return fail(c, MLEM_ERR_INVALID, "frame tile %d does not divide the padded frame count %u",
+                    n.frame_tile, c->Bp);
+    c->tuning = n;
+    c->graph_dirty = true;
+    return MLEM_OK;
+}
+
+int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
+    if (!c) return fail(nullptr, MLEM_ERR_INVALID, "null context");
+    if (!c->B || !c->images_ready) return fail(c, MLEM_ERR_STATE, "set sinograms and images first");
+    if (c->flags & MLEM_FLAG_EXACT) {
+        if (best_out) *best_out = c->tuning;
+        return MLEM_OK;
+    }
+    TRY(set_device(c));
+    // Save the images: tuning runs real iterations.
+    float* saved = nullptr;
+    const size_t xb = (size_t)c->C * c->Bp * 4;
+    TRY(dev_alloc(c, &saved, (size_t)c->C * c->Bp));
+    CK(c, cudaMemcpyAsync(saved, c->x, xb, cudaMemcpyDeviceToDevice, c->stream));
+    std::vector<int> modes;
+    if (c->has_csc) modes.push_back(MLEM_BK_CSC);
+    if (!deterministic_only) { modes.push_back(MLEM_BK_ATOMIC); modes.push_back(MLEM_BK_FUSED); }
+    cudaEvent_t e0, e1;
+    CK(c, cudaEventCreate(&e0));
+    CK(c, cudaEventCreate(&e1));
+    mlem_tuning best = c->tuning;
+    best.ms_per_iter = 1e30;
+    const mlem_tuning orig = c->tuning;
+    for (int mode : modes)
+        for (int group : {8, 16, 32})
+            for (int tile : {1, 2, 4, 8, 16}) {
+                if (tile > group || (c->Bp % (uint32_t)tile)) continue;
+                for (int bps : {4, 8}) {
+                    mlem_tuning t{mode, group, tile, bps, 0.0};
+                    // warm-up once, then time two iterations
+                    int s = enqueue_iteration(c, t, false);
+                    if (s != MLEM_OK) { c->tuning = orig; return s; }
+                    CK(c, cudaEventRecord(e0, c->stream));
+                    for (int i = 0; i < 2; ++i) TRY(enqueue_iteration(c, t, false));
+                    CK(c, cudaEventRecord(e1, c->stream));
+                    CK(c, cudaEventSynchronize(e1));
+                    float ms = 0.0f;
+                    CK(c, cudaEventElapsedTime(&ms, e0, e1));
+                    t.ms_per_iter = ms / 2.0;
+                    if (t.ms_per_iter < best.ms_per_iter) best = t;
+                    CK(c, cudaMemcpyAsync(c->x, saved, xb, cudaMemcpyDeviceToDevice, c->stream));
+                }
+            }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    CK(c, cudaMemcpyAsync(c->x, saved, xb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(c, cudaMemsetAsync(c->update, 0, xb, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    cudaFree(saved);
+    c->device_bytes -= xb;
+    c->tuning = best;
+    c->graph_dirty = true;
+    if (best_out) *best_out = best;
+    return MLEM_OK;
+}
+
+// ---- device-pointer entry points ---------------------------------------------
+int mlem_fwproj_d(mlem_ctx* c, const float* x, float* y, uint32_t B, void* stream) {
+    if (!c || !x || !y || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
+    TRY(set_device(c));
+    const LaunchCfg cfg = cfg_for_frames(c, B);
+    for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
+        CK(c, fwproj(csr_view(c), x, B, f0, nullptr, nullptr, y, cfg, (cudaStream_t)stream));
+    return MLEM_OK;
+}
+
+int mlem_bkproj_d(mlem_ctx* c, const float* y, float* x, uint32_t B, void* stream) {
+    if (!c || !x || !y || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
+    TRY(set_device(c));
+    const LaunchCfg cfg = cfg_for_frames(c, B);
+    cudaStream_t st = (cudaStream_t)stream;
+    for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile) {
+        if (c->has_csc) {
+            CK(c, bkproj_csc(csc_view(c), y, B, f0, nullptr, nullptr, x, cfg, st));
+        } else {
+            if (f0 == 0) CK(c, cudaMemsetAsync(x, 0, (size_t)c->C * B * 4, st));
+            CK(c, bkproj_scatter(csr_view(c), y, B, f0, x, cfg, st));
+        }
+    }
+    return MLEM_OK;
+}
+
+int mlem_fwproj_correl_d(mlem_ctx* c, const float* x, const int32_t* sino, float* correl,
+                         uint32_t B, void* stream) {
+    if (!c || !x || !sino || !correl || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
+    TRY(set_device(c));
+    const LaunchCfg cfg = cfg_for_frames(c, B);
+    for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
+        CK(c, fwproj(csr_view(c), x, B, f0, sino, correl, nullptr, cfg, (cudaStream_t)stream));
+    return MLEM_OK;
+}
+
+int mlem_bkproj_update_d(mlem_ctx* c, const float* correl, float* x, uint32_t B, void* stream) {
+    if (!c || !x || !correl || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
+    if (!c->has_csc) return fail(c, MLEM_ERR_STATE, "fused back projection needs the CSC copy");
+    TRY(set_device(c));
+    const LaunchCfg cfg = cfg_for_frames(c, B);
+    for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
+        CK(c, bkproj_csc(csc_view(c), correl, B, f0, c->norm, x, nullptr, cfg, (cudaStream_t)stream));
+    return MLEM_OK;
+}
+
+int mlem_apply_update_d(mlem_ctx* c, const float* update, float* x, uint32_t B, void* stream) {
+    if (!c || !x || !update || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
+    TRY(set_device(c));
+    CK(c, apply_update(x, const_cast<float*>(update), c->norm, c->C, B, false, (cudaStream_t)stream));
+    return MLEM_OK;
+}
+
+int mlem_norm_d(mlem_ctx* c, const float** norm) {
+    if (!c || !norm) return fail(c, MLEM_ERR_INVALID, "null argument");
+    *norm = c->norm;
+    return MLEM_OK;
+}
+
+int mlem_set_norm_d(mlem_ctx* c, const float* norm, void* stream) {
+    if (!c || !norm) return fail(c, MLEM_ERR_INVALID, "null argument");
+    TRY(set_device(c));
+    cudaStream_t st = (cudaStream_t)stream;
+    CK(c, cudaMemcpyAsync(c->norm, norm, (size_t)c->C * 4, cudaMemcpyDeviceToDevice, st));
+    CK(c, cudaMemcpyAsync(c->norm_host.data(), norm, (size_t)c->C * 4, cudaMemcpyDeviceToHost, st));
+    CK(c, cudaStreamSynchronize(st));
+    double s = 0.0;
+    for (uint32_t i = 0; i < c->C; ++i) s += c->norm_host[i];
+    c->sumnorm = s;
+    return MLEM_OK;
+}
+
+int mlem_project_f64(mlem_ctx* c, const float* x, double* out) {
+    if (!c || !x || !out) return fail(c, MLEM_ERR_INVALID, "null argument");
+    TRY(set_device(c));
+    TRY(ensure_tmp(c));
+    if (!c->tmp_d) TRY(dev_alloc(c, &c->tmp_d, std::max<uint32_t>(c->R, 1)));
+    CK(c, cudaMemcpyAsync(c->tmp_c[0], x, (size_t)c->C * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(c, project_f64(csr_view(c), c->tmp_c[0], c->tmp_d, c->stream));
+    CK(c, cudaMemcpyAsync(out, c->tmp_d, (size_t)c->R * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    return MLEM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,129 @@
+// kernels.h -- host-side launchers of the sm_100a MLEM kernels.
+//
+// Device layouts (all in HBM, 256-byte aligned by cudaMalloc):
+//   CSR  : ptr u64[R+1] (leading 0, then the CSR4 row END offsets),
+//          elements {u32 column, f32 value} x Z, padded to an even count so
+//          that they can be read as 16-byte pairs.
+//   CSC  : ptr u64[C+1], elements {u32 row, f32 value} x Z (same padding),
+//          rows ascending inside a column (stable transpose of CSR order).
+//   frame-interleaved vectors for B frames: image x[C][B], sinogram s[R][B],
+//   correlation c[R][B], update u[C][B]; norm[C] is shared by all frames.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace mlem {
+
+struct SparseView {
+    const uint64_t* ptr;  // n+1 offsets
+    const uint4* pairs;   // elements as 16-byte pairs
+    uint32_t n;           // rows (CSR) or columns (CSC)
+    uint64_t nnz;
+};
+
+// Per-matrix launch configuration (chosen by the autotuner).
+struct LaunchCfg {
+    int group = 32;       // lanes cooperating on one row / column: 4, 8, 16 or 32
+    int frame_tile = 1;   // frames per pass over the matrix: 1, 2, 4, 8 or 16
+    int blocks_per_sm = 8;
+    int sm_count = 148;
+};
+
+// Valid (group, frame_tile) pairs: frame_tile <= group.
+bool cfg_valid(const LaunchCfg& c);
+
+// ---- forward projection -------------------------------------------------
+// y[r][f] = sum_k v_k x[col_k][f] for frames f in [f0, f0+BT); when sino is
+// non-null also c[r][f] = calcCorrel(sino, y).  y and/or c may be null.
+cudaError_t fwproj(const SparseView& csr, const float* x, uint32_t B, uint32_t f0,
+                   const int32_t* sino, float* c, float* y, const LaunchCfg& cfg,
+                   cudaStream_t st);
+
+// ---- back projection over the CSC copy ----------------------------------
+// u[col][f] = sum_k v_k c[row_k][f]; with norm non-null, instead
+// x[col][f] *= calcUpdate factor(u, norm[col]) (u not stored).
+cudaError_t bkproj_csc(const SparseView& csc, const float* c, uint32_t B, uint32_t f0,
+                       const float* norm, float* x, float* u, const LaunchCfg& cfg,
+                       cudaStream_t st);
+
+// ---- back projection by atomic scatter over the CSR ---------------------
+// u[col][f] += v_k c[r][f] (u must be zeroed before the first call).
+cudaError_t bkproj_scatter(const SparseView& csr, const float* c, uint32_t B, uint32_t f0,
+                           float* u, const LaunchCfg& cfg, cudaStream_t st);
+
+// ---- one pass per row: forward projection, correlation, scatter ---------
+cudaError_t fused_row(const SparseView& csr, const float* x, uint32_t B, uint32_t f0,
+                      const int32_t* sino, float* u, const LaunchCfg& cfg, cudaStream_t st);
+
+// x[i] *= factor(u[i], norm[i/B]); u[i] = 0 when zero_u.
+cudaError_t apply_update(float* x, float* u, const float* norm, uint32_t C, uint32_t B,
+                         bool zero_u, cudaStream_t st);
+
+// ---- bit-exact kernels: the float operation order of seqcsr4mlem --------
+cudaError_t fwproj_exact(const SparseView& csr, const float* x, uint32_t B, const int32_t* sino,
+                         float* c, float* y, cudaStream_t st);
+cudaError_t bkproj_exact(const SparseView& csc, const float* c, uint32_t B, const float* norm,
+                         float* x, float* u, cudaStream_t st);
+cudaError_t column_sums_exact(const SparseView& csc, float* norm, cudaStream_t st);
+cudaError_t column_sums_atomic(const SparseView& csr, uint32_t C, float* norm, cudaStream_t st);
+
+// ---- per-frame image statistics (sum in double, zeros, subnormals) -----
+// Deterministic: fixed-order block tree.  `partial` needs stats_scratch_bytes.
+// B is the interleave stride; the first n_out frames are written.  When
+// `slot` is non-null, results go to row *slot of [n][n_out] outputs and the
+// kernel then increments *slot (so one captured graph serves every
+// iteration).
+size_t stats_scratch_bytes(uint32_t B);
+cudaError_t image_stats(const float* x, uint32_t C, uint32_t B, uint32_t n_out, void* partial,
+                        unsigned int* slot, double* sums, unsigned long long* zeros,
+                        unsigned long long* subnormals, cudaStream_t st);
+
+// ---- layout helpers -------------------------------------------------------
+// out[i*Bp + b] = in[b*n + i] for b < B (n items per frame; pad frames
+// untouched), and back: out[b*n + i] = in[i*Bp + b].
+cudaError_t interleave_i32(const int32_t* in, int32_t* out, uint64_t n, uint32_t B, uint32_t Bp,
+                           cudaStream_t st);
+cudaError_t interleave_f32(const float* in, float* out, uint64_t n, uint32_t B, uint32_t Bp,
+                           cudaStream_t st);
+cudaError_t deinterleave_f32(const float* in, float* out, uint64_t n, uint32_t B, uint32_t Bp,
+                             cudaStream_t st);
+cudaError_t fill_f32(float* p, float v, uint64_t n, cudaStream_t st);
+// x[i][b] = b < B ? vals[b] : 0 for the Bp-interleaved image (vals: device, B floats).
+cudaError_t fill_frames(float* x, uint64_t n, uint32_t Bp, uint32_t B, const float* vals,
+                        cudaStream_t st);
+// c[i] = calcCorrel(s[i], f[i]).
+cudaError_t correl_elementwise(const float* f, const int32_t* s, float* c, uint64_t n,
+                               cudaStream_t st);
+
+// ---- prefix sums ----------------------------------------------------------
+// out[0] = 0, out[i+1] = in[0] + ... + in[i]  (n+1 outputs).
+size_t scan_scratch_bytes(uint64_t n);
+cudaError_t exclusive_scan_u64(const uint64_t* in, uint64_t* out, uint64_t n, void* scratch,
+                               cudaStream_t st);
+
+// ---- deterministic CSR -> CSC transpose -----------------------------------
+// col_ptr: C+1 entries; celems: Z (+ padding) 8-byte elements.  scratch is
+// transpose_scratch_bytes(C) bytes.  Result is identical to a stable
+// counting-sort transpose (ascending row, then in-row position).
+size_t transpose_scratch_bytes(uint32_t C);
+cudaError_t transpose(const SparseView& csr, uint32_t C, uint64_t* col_ptr, uint2* celems,
+                      void* scratch, uint32_t* max_col_len, cudaStream_t st);
+
+// ---- matrix validation: every column < C and offsets non-decreasing ------
+cudaError_t validate_csr(const SparseView& csr, uint32_t C, unsigned int* bad_flag,
+                         cudaStream_t st);
+
+// ---- synthetic Siddon generator on the device -----------------------------
+struct SiddonSpec {
+    uint32_t nx, ny, nz, n_rows, min_count, max_count;
+    double radius_scale, min_len;
+    uint64_t seed;
+};
+cudaError_t siddon_counts(const SiddonSpec& s, uint64_t* counts, cudaStream_t st);
+cudaError_t siddon_fill(const SiddonSpec& s, const uint64_t* row_ptr, uint2* elems,
+                        cudaStream_t st);
+// out[r] = sequential double sum of v_k * x[col_k] (bit-identical to the host).
+cudaError_t project_f64(const SparseView& csr, const float* x, double* out, cudaStream_t st);
+
+}  // namespace mlem

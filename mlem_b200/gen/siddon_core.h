@@ -106,11 +106,19 @@ SD_FN void sd_endpoint(const siddon_geom* g, uint64_t key, double* p) {
 }
 
 /*
- * Trace one LOR (p0 -> p1).  When cols/vals are non-null the elements are
- * written there (capacity nx+ny+nz+4).  Returns the number of elements.
+ * Trace one LOR (p0 -> p1).  When `out` is non-null the elements are written
+ * there as interleaved 32-bit words {voxel index, float32 length bits}, the
+ * CSR4 element layout (capacity nx+ny+nz+4 elements).  Returns the number of
+ * elements.
  */
+SD_FN uint32_t sd_f32_bits(float f) {
+    union { float f; uint32_t u; } cv;
+    cv.f = f;
+    return cv.u;
+}
+
 SD_FN uint32_t sd_trace(const siddon_geom* g, const double* p0, const double* p1,
-                        uint32_t* cols, float* vals) {
+                        uint32_t* out) {
     const double n[3] = {(double)g->nx, (double)g->ny, (double)g->nz};
     double d[3];
     double amin = 0.0, amax = 1.0;
@@ -159,10 +167,10 @@ SD_FN uint32_t sd_trace(const siddon_geom* g, const double* p0, const double* p1
         if (an >= amax) { an = amax; last = 1; }
         double len = SD_MUL(SD_SUB(an, cur), L);
         if (len >= g->min_len) {
-            if (cols) {
-                cols[count] = (uint32_t)idx[0] +
-                              g->nx * ((uint32_t)idx[1] + g->ny * (uint32_t)idx[2]);
-                vals[count] = (float)len;
+            if (out) {
+                out[2 * count] = (uint32_t)idx[0] +
+                                 g->nx * ((uint32_t)idx[1] + g->ny * (uint32_t)idx[2]);
+                out[2 * count + 1] = sd_f32_bits((float)len);
             }
             ++count;
         }
@@ -178,14 +186,14 @@ SD_FN uint32_t sd_trace(const siddon_geom* g, const double* p0, const double* p1
 }
 
 /* Row generator: draws LORs for `row` until one has an accepted element
- * count, then traces it once more into cols/vals (when non-null). */
-SD_FN uint32_t sd_row(const siddon_geom* g, uint32_t row, uint32_t* cols, float* vals) {
+ * count, then traces it once more into `out` (when non-null). */
+SD_FN uint32_t sd_row(const siddon_geom* g, uint32_t row, uint32_t* out) {
     int32_t keep = -1;
     for (uint32_t a = 0; a < SIDDON_MAX_ATTEMPTS; ++a) {
         double p0[3], p1[3];
         sd_endpoint(g, sd_stream(g->seed, row, a, 0), p0);
         sd_endpoint(g, sd_stream(g->seed, row, a, 1), p1);
-        uint32_t c = sd_trace(g, p0, p1, 0, 0);
+        uint32_t c = sd_trace(g, p0, p1, 0);
         if (c > 0) keep = (int32_t)a;
         if (c > 0 && c >= g->min_count && c <= g->max_count) break;
     }
@@ -193,8 +201,7 @@ SD_FN uint32_t sd_row(const siddon_geom* g, uint32_t row, uint32_t* cols, float*
     double p0[3], p1[3];
     sd_endpoint(g, sd_stream(g->seed, row, (uint32_t)keep, 0), p0);
     sd_endpoint(g, sd_stream(g->seed, row, (uint32_t)keep, 1), p1);
-    if (!cols) return sd_trace(g, p0, p1, 0, 0);
-    return sd_trace(g, p0, p1, cols, vals);
+    return sd_trace(g, p0, p1, out);
 }
 
 SD_FN uint32_t sd_row_capacity(const siddon_geom* g) { return g->nx + g->ny + g->nz + 4; }

@@ -34,7 +34,7 @@ GEN_API uint64_t mlem_gen_siddon_counts(uint32_t nx, uint32_t ny, uint32_t nz, u
     uint64_t total = 0;
 #pragma omp parallel for schedule(dynamic, 1024) reduction(+ : total)
     for (int64_t r = 0; r < (int64_t)R; ++r) {
-        counts[r] = sd_row(&g, (uint32_t)r, 0, 0);
+        counts[r] = sd_row(&g, (uint32_t)r, 0);
         total += counts[r];
     }
     return total;
@@ -47,27 +47,14 @@ GEN_API int mlem_gen_siddon_fill(uint32_t nx, uint32_t ny, uint32_t nz, uint32_t
                                  double radius_scale, double min_len, uint64_t seed,
                                  const uint64_t* row_end, void* elems) {
     siddon_geom g = make_geom(nx, ny, nz, min_count, max_count, radius_scale, min_len, seed);
-    uint32_t cap = sd_row_capacity(&g);
     int bad = 0;
-#pragma omp parallel reduction(| : bad)
-    {
-        uint32_t* cols = (uint32_t*)malloc(cap * sizeof(uint32_t));
-        float* vals = (float*)malloc(cap * sizeof(float));
-#pragma omp for schedule(dynamic, 1024)
-        for (int64_t r = 0; r < (int64_t)R; ++r) {
-            uint64_t begin = r == 0 ? 0 : row_end[r - 1];
-            uint32_t c = sd_row(&g, (uint32_t)r, cols, vals);
-            if (begin + c != row_end[r]) { bad = 1; continue; }
-            uint32_t* out = (uint32_t*)elems + 2 * begin;
-            for (uint32_t k = 0; k < c; ++k) {
-                out[2 * k] = cols[k];
-                union { float f; uint32_t u; } cv;
-                cv.f = vals[k];
-                out[2 * k + 1] = cv.u;
-            }
-        }
-        free(cols);
-        free(vals);
+#pragma omp parallel for schedule(dynamic, 1024) reduction(| : bad)
+    for (int64_t r = 0; r < (int64_t)R; ++r) {
+        uint64_t begin = r == 0 ? 0 : row_end[r - 1];
+        uint32_t expect = (uint32_t)(row_end[r] - begin);
+        /* count first: never write past the slot the counts pass reserved */
+        if (sd_row(&g, (uint32_t)r, 0) != expect) { bad = 1; continue; }
+        sd_row(&g, (uint32_t)r, (uint32_t*)elems + 2 * begin);
     }
     return bad ? -1 : 0;
 }

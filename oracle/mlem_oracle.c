@@ -237,5 +237,7 @@ void oracle_partition(uint32_t R, const uint64_t* row_end, int n_ranks,
             starts[idx] = r + 1;
         }
     }
-    ends[n_ranks - 1] = R;
+    /* ranks the threshold never reached get empty ranges at the end */
+    for (int i = idx + 1; i < n_ranks; ++i) starts[i] = R;
+    for (int i = idx; i < n_ranks; ++i) ends[i] = R;
 }

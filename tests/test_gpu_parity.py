@@ -1,0 +1,228 @@
+"""GPU parity: the CUDA path through the C ABI against the oracle and the
+golden images of the reference binary.
+
+Tolerances: bit-exact for index work (CSC transpose, generator, column sums,
+MLEM_FLAG_EXACT runs); relative L2 <= 1e-4 for the fast float kernels after
+the full iteration count (the tolerance the hot path is held to); 1e-5 for
+a single projection.
+"""
+import numpy as np
+import pytest
+
+from mlem_b200 import api, formats, synth
+
+import oracle_bind as ob
+from golden_cases import CASES
+
+pytestmark = pytest.mark.gpu
+
+TOL_MLEM = 1e-4
+TOL_PROJ = 1e-5
+
+
+@pytest.fixture(scope="module")
+def ctxs(golden):
+    out = {}
+    for name in CASES:
+        m, sino, iters, gold, entry = golden.case(name)
+        out[name] = (api.Context.from_matrix(m), m, sino, iters, gold)
+    yield out
+    for v in out.values():
+        v[0].close()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_csc_transpose_bit_exact(ctxs, name):
+    ctx, m, *_ = ctxs[name]
+    col_ptr, ce = ctx.csc()
+    cp_o, ce_o = ob.transpose(m)
+    assert np.array_equal(col_ptr, cp_o)
+    assert ce.tobytes() == ce_o.tobytes()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_csr_roundtrip(ctxs, name):
+    ctx, m, *_ = ctxs[name]
+    row_end, el = ctx.csr()
+    assert np.array_equal(row_end, m.row_end)
+    assert el.tobytes() == np.ascontiguousarray(m.elems).tobytes()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_column_sums_bit_exact(ctxs, name):
+    ctx, m, *_ = ctxs[name]
+    assert ctx.column_sums().tobytes() == ob.column_sums(m).tobytes()
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_pieces_against_oracle(ctxs, name):
+    ctx, m, sino, *_ = ctxs[name]
+    rng = np.random.default_rng(3)
+    x = rng.uniform(0.5, 2.0, m.n_cols).astype(np.float32)
+    f, f_o = ctx.fwproj(x), ob.fwproj(m, x)
+    assert ob.rel_l2(f, f_o) < TOL_PROJ
+    c, c_o = ctx.correl(f_o, sino), ob.correl(f_o, sino)
+    assert c.tobytes() == c_o.tobytes()  # elementwise IEEE divide: bit-exact
+    u, u_o = ctx.bkproj(c_o), ob.bkproj(m, c_o)
+    assert ob.rel_l2(u, u_o) < TOL_PROJ
+    norm = ob.column_sums(m)
+    xu, xu_o = ctx.update(u_o, norm, x), ob.update(u_o, norm, x)
+    assert xu.tobytes() == xu_o.tobytes()
+    assert ctx.init_value(sino) == ob.init_value(norm, sino)
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("mode", [api.BK_CSC, api.BK_ATOMIC, api.BK_FUSED])
+def test_mlem_matches_reference_image(ctxs, name, mode):
+    ctx, m, sino, iters, gold = ctxs[name]
+    ctx.set_sinograms(sino)
+    ctx.set_tuning(bk_mode=mode, group=32, frame_tile=1, blocks_per_sm=8)
+    ctx.init_images()
+    sums, zeros, _ = ctx.iterate(iters)
+    img = ctx.get_images()[0]
+    err_ref = ob.rel_l2(img, gold)
+    assert err_ref <= TOL_MLEM, err_ref
+    ref64 = ob.mlem_f64(m, sino, iters)
+    assert ob.rel_l2(img, ref64) <= TOL_MLEM
+    assert abs(sums[-1, 0] - float(np.sum(img, dtype=np.float64))) <= 1e-9 * abs(sums[-1, 0]) + 1e-30
+    assert zeros[-1, 0] == int((img == 0).sum())
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_exact_mode_is_bit_exact_with_reference_binary(golden, name):
+    m, sino, iters, gold, _ = golden.case(name)
+    with api.Context.from_matrix(m, flags=api.FLAG_EXACT) as ctx:
+        img, _ = api.mlem(ctx, sino, nIterations=iters)
+        assert img[0].tobytes() == gold.tobytes()
+        # the piecewise functions are bit-exact too
+        x = np.full(m.n_cols, 1.5, np.float32)
+        assert ctx.fwproj(x).tobytes() == ob.fwproj(m, x).tobytes()
+        c = ob.correl(ob.fwproj(m, x), sino)
+        assert ctx.bkproj(c).tobytes() == ob.bkproj(m, c).tobytes()
+
+
+def test_csc_mode_is_deterministic(ctxs):
+    ctx, m, sino, iters, gold = ctxs["plain_small_it10"]
+    ctx.set_sinograms(sino)
+    ctx.set_tuning(bk_mode=api.BK_CSC, group=16, frame_tile=1, blocks_per_sm=4)
+    ctx.init_images()
+    ctx.iterate(iters)
+    a = ctx.get_images()
+    ctx.init_images()
+    for _ in range(iters):
+        ctx.iterate(1)
+    b = ctx.get_images()
+    assert a.tobytes() == b.tobytes()
+
+
+@pytest.mark.parametrize("group,tile", [(8, 1), (16, 4), (32, 8), (32, 16), (16, 16)])
+@pytest.mark.parametrize("mode", [api.BK_CSC, api.BK_ATOMIC, api.BK_FUSED])
+def test_batched_frames_match_separate_runs(golden, group, tile, mode):
+    m, sino, iters, gold, _ = golden.case("tiny_it10")
+    rng = np.random.default_rng(group * 100 + tile)
+    B = 16
+    sinos = np.stack([rng.permutation(sino) if b else sino for b in range(B)]).astype(np.int32)
+    with api.Context.from_matrix(m) as ctx:
+        ctx.set_sinograms(sinos)
+        ctx.set_tuning(bk_mode=mode, group=group, frame_tile=tile, blocks_per_sm=8)
+        ctx.init_images()
+        ctx.iterate(iters)
+        imgs = ctx.get_images()
+    for b in range(B):
+        want, _ = ob.mlem(m, sinos[b], iters)
+        assert ob.rel_l2(imgs[b], want) <= TOL_MLEM, b
+
+
+@pytest.mark.parametrize("B", [3, 5, 12])
+def test_odd_frame_counts(golden, B):
+    m, sino, iters, gold, _ = golden.case("edge_it7")
+    sinos = np.stack([np.roll(sino, b) for b in range(B)]).astype(np.int32)
+    with api.Context.from_matrix(m) as ctx:
+        imgs, sums = api.mlem(ctx, sinos, nIterations=iters)
+        assert sums.shape == (iters, B)
+    for b in range(B):
+        want, _ = ob.mlem(m, sinos[b], iters)
+        assert ob.rel_l2(imgs[b], want) <= TOL_MLEM
+
+
+def test_step_host_matches_iterate(ctxs):
+    ctx, m, sino, iters, gold = ctxs["tiny_it10"]
+    ctx.set_sinograms(sino)
+    ctx.set_tuning(bk_mode=api.BK_CSC, group=32, frame_tile=1, blocks_per_sm=8)
+    init = ctx.init_images()
+    x = np.full((1, m.n_cols), init[0], np.float32)
+    for _ in range(iters):
+        ctx.step_host(sino, x)
+    ctx.init_images()
+    ctx.iterate(iters)
+    assert x.tobytes() == ctx.get_images().tobytes()
+
+
+def test_device_generator_matches_host_generator():
+    g = synth.Geometry(32, 32, 16, 20000, 20, 80, seed=9)
+    hm = synth.host_matrix(g)
+    with api.Context.siddon(g) as ctx:
+        row_end, el = ctx.csr()
+        assert np.array_equal(row_end, hm.row_end)
+        assert el.tobytes() == hm.elems.tobytes()
+        x = synth.phantom(32, 32, 16, 4, 2)
+        assert np.array_equal(ctx.project_f64(x), synth.project_f64(hm, x))
+
+
+def test_skewed_matrix_long_rows_and_columns():
+    """A 12k-element row and columns longer than the shared-memory sort."""
+    rng = np.random.default_rng(7)
+    R, C = 3000, 512
+    rows = [rng.integers(0, C, size=int(rng.integers(0, 30))) for _ in range(R)]
+    rows[5] = rng.integers(0, C, size=12000)
+    rows[6] = np.full(5000, 3)            # one column of > 4096 entries, duplicates in one row
+    rows[2000] = np.full(9000, 100)
+    counts = np.array([len(r) for r in rows], np.uint64)
+    row_end = np.cumsum(counts, dtype=np.uint64)
+    el = np.zeros(int(row_end[-1]), api.ELEM_DTYPE)
+    el["index"] = np.concatenate(rows).astype(np.uint32)
+    el["value"] = rng.uniform(0.1, 1.7, el.size).astype(np.float32)
+    m = formats.Csr4(R, C, row_end, el)
+    sino = rng.poisson(50, R).astype(np.int32)
+    with api.Context.from_matrix(m) as ctx:
+        cp, ce = ctx.csc()
+        cp_o, ce_o = ob.transpose(m)
+        assert np.array_equal(cp, cp_o) and ce.tobytes() == ce_o.tobytes()
+        assert ctx.column_sums().tobytes() == ob.column_sums(m).tobytes()
+        for mode in (api.BK_CSC, api.BK_ATOMIC, api.BK_FUSED):
+            ctx.set_sinograms(sino)
+            ctx.set_tuning(bk_mode=mode, group=32, frame_tile=1, blocks_per_sm=8)
+            ctx.init_images()
+            ctx.iterate(5)
+            want, _ = ob.mlem(m, sino, 5)
+            assert ob.rel_l2(ctx.get_images()[0], want) <= TOL_MLEM
+
+
+def test_invalid_inputs_raise():
+    re_ = np.array([2, 3], np.uint64)
+    el = np.zeros(3, api.ELEM_DTYPE)
+    el["index"] = [0, 5, 1]  # column 5 >= C = 2
+    with pytest.raises(api.MlemError) as e:
+        api.Context(re_, el, 2, 2)
+    assert e.value.status == api.MLEM_ERR_MATRIX
+    el["index"] = [0, 1, 1]
+    with api.Context(re_, el, 2, 2) as ctx:
+        with pytest.raises(api.MlemError):
+            ctx.set_sinograms(np.ones(3, np.int32))  # wrong length
+        with pytest.raises(api.MlemError) as e:
+            ctx.iterate(1)
+        assert e.value.status == api.MLEM_ERR_STATE
+        with pytest.raises(api.MlemError):
+            ctx.set_tuning(bk_mode=api.BK_CSC, group=4, frame_tile=8)
+
+
+def test_autotune_restores_images(ctxs):
+    ctx, m, sino, iters, gold = ctxs["plain_small_it10"]
+    ctx.set_sinograms(np.stack([sino, sino]))
+    ctx.init_images()
+    before = ctx.get_images()
+    best = ctx.autotune()
+    assert best["ms_per_iter"] > 0
+    assert ctx.get_images().tobytes() == before.tobytes()
+    ctx.iterate(iters)
+    assert ob.rel_l2(ctx.get_images()[0], gold) <= TOL_MLEM
