@@ -127,6 +127,7 @@ class Context:
         info = sig.MlemInfo()
         _raise(core_lib().mlem_get_info(self._h, ctypes.byref(info)), self._h)
         self.n_rows, self.n_cols, self.nnz = info.n_rows, info.n_cols, info.nnz
+        self.n_frames = info.n_frames
         self.info = info
 
     def close(self):

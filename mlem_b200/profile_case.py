@@ -1,0 +1,50 @@
+"""Run a synthetic MLEM workload for a few iterations with a fixed kernel
+configuration -- the command the committed ncu summaries were captured with.
+
+    python -m mlem_b200.profile_case --grid 128 128 64 --rows 1048576 \\
+        --count 150 250 --mode fused --frames 1 --iters 3
+
+Prints one JSON line with the per-phase device times of the last iteration.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+
+from . import api, synth
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--grid", type=int, nargs=3, default=[128, 128, 64])
+    ap.add_argument("--rows", type=int, default=1 << 20)
+    ap.add_argument("--count", type=int, nargs=2, default=[150, 250])
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--mode", choices=["csc", "atomic", "fused", "exact"], default="csc")
+    ap.add_argument("--group", type=int, default=32)
+    ap.add_argument("--frame-tile", type=int, default=1)
+    ap.add_argument("--blocks-per-sm", type=int, default=8)
+    ap.add_argument("--frames", type=int, default=1)
+    ap.add_argument("--iters", type=int, default=3)
+    a = ap.parse_args(argv)
+    nx, ny, nz = a.grid
+    g = synth.Geometry(nx, ny, nz, a.rows, a.count[0], a.count[1], seed=a.seed)
+    flags = api.FLAG_EXACT if a.mode == "exact" else 0
+    with api.Context.siddon(g, flags=flags) as ctx:
+        w = synth.Workload("profile", g, a.frames, a.iters, 0, (3, 12), (1e6, 1e9), 9000)
+        fr = synth.make_frames(w, ctx.project_f64)
+        ctx.set_sinograms(fr.sinograms)
+        if a.mode != "exact":
+            mode = {"csc": api.BK_CSC, "atomic": api.BK_ATOMIC, "fused": api.BK_FUSED}[a.mode]
+            ctx.set_tuning(bk_mode=mode, group=a.group, frame_tile=a.frame_tile,
+                           blocks_per_sm=a.blocks_per_sm)
+        ctx.init_images()
+        ms, by, ln = ctx.profile_phases(a.iters)
+        print(json.dumps({"nnz": int(ctx.nnz), "mode": a.mode, "frames": a.frames,
+                          "phase_ms": [round(float(x), 4) for x in ms],
+                          "phase_GBps": [round(float(b / (t / 1e3) / 1e9), 1) if t > 0 else 0
+                                         for b, t in zip(by, ms)]}))
+
+
+if __name__ == "__main__":
+    main()

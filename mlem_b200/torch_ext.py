@@ -1,0 +1,155 @@
+"""Differentiable MLEM for PyTorch over the same C ABI.
+
+* `forward_project(x, ctx)`: y = A x as a torch.autograd.Function whose
+  backward is the hand-written back-projection kernel (A^T g), and
+  `back_project(y, ctx)` the converse.  x is float32 [C] or [B, C] on the
+  context's GPU; work runs on torch's current stream.
+* `unrolled_mlem(x0, omega, sino, ctx)`: K relaxed MLEM iterations
+      x_{k+1} = x_k * r_k ** omega_k,  r_k = calcUpdate factor(A^T (s / A x_k), norm)
+  (omega_k = 1 is the reference iteration, mlem_seq/seqcsr4mlem.cpp:163-167)
+  with gradients with respect to x0 and omega.  The backward pass keeps
+  only the K images x_k (per-iteration checkpoints) and recomputes A x_k and
+  A^T(s / A x_k) from them, then propagates the adjoint with one forward and
+  one back projection per iteration.
+
+Zero rules follow the reference: the correlation is 0 where the projection
+is 0 (calcCorrel), the update factor is the raw back projection where the
+column sum is 0 (calcUpdate); where r_k == 0 the image entry is 0 and its
+gradient with respect to omega_k is taken as 0.
+"""
+from __future__ import annotations
+
+import torch
+
+from . import api
+
+
+def _check(x: torch.Tensor, n: int, what: str) -> torch.Tensor:
+    if not x.is_cuda or x.dtype != torch.float32:
+        raise api.MlemError(api.MLEM_ERR_INVALID, f"{what} must be a float32 CUDA tensor")
+    if x.shape[-1] != n:
+        raise api.MlemError(api.MLEM_ERR_INVALID, f"{what} has {x.shape[-1]} entries, expected {n}")
+    return x
+
+
+def _frames(x: torch.Tensor):
+    """[C] -> ([C, 1], 1); [B, C] -> ([C, B] interleaved, B)."""
+    if x.dim() == 1:
+        return x.contiguous().view(-1, 1), 1
+    return x.t().contiguous(), x.shape[0]
+
+
+def _unframes(y: torch.Tensor, B: int, batched: bool):
+    return y.view(-1) if not batched else y.t().contiguous()
+
+
+def _stream():
+    return torch.cuda.current_stream().cuda_stream
+
+
+def _fw(ctx: "api.Context", x: torch.Tensor) -> torch.Tensor:
+    xi, B = _frames(_check(x, ctx.n_cols, "image"))
+    y = torch.empty((ctx.n_rows, B), dtype=torch.float32, device=x.device)
+    ctx.fwproj_d(xi.data_ptr(), y.data_ptr(), B, _stream())
+    return _unframes(y, B, x.dim() > 1)
+
+
+def _bk(ctx: "api.Context", y: torch.Tensor) -> torch.Tensor:
+    yi, B = _frames(_check(y, ctx.n_rows, "projection"))
+    x = torch.empty((ctx.n_cols, B), dtype=torch.float32, device=y.device)
+    ctx.bkproj_d(yi.data_ptr(), x.data_ptr(), B, _stream())
+    return _unframes(x, B, y.dim() > 1)
+
+
+class _ForwardProject(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, x, ctx):
+        fctx.mctx = ctx
+        return _fw(ctx, x)
+
+    @staticmethod
+    def backward(fctx, g):
+        return _bk(fctx.mctx, g.contiguous()), None
+
+
+class _BackProject(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, y, ctx):
+        fctx.mctx = ctx
+        return _bk(ctx, y)
+
+    @staticmethod
+    def backward(fctx, g):
+        return _fw(fctx.mctx, g.contiguous()), None
+
+
+def forward_project(x: torch.Tensor, ctx: "api.Context") -> torch.Tensor:
+    return _ForwardProject.apply(x, ctx)
+
+
+def back_project(y: torch.Tensor, ctx: "api.Context") -> torch.Tensor:
+    return _BackProject.apply(y, ctx)
+
+
+def norm_tensor(ctx: "api.Context", device) -> torch.Tensor:
+    return torch.from_numpy(ctx.column_sums()).to(device)
+
+
+def _ratio(ctx, x, sino_f, norm):
+    """(f, u, r): f = A x, u = A^T (s / f), r = calcUpdate factor(u, norm)."""
+    f = _fw(ctx, x)
+    c = torch.where(f != 0, sino_f / torch.where(f != 0, f, torch.ones_like(f)), torch.zeros_like(f))
+    u = _bk(ctx, c)
+    r = torch.where(norm != 0, u / torch.where(norm != 0, norm, torch.ones_like(norm)), u)
+    return f, u, r
+
+
+class _UnrolledMLEM(torch.autograd.Function):
+    @staticmethod
+    def forward(fctx, x0, omega, sino_f, norm, ctx):
+        K = omega.shape[0]
+        xs = [x0.detach()]
+        x = x0.detach()
+        for k in range(K):
+            _, _, r = _ratio(ctx, x, sino_f, norm)
+            x = x * torch.where(r > 0, r.clamp_min(1e-38) ** omega[k], torch.zeros_like(r))
+            xs.append(x)
+        fctx.mctx = ctx
+        fctx.save_for_backward(torch.stack(xs[:-1]), omega, sino_f, norm, x)
+        return x
+
+    @staticmethod
+    def backward(fctx, g):
+        ctx = fctx.mctx
+        xs, omega, sino_f, norm, _ = fctx.saved_tensors
+        K = omega.shape[0]
+        g = g.contiguous()
+        d_omega = torch.zeros_like(omega)
+        for k in range(K - 1, -1, -1):
+            xk = xs[k]
+            f, u, r = _ratio(ctx, xk, sino_f, norm)           # recompute from the checkpoint
+            pos = r > 0
+            rs = torch.where(pos, r, torch.ones_like(r))
+            p = torch.where(pos, rs ** omega[k], torch.zeros_like(r))  # r^w
+            x_next = xk * p
+            d_omega[k] = torch.sum(g * x_next * torch.where(pos, torch.log(rs), torch.zeros_like(r)))
+            gx = g * p                                          # direct path
+            dr = torch.where(pos, g * xk * omega[k] * rs ** (omega[k] - 1), torch.zeros_like(r))
+            du = torch.where(norm != 0, dr / torch.where(norm != 0, norm, torch.ones_like(norm)), dr)
+            dc = _fw(ctx, du)                                   # adjoint of A^T
+            fnz = f != 0
+            fs = torch.where(fnz, f, torch.ones_like(f))
+            df = torch.where(fnz, -dc * sino_f / (fs * fs), torch.zeros_like(f))
+            gx = gx + _bk(ctx, df)                              # adjoint of A
+            g = gx
+        return g, d_omega, None, None, None
+
+
+def unrolled_mlem(x0: torch.Tensor, omega: torch.Tensor, sino: torch.Tensor,
+                  ctx: "api.Context", norm: torch.Tensor | None = None) -> torch.Tensor:
+    """K = len(omega) relaxed MLEM iterations from x0 (float32 [C] CUDA)."""
+    _check(x0, ctx.n_cols, "x0")
+    if norm is None:
+        norm = norm_tensor(ctx, x0.device)
+    sino_f = sino.to(device=x0.device, dtype=torch.float32)
+    return _UnrolledMLEM.apply(x0, omega.to(device=x0.device, dtype=torch.float32), sino_f, norm, ctx)
