@@ -55,7 +55,8 @@ extern "C" {
 /* ---- context flags ------------------------------------------------------ */
 #define MLEM_FLAG_EXACT 0x1u    /* bit-exact kernels: the float operation order of seqcsr4mlem */
 #define MLEM_FLAG_NO_CSC 0x2u   /* do not build the CSC copy (atomic back projection only) */
-#define MLEM_FLAG_CHECKED 0x4u  /* validate offsets and column indices on the device at create */
+#define MLEM_FLAG_CHECKED 0x4u  /* accepted for compatibility: offsets and column indices are always validated */
+#define MLEM_FLAG_NATURAL_LAYOUT 0x8u /* keep the natural voxel order on the device (no brick layout) */
 
 /* ---- back-projection strategies ---------------------------------------- */
 #define MLEM_BK_AUTO 0    /* the autotuner's choice (CSC when not tuned) */
@@ -100,7 +101,18 @@ int mlem_version(void);
 int mlem_create(mlem_ctx** out, const uint64_t* row_end, const void* elems, uint32_t n_rows,
                 uint32_t n_cols, uint64_t nnz, uint32_t flags, int device);
 
-/* Same, from a CSR4 file (the command-line driver's path). */
+/* Same, with the voxel grid (nx, ny, nz; nx*ny*nz == n_cols): the device
+ * then stores the image in 8x8x8 bricks (Morton order inside), which keeps a
+ * ray's voxels in few cache lines.  Only the device layout changes; every
+ * host- and device-pointer interface keeps the natural voxel order
+ * ix + nx*(iy + ny*iz) (helper_files_common/scannerconfig.cpp getVoxelNr)
+ * and every result is unchanged.  grid == NULL: natural order. */
+int mlem_create_grid(mlem_ctx** out, const uint64_t* row_end, const void* elems, uint32_t n_rows,
+                     uint32_t n_cols, uint64_t nnz, const uint32_t grid[3], uint32_t flags,
+                     int device);
+
+/* Same, from a CSR4 file (the command-line driver's path; the grid comes
+ * from the file's scanner block). */
 int mlem_create_from_file(mlem_ctx** out, const char* csr4_path, uint32_t flags, int device);
 
 /* Synthetic Siddon matrix generated on the device (bit-identical to the host

@@ -37,6 +37,7 @@ MLEM_NO_CHECKPOINT = 8
 FLAG_EXACT = 0x1
 FLAG_NO_CSC = 0x2
 FLAG_CHECKED = 0x4
+FLAG_NATURAL_LAYOUT = 0x8
 
 BK_AUTO, BK_CSC, BK_ATOMIC, BK_FUSED = 0, 1, 2, 3
 BK_NAMES = {BK_CSC: "csc", BK_ATOMIC: "atomic", BK_FUSED: "fused"}
@@ -84,14 +85,20 @@ def _i32(a, n=None, name="array"):
 class Context:
     """A CSR4 matrix on one GPU (mlem_create)."""
 
-    def __init__(self, row_end, elems, n_rows: int, n_cols: int, flags: int = 0, device: int = 0):
+    def __init__(self, row_end, elems, n_rows: int, n_cols: int, flags: int = 0, device: int = 0,
+                 grid=None):
+        """grid = (nx, ny, nz) with nx*ny*nz == n_cols enables the device brick
+        layout of the image (results are unchanged); None keeps natural order."""
         lib = core_lib()
         row_end = np.ascontiguousarray(row_end, dtype=np.uint64)
         elems = np.ascontiguousarray(elems)
         nnz = int(row_end[-1]) if n_rows else 0
         h = ctypes.c_void_p()
-        st = lib.mlem_create(ctypes.byref(h), _p(row_end), _p(elems), n_rows, n_cols, nnz, flags,
-                             device)
+        g = None
+        if grid is not None and int(np.prod(grid)) == n_cols:
+            g = (ctypes.c_uint32 * 3)(*[int(v) for v in grid])
+        st = lib.mlem_create_grid(ctypes.byref(h), _p(row_end), _p(elems), n_rows, n_cols, nnz, g,
+                                  flags, device)
         _raise(st)
         self._h = h
         self._refresh()
@@ -105,8 +112,11 @@ class Context:
 
     @classmethod
     def from_matrix(cls, m, flags: int = 0, device: int = 0) -> "Context":
-        """From a formats.Csr4 (host arrays or a memory-mapped file)."""
-        return cls(m.row_end, m.elems, m.n_rows, m.n_cols, flags, device)
+        """From a formats.Csr4 (host arrays or a memory-mapped file); its grid
+        selects the device brick layout when it matches the column count."""
+        grid = getattr(m, "grid", None)
+        return cls(m.row_end, m.elems, m.n_rows, m.n_cols, flags, device,
+                   grid if grid and int(np.prod(grid)) == m.n_cols else None)
 
     @classmethod
     def from_file(cls, path: str, flags: int = 0, device: int = 0) -> "Context":

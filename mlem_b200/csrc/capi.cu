@@ -38,9 +38,20 @@ struct mlem_ctx {
     uint2* celems = nullptr;
     bool has_csc = false;
     uint32_t max_col_len = 0, max_row_len = 0;
-    float* norm = nullptr;
-    std::vector<float> norm_host;
+    float* norm = nullptr;       // column sums, device voxel order
+    float* norm_nat = nullptr;   // column sums, natural voxel order
+    std::vector<float> norm_host;  // natural order
     double sumnorm = 0.0;
+
+    // Voxel order on the device.  With a known grid the columns are
+    // relabelled into 8x8x8 bricks with Morton order inside (see
+    // brick_order); perm maps a natural voxel index to its device index.
+    bool bricked = false;
+    uint32_t grid[3] = {0, 0, 0};
+    uint32_t* perm = nullptr;
+    std::vector<uint32_t> perm_host, iperm_host;
+    float* pscratch[2] = {nullptr, nullptr};
+    size_t pscratch_floats = 0;
 
     // frames
     uint32_t B = 0, Bp = 0;
@@ -175,7 +186,61 @@ void default_tuning(mlem_ctx* c) {
 }
 
 // ---------------------------------------------------------------------------
-// Setup common to all create paths: validate, CSC, column sums.
+// Device voxel order.  A ray's consecutive voxels are neighbours in 3-D; in
+// the natural order (ix + nx*(iy + ny*iz), scannerconfig.cpp getVoxelNr)
+// only its x-steps stay inside a 128-byte line.  Bricks of 8x8x8 voxels in
+// raster order with a Morton (Z-order) curve inside put every 2x2x2 cube in
+// one 32-byte sector and every 4x4x2 block in one 128-byte line, so the
+// image gathers and update scatters of a ray touch far fewer lines.  Grids
+// that are not multiples of 8 are padded conceptually and the codes ranked.
+// The relabelling changes no arithmetic: rows keep their element order and
+// columns keep their ascending row order.
+// ---------------------------------------------------------------------------
+uint32_t morton9(uint32_t x, uint32_t y, uint32_t z) {
+    uint32_t m = 0;
+    for (int b = 0; b < 3; ++b)
+        m |= (((x >> b) & 1u) << (3 * b)) | (((y >> b) & 1u) << (3 * b + 1)) |
+             (((z >> b) & 1u) << (3 * b + 2));
+    return m;
+}
+
+void brick_order(uint32_t nx, uint32_t ny, uint32_t nz, std::vector<uint32_t>& perm) {
+    const uint64_t C = (uint64_t)nx * ny * nz;
+    const uint32_t bx = (nx + 7) / 8, by = (ny + 7) / 8;
+    perm.resize(C);
+    std::vector<uint64_t> code(C);
+    for (uint32_t iz = 0; iz < nz; ++iz)
+        for (uint32_t iy = 0; iy < ny; ++iy)
+            for (uint32_t ix = 0; ix < nx; ++ix) {
+                const uint64_t brick = (ix >> 3) + (uint64_t)bx * ((iy >> 3) + (uint64_t)by * (iz >> 3));
+                code[ix + (uint64_t)nx * (iy + (uint64_t)ny * iz)] =
+                    brick * 512 + morton9(ix & 7, iy & 7, iz & 7);
+            }
+    if (nx % 8 == 0 && ny % 8 == 0 && nz % 8 == 0) {
+        for (uint64_t v = 0; v < C; ++v) perm[v] = (uint32_t)code[v];
+        return;
+    }
+    std::vector<uint32_t> order(C);
+    for (uint64_t v = 0; v < C; ++v) order[v] = (uint32_t)v;
+    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return code[a] < code[b]; });
+    for (uint64_t k = 0; k < C; ++k) perm[order[k]] = (uint32_t)k;
+}
+
+// Scratch for converting caller vectors between natural and device order.
+int perm_scratch(mlem_ctx* c, size_t floats) {
+    if (c->pscratch_floats >= floats) return MLEM_OK;
+    for (auto& p : c->pscratch) {
+        if (p) { cudaFree(p); c->device_bytes -= c->pscratch_floats * 4; }
+        p = nullptr;
+    }
+    c->pscratch_floats = 0;
+    for (auto& p : c->pscratch) TRY(dev_alloc(c, &p, floats));
+    c->pscratch_floats = floats;
+    return MLEM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Setup common to all create paths: validate, voxel order, CSC, column sums.
 // ---------------------------------------------------------------------------
 int finish_create(mlem_ctx* c) {
     // device-side validation: offsets non-decreasing, last offset == Z, columns < C
@@ -190,6 +255,18 @@ int finish_create(mlem_ctx* c) {
     if (hbad & 1u) return fail(c, MLEM_ERR_MATRIX, "row offsets decrease");
     if (hbad & 2u) return fail(c, MLEM_ERR_MATRIX, "last row offset differs from nnz");
     if (hbad & 4u) return fail(c, MLEM_ERR_MATRIX, "a column index is >= the number of columns");
+
+    const uint64_t gC = (uint64_t)c->grid[0] * c->grid[1] * c->grid[2];
+    if (!(c->flags & MLEM_FLAG_NATURAL_LAYOUT) && gC == c->C && c->C > 0) {
+        brick_order(c->grid[0], c->grid[1], c->grid[2], c->perm_host);
+        c->iperm_host.resize(c->C);
+        for (uint32_t v = 0; v < c->C; ++v) c->iperm_host[c->perm_host[v]] = v;
+        TRY(dev_alloc(c, &c->perm, c->C));
+        CK(c, cudaMemcpyAsync(c->perm, c->perm_host.data(), (size_t)c->C * 4,
+                              cudaMemcpyHostToDevice, c->stream));
+        CK(c, remap_columns(c->elems, c->Z, c->perm, c->stream));
+        c->bricked = true;
+    }
 
     if (!(c->flags & MLEM_FLAG_NO_CSC)) {
         TRY(dev_alloc(c, &c->col_ptr, (size_t)c->C + 1));
@@ -208,9 +285,15 @@ int finish_create(mlem_ctx* c) {
     } else {
         CK(c, column_sums_atomic(csr_view(c), c->C, c->norm, c->stream));
     }
+    TRY(dev_alloc(c, &c->norm_nat, std::max<uint32_t>(c->C, 1)));
+    if (c->bricked)
+        CK(c, permute_to_natural(c->norm, c->norm_nat, c->perm, c->C, 1, c->stream));
+    else if (c->C)
+        CK(c, cudaMemcpyAsync(c->norm_nat, c->norm, (size_t)c->C * 4, cudaMemcpyDeviceToDevice,
+                              c->stream));
     c->norm_host.resize(c->C);
     if (c->C)
-        CK(c, cudaMemcpyAsync(c->norm_host.data(), c->norm, (size_t)c->C * 4,
+        CK(c, cudaMemcpyAsync(c->norm_host.data(), c->norm_nat, (size_t)c->C * 4,
                               cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     // initImage's sum (seqcsr4mlem.cpp:55-56): sequential double sum of the norm.
@@ -239,7 +322,7 @@ int new_ctx(mlem_ctx** out, uint32_t R, uint32_t C, uint64_t Z, uint32_t flags, 
                     e != cudaSuccess ? cudaGetErrorString(e) : "0 devices");
     if (device < 0 || device >= n_dev)
         return fail(nullptr, MLEM_ERR_INVALID, "device %d out of range (%d devices)", device, n_dev);
-    if (flags & ~(MLEM_FLAG_EXACT | MLEM_FLAG_NO_CSC | MLEM_FLAG_CHECKED))
+    if (flags & ~(MLEM_FLAG_EXACT | MLEM_FLAG_NO_CSC | MLEM_FLAG_CHECKED | MLEM_FLAG_NATURAL_LAYOUT))
         return fail(nullptr, MLEM_ERR_INVALID, "unknown flags 0x%x", flags);
     if ((flags & MLEM_FLAG_EXACT) && (flags & MLEM_FLAG_NO_CSC))
         return fail(nullptr, MLEM_ERR_INVALID, "MLEM_FLAG_EXACT needs the CSC copy");
@@ -307,7 +390,6 @@ int alloc_frames(mlem_ctx* c, uint32_t B) {
     CK(c, cudaMemsetAsync(c->update, 0, (size_t)c->C * Bp * 4, c->stream));
     c->tuning.frame_tile = std::min(c->tuning.frame_tile > 0 ? c->tuning.frame_tile : 16,
                                     default_tile(Bp));
-    if (c->tuning.frame_tile > c->tuning.group) c->tuning.frame_tile = c->tuning.group;
     c->graph_dirty = true;
     return MLEM_OK;
 }
@@ -315,7 +397,8 @@ int alloc_frames(mlem_ctx* c, uint32_t B) {
 // Frame-major host [B][n] -> interleaved device [n][Bp] (pad frames untouched).
 template <typename T>
 int upload_frames(mlem_ctx* c, const T* host, T* dev, uint64_t n) {
-    if (c->Bp == 1) {
+    const bool voxels = std::is_same<T, float>::value && c->bricked;
+    if (c->Bp == 1 && !voxels) {
         CK(c, cudaMemcpyAsync(dev, host, n * sizeof(T), cudaMemcpyHostToDevice, c->stream));
         return MLEM_OK;
     }
@@ -326,18 +409,19 @@ int upload_frames(mlem_ctx* c, const T* host, T* dev, uint64_t n) {
                              reinterpret_cast<int32_t*>(dev), n, c->B, c->Bp, c->stream));
     else
         CK(c, interleave_f32(reinterpret_cast<const float*>(c->stage),
-                             reinterpret_cast<float*>(dev), n, c->B, c->Bp, c->stream));
+                             reinterpret_cast<float*>(dev), n, c->B, c->Bp,
+                             voxels ? c->perm : nullptr, c->stream));
     return MLEM_OK;
 }
 
 int download_images(mlem_ctx* c, float* host) {
-    if (c->Bp == 1) {
+    if (c->Bp == 1 && !c->bricked) {
         CK(c, cudaMemcpyAsync(host, c->x, (size_t)c->C * 4, cudaMemcpyDeviceToHost, c->stream));
         return MLEM_OK;
     }
     TRY(ensure_stage(c, (size_t)c->C * c->B * 4));
     float* st = static_cast<float*>(c->stage);
-    CK(c, deinterleave_f32(c->x, st, c->C, c->B, c->Bp, c->stream));
+    CK(c, deinterleave_f32(c->x, st, c->C, c->B, c->Bp, c->bricked ? c->perm : nullptr, c->stream));
     CK(c, cudaMemcpyAsync(host, st, (size_t)c->C * c->B * 4, cudaMemcpyDeviceToHost, c->stream));
     return MLEM_OK;
 }
@@ -495,7 +579,6 @@ LaunchCfg cfg_for_frames(const mlem_ctx* c, uint32_t B) {
     for (int v : {16, 8, 4, 2})
         if (B % v == 0) { t = v; break; }
     cfg.frame_tile = t;
-    if (cfg.group < t) cfg.group = t;
     return cfg;
 }
 
@@ -529,6 +612,12 @@ const char* mlem_status_string(int s) {
 
 int mlem_create(mlem_ctx** out, const uint64_t* row_end, const void* elems, uint32_t n_rows,
                 uint32_t n_cols, uint64_t nnz, uint32_t flags, int device) {
+    return mlem_create_grid(out, row_end, elems, n_rows, n_cols, nnz, nullptr, flags, device);
+}
+
+int mlem_create_grid(mlem_ctx** out, const uint64_t* row_end, const void* elems, uint32_t n_rows,
+                     uint32_t n_cols, uint64_t nnz, const uint32_t grid[3], uint32_t flags,
+                     int device) {
     if (!out) return fail(nullptr, MLEM_ERR_INVALID, "out is null");
     *out = nullptr;
     if ((n_rows && !row_end) || (nnz && !elems))
@@ -545,6 +634,8 @@ int mlem_create(mlem_ctx** out, const uint64_t* row_end, const void* elems, uint
                     (unsigned long long)prev, (unsigned long long)nnz);
     mlem_ctx* c = nullptr;
     TRY(new_ctx(&c, n_rows, n_cols, nnz, flags, device));
+    if (grid)
+        for (int i = 0; i < 3; ++i) c->grid[i] = grid[i];
     c->max_row_len = (uint32_t)std::min<uint64_t>(max_row, 0xffffffffu);
     int s = alloc_matrix(c);
     if (s == MLEM_OK && n_rows) {
@@ -575,6 +666,9 @@ int mlem_create_siddon(mlem_ctx** out, uint32_t nx, uint32_t ny, uint32_t nz, ui
     if (!(min_len > 0.0)) return fail(nullptr, MLEM_ERR_INVALID, "min_len must be > 0");
     mlem_ctx* c = nullptr;
     TRY(new_ctx(&c, n_rows, (uint32_t)C64, 0, flags, device));
+    c->grid[0] = nx;
+    c->grid[1] = ny;
+    c->grid[2] = nz;
     SiddonSpec spec{nx, ny, nz, n_rows, min_count, max_count, radius_scale, min_len, seed};
     int s = MLEM_OK;
     uint64_t* counts = nullptr;
@@ -628,7 +722,8 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->norm, c->stage, (void*)c->stats_slot, (void*)c->hist_sums,
                     (void*)c->hist_zeros, (void*)c->hist_subn, (void*)c->tmp_r[0],
                     (void*)c->tmp_r[1], (void*)c->tmp_c[0], (void*)c->tmp_c[1], (void*)c->tmp_c[2],
-                    (void*)c->tmp_sino, (void*)c->tmp_d})
+                    (void*)c->tmp_sino, (void*)c->tmp_d, (void*)c->norm_nat, (void*)c->perm,
+                    (void*)c->pscratch[0], (void*)c->pscratch[1]})
         dev_free(p);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -677,7 +772,13 @@ int mlem_get_csr(mlem_ctx* c, uint64_t* row_end, void* elems) {
     TRY(set_device(c));
     if (row_end && c->R)
         CK(c, cudaMemcpy(row_end, c->row_ptr + 1, (size_t)c->R * 8, cudaMemcpyDeviceToHost));
-    if (elems && c->Z) CK(c, cudaMemcpy(elems, c->elems, c->Z * 8, cudaMemcpyDeviceToHost));
+    if (elems && c->Z) {
+        CK(c, cudaMemcpy(elems, c->elems, c->Z * 8, cudaMemcpyDeviceToHost));
+        if (c->bricked) {
+            uint32_t* w = static_cast<uint32_t*>(elems);
+            for (uint64_t k = 0; k < c->Z; ++k) w[2 * k] = c->iperm_host[w[2 * k]];
+        }
+    }
     return MLEM_OK;
 }
 
@@ -685,8 +786,26 @@ int mlem_get_csc(mlem_ctx* c, uint64_t* col_ptr, void* elems) {
     if (!c) return fail(nullptr, MLEM_ERR_INVALID, "null context");
     if (!c->has_csc) return fail(c, MLEM_ERR_STATE, "context has no CSC copy");
     TRY(set_device(c));
-    if (col_ptr) CK(c, cudaMemcpy(col_ptr, c->col_ptr, ((size_t)c->C + 1) * 8, cudaMemcpyDeviceToHost));
-    if (elems && c->Z) CK(c, cudaMemcpy(elems, c->celems, c->Z * 8, cudaMemcpyDeviceToHost));
+    if (!c->bricked) {
+        if (col_ptr)
+            CK(c, cudaMemcpy(col_ptr, c->col_ptr, ((size_t)c->C + 1) * 8, cudaMemcpyDeviceToHost));
+        if (elems && c->Z) CK(c, cudaMemcpy(elems, c->celems, c->Z * 8, cudaMemcpyDeviceToHost));
+        return MLEM_OK;
+    }
+    // device columns are in brick order: reassemble in natural column order
+    std::vector<uint64_t> dptr((size_t)c->C + 1);
+    CK(c, cudaMemcpy(dptr.data(), c->col_ptr, dptr.size() * 8, cudaMemcpyDeviceToHost));
+    std::vector<uint2> del(c->Z);
+    if (c->Z) CK(c, cudaMemcpy(del.data(), c->celems, c->Z * 8, cudaMemcpyDeviceToHost));
+    uint64_t pos = 0;
+    uint2* eo = static_cast<uint2*>(elems);
+    for (uint32_t v = 0; v < c->C; ++v) {
+        const uint32_t d = c->perm_host[v];
+        if (col_ptr) col_ptr[v] = pos;
+        for (uint64_t k = dptr[d]; k < dptr[d + 1]; ++k, ++pos)
+            if (eo) eo[pos] = del[k];
+    }
+    if (col_ptr) col_ptr[c->C] = pos;
     return MLEM_OK;
 }
 
@@ -710,11 +829,16 @@ int mlem_calc_fwproj(mlem_ctx* c, const float* image, float* out) {
     TRY(set_device(c));
     TRY(ensure_tmp(c));
     CK(c, cudaMemcpyAsync(c->tmp_c[0], image, (size_t)c->C * 4, cudaMemcpyHostToDevice, c->stream));
+    const float* xd = c->tmp_c[0];
+    if (c->bricked) {
+        CK(c, permute_to_device(c->tmp_c[0], c->tmp_c[1], c->perm, c->C, 1, c->stream));
+        xd = c->tmp_c[1];
+    }
     if (c->flags & MLEM_FLAG_EXACT)
-        CK(c, fwproj_exact(csr_view(c), c->tmp_c[0], 1, nullptr, nullptr, c->tmp_r[0], c->stream));
+        CK(c, fwproj_exact(csr_view(c), xd, 1, nullptr, nullptr, c->tmp_r[0], c->stream));
     else
-        CK(c, fwproj(csr_view(c), c->tmp_c[0], 1, 0, nullptr, nullptr, c->tmp_r[0],
-                     cfg_for_frames(c, 1), c->stream));
+        CK(c, fwproj(csr_view(c), xd, 1, 0, nullptr, nullptr, c->tmp_r[0], cfg_for_frames(c, 1),
+                     c->stream));
     CK(c, cudaMemcpyAsync(out, c->tmp_r[0], (size_t)c->R * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     return MLEM_OK;
@@ -740,16 +864,17 @@ int mlem_calc_bkproj(mlem_ctx* c, const float* correl, float* update) {
     TRY(set_device(c));
     TRY(ensure_tmp(c));
     CK(c, cudaMemcpyAsync(c->tmp_r[0], correl, (size_t)c->R * 4, cudaMemcpyHostToDevice, c->stream));
+    float* ud = c->bricked ? c->tmp_c[1] : c->tmp_c[0];
     if (c->flags & MLEM_FLAG_EXACT) {
-        CK(c, bkproj_exact(csc_view(c), c->tmp_r[0], 1, nullptr, nullptr, c->tmp_c[0], c->stream));
+        CK(c, bkproj_exact(csc_view(c), c->tmp_r[0], 1, nullptr, nullptr, ud, c->stream));
     } else if (c->has_csc) {
-        CK(c, bkproj_csc(csc_view(c), c->tmp_r[0], 1, 0, nullptr, nullptr, c->tmp_c[0],
+        CK(c, bkproj_csc(csc_view(c), c->tmp_r[0], 1, 0, nullptr, nullptr, ud,
                          cfg_for_frames(c, 1), c->stream));
     } else {
-        CK(c, cudaMemsetAsync(c->tmp_c[0], 0, (size_t)c->C * 4, c->stream));
-        CK(c, bkproj_scatter(csr_view(c), c->tmp_r[0], 1, 0, c->tmp_c[0], cfg_for_frames(c, 1),
-                             c->stream));
+        CK(c, cudaMemsetAsync(ud, 0, (size_t)c->C * 4, c->stream));
+        CK(c, bkproj_scatter(csr_view(c), c->tmp_r[0], 1, 0, ud, cfg_for_frames(c, 1), c->stream));
     }
+    if (c->bricked) CK(c, permute_to_natural(ud, c->tmp_c[0], c->perm, c->C, 1, c->stream));
     CK(c, cudaMemcpyAsync(update, c->tmp_c[0], (size_t)c->C * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     return MLEM_OK;
@@ -964,7 +1089,7 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
     for (int mode : modes)
         for (int group : {8, 16, 32})
             for (int tile : {1, 2, 4, 8, 16}) {
-                if (tile > group || (c->Bp % (uint32_t)tile)) continue;
+                if (c->Bp % (uint32_t)tile) continue;
                 for (int bps : {4, 8}) {
                     mlem_tuning t{mode, group, tile, bps, 0.0};
                     // warm-up once, then time two iterations
@@ -995,12 +1120,21 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
 }
 
 // ---- device-pointer entry points ---------------------------------------------
+// Caller vectors are in natural voxel order; with the brick layout they are
+// converted through the context's scratch buffers.
 int mlem_fwproj_d(mlem_ctx* c, const float* x, float* y, uint32_t B, void* stream) {
     if (!c || !x || !y || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
     TRY(set_device(c));
+    cudaStream_t st = (cudaStream_t)stream;
+    const float* xd = x;
+    if (c->bricked) {
+        TRY(perm_scratch(c, (size_t)c->C * B));
+        CK(c, permute_to_device(x, c->pscratch[0], c->perm, c->C, B, st));
+        xd = c->pscratch[0];
+    }
     const LaunchCfg cfg = cfg_for_frames(c, B);
     for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
-        CK(c, fwproj(csr_view(c), x, B, f0, nullptr, nullptr, y, cfg, (cudaStream_t)stream));
+        CK(c, fwproj(csr_view(c), xd, B, f0, nullptr, nullptr, y, cfg, st));
     return MLEM_OK;
 }
 
@@ -1009,14 +1143,20 @@ int mlem_bkproj_d(mlem_ctx* c, const float* y, float* x, uint32_t B, void* strea
     TRY(set_device(c));
     const LaunchCfg cfg = cfg_for_frames(c, B);
     cudaStream_t st = (cudaStream_t)stream;
+    float* xd = x;
+    if (c->bricked) {
+        TRY(perm_scratch(c, (size_t)c->C * B));
+        xd = c->pscratch[0];
+    }
     for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile) {
         if (c->has_csc) {
-            CK(c, bkproj_csc(csc_view(c), y, B, f0, nullptr, nullptr, x, cfg, st));
+            CK(c, bkproj_csc(csc_view(c), y, B, f0, nullptr, nullptr, xd, cfg, st));
         } else {
-            if (f0 == 0) CK(c, cudaMemsetAsync(x, 0, (size_t)c->C * B * 4, st));
-            CK(c, bkproj_scatter(csr_view(c), y, B, f0, x, cfg, st));
+            if (f0 == 0) CK(c, cudaMemsetAsync(xd, 0, (size_t)c->C * B * 4, st));
+            CK(c, bkproj_scatter(csr_view(c), y, B, f0, xd, cfg, st));
         }
     }
+    if (c->bricked) CK(c, permute_to_natural(xd, x, c->perm, c->C, B, st));
     return MLEM_OK;
 }
 
@@ -1024,9 +1164,16 @@ int mlem_fwproj_correl_d(mlem_ctx* c, const float* x, const int32_t* sino, float
                          uint32_t B, void* stream) {
     if (!c || !x || !sino || !correl || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
     TRY(set_device(c));
+    cudaStream_t st = (cudaStream_t)stream;
+    const float* xd = x;
+    if (c->bricked) {
+        TRY(perm_scratch(c, (size_t)c->C * B));
+        CK(c, permute_to_device(x, c->pscratch[0], c->perm, c->C, B, st));
+        xd = c->pscratch[0];
+    }
     const LaunchCfg cfg = cfg_for_frames(c, B);
     for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
-        CK(c, fwproj(csr_view(c), x, B, f0, sino, correl, nullptr, cfg, (cudaStream_t)stream));
+        CK(c, fwproj(csr_view(c), xd, B, f0, sino, correl, nullptr, cfg, st));
     return MLEM_OK;
 }
 
@@ -1034,22 +1181,31 @@ int mlem_bkproj_update_d(mlem_ctx* c, const float* correl, float* x, uint32_t B,
     if (!c || !x || !correl || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
     if (!c->has_csc) return fail(c, MLEM_ERR_STATE, "fused back projection needs the CSC copy");
     TRY(set_device(c));
+    cudaStream_t st = (cudaStream_t)stream;
+    float* xd = x;
+    if (c->bricked) {
+        TRY(perm_scratch(c, (size_t)c->C * B));
+        CK(c, permute_to_device(x, c->pscratch[0], c->perm, c->C, B, st));
+        xd = c->pscratch[0];
+    }
     const LaunchCfg cfg = cfg_for_frames(c, B);
     for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
-        CK(c, bkproj_csc(csc_view(c), correl, B, f0, c->norm, x, nullptr, cfg, (cudaStream_t)stream));
+        CK(c, bkproj_csc(csc_view(c), correl, B, f0, c->norm, xd, nullptr, cfg, st));
+    if (c->bricked) CK(c, permute_to_natural(xd, x, c->perm, c->C, B, st));
     return MLEM_OK;
 }
 
 int mlem_apply_update_d(mlem_ctx* c, const float* update, float* x, uint32_t B, void* stream) {
     if (!c || !x || !update || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
     TRY(set_device(c));
-    CK(c, apply_update(x, const_cast<float*>(update), c->norm, c->C, B, false, (cudaStream_t)stream));
+    CK(c, apply_update(x, const_cast<float*>(update), c->norm_nat, c->C, B, false,
+                       (cudaStream_t)stream));
     return MLEM_OK;
 }
 
 int mlem_norm_d(mlem_ctx* c, const float** norm) {
     if (!c || !norm) return fail(c, MLEM_ERR_INVALID, "null argument");
-    *norm = c->norm;
+    *norm = c->norm_nat;
     return MLEM_OK;
 }
 
@@ -1057,8 +1213,11 @@ int mlem_set_norm_d(mlem_ctx* c, const float* norm, void* stream) {
     if (!c || !norm) return fail(c, MLEM_ERR_INVALID, "null argument");
     TRY(set_device(c));
     cudaStream_t st = (cudaStream_t)stream;
-    CK(c, cudaMemcpyAsync(c->norm, norm, (size_t)c->C * 4, cudaMemcpyDeviceToDevice, st));
-    CK(c, cudaMemcpyAsync(c->norm_host.data(), norm, (size_t)c->C * 4, cudaMemcpyDeviceToHost, st));
+    CK(c, cudaMemcpyAsync(c->norm_nat, norm, (size_t)c->C * 4, cudaMemcpyDeviceToDevice, st));
+    if (c->bricked) CK(c, permute_to_device(c->norm_nat, c->norm, c->perm, c->C, 1, st));
+    else CK(c, cudaMemcpyAsync(c->norm, norm, (size_t)c->C * 4, cudaMemcpyDeviceToDevice, st));
+    CK(c, cudaMemcpyAsync(c->norm_host.data(), c->norm_nat, (size_t)c->C * 4,
+                          cudaMemcpyDeviceToHost, st));
     CK(c, cudaStreamSynchronize(st));
     double s = 0.0;
     for (uint32_t i = 0; i < c->C; ++i) s += c->norm_host[i];
@@ -1072,7 +1231,12 @@ int mlem_project_f64(mlem_ctx* c, const float* x, double* out) {
     TRY(ensure_tmp(c));
     if (!c->tmp_d) TRY(dev_alloc(c, &c->tmp_d, std::max<uint32_t>(c->R, 1)));
     CK(c, cudaMemcpyAsync(c->tmp_c[0], x, (size_t)c->C * 4, cudaMemcpyHostToDevice, c->stream));
-    CK(c, project_f64(csr_view(c), c->tmp_c[0], c->tmp_d, c->stream));
+    const float* xd = c->tmp_c[0];
+    if (c->bricked) {
+        CK(c, permute_to_device(c->tmp_c[0], c->tmp_c[1], c->perm, c->C, 1, c->stream));
+        xd = c->tmp_c[1];
+    }
+    CK(c, project_f64(csr_view(c), xd, c->tmp_d, c->stream));
     CK(c, cudaMemcpyAsync(out, c->tmp_d, (size_t)c->R * 8, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     return MLEM_OK;

@@ -39,6 +39,23 @@ __device__ __forceinline__ uint4 ld_stream(const uint4* ptr, uint64_t pol) {
     return r;
 }
 
+// 8-byte streaming load of one element.
+__device__ __forceinline__ uint2 ld_stream2(const uint2* ptr, uint64_t pol) {
+    uint2 r;
+    asm("ld.global.nc.L1::no_allocate.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;"
+        : "=r"(r.x), "=r"(r.y)
+        : "l"(ptr), "l"(pol));
+    return r;
+}
+
+__device__ __forceinline__ uint2 ld_keep2(const uint2* ptr, uint64_t pol) {
+    uint2 r;
+    asm("ld.global.nc.L2::cache_hint.v2.u32 {%0,%1}, [%2], %3;"
+        : "=r"(r.x), "=r"(r.y)
+        : "l"(ptr), "l"(pol));
+    return r;
+}
+
 // 16-byte load that allocates in L1 (the fused one-pass kernel re-reads the row).
 __device__ __forceinline__ uint4 ld_keep(const uint4* ptr, uint64_t pol) {
     uint4 r;

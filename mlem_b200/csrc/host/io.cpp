@@ -351,7 +351,7 @@ int mlem_create_from_file(mlem_ctx** out, const char* path, uint32_t flags, int 
         std::memcpy(aligned.data(), base + h.data_offset, 8ull * h.n_rows);
         row_end = aligned.data();
     }
-    s = mlem_create(out, row_end, elems, h.n_rows, h.n_cols, h.nnz, flags, device);
+    s = mlem_create_grid(out, row_end, elems, h.n_rows, h.n_cols, h.nnz, h.grid, flags, device);
     if (map) ::munmap(map, h.file_size);
     return s;
 }

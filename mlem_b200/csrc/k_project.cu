@@ -5,15 +5,19 @@
 // per-row kernel, and the bit-exact variants.  Reference functions:
 // calcFwProj/calcCorrel/calcBkProj/calcUpdate, mlem_seq/seqcsr4mlem.cpp:69-134.
 //
-// Work decomposition: G lanes (4..32) own one row (or column); a warp owns
+// Work decomposition.  G lanes (4..32) own one row (or column); a warp owns
 // 32/G rows; warps stride over rows (grid = blocks_per_sm x SMs, persistent
-// style).  Each lane reads whole 16-byte element pairs, so a warp issues
-// fully coalesced 512-byte reads of the element stream.  A row that starts
-// on an odd element shares its first pair with the previous row: the lane
-// masks the element that is not its own.  Frames (B sinograms reconstructed
-// together) are interleaved in the vectors, and a kernel instance processes a
-// tile of BT frames per pass over the matrix, gathering BT contiguous floats
-// per element with 16-byte loads.
+// style).  A kernel instance handles a tile of BT frames of the B frames that
+// are interleaved in the vectors (x[col][B], c[row][B], ...).  Each element's
+// BT floats are split over FL = BT/VW lanes of VW <= 4 floats, so the G lanes
+// work on EPS = G/FL consecutive elements at a time: lane (slot, sub) takes
+// element b + slot + j*EPS and frames [sub*VW, sub*VW + VW) of the tile.
+// One gather instruction therefore reads, per element, one contiguous
+// 4..64-byte block of the vector, and with one frame the 32 lanes hold 32
+// consecutive voxels of a ray (packed into few sectors by the brick layout).
+// Element loads are 8 bytes per lane with an L2 evict_first policy (the
+// matrix is streamed once per pass); vector gathers use evict_last.  The
+// per-row sums are combined by a butterfly over the slot bits of the lane.
 #include <algorithm>
 
 #include "common.cuh"
@@ -24,78 +28,131 @@ namespace mlem {
 namespace {
 
 template <int BT>
-__device__ __forceinline__ void gather(const float* __restrict__ p, float (&v)[BT], uint64_t pol) {
-    if constexpr (BT % 4 == 0) {
-#pragma unroll
-        for (int i = 0; i < BT / 4; ++i) {
-            float4 t = ld_hot4(reinterpret_cast<const float4*>(p) + i, pol);
-            v[4 * i + 0] = t.x; v[4 * i + 1] = t.y; v[4 * i + 2] = t.z; v[4 * i + 3] = t.w;
-        }
+struct Lanes {
+    static constexpr int VW = BT < 4 ? BT : 4;  // floats per lane
+    static constexpr int FL = BT / VW;          // lanes per element
+};
+
+__device__ __forceinline__ float2 ld_hot2(const float2* ptr, uint64_t pol) {
+    float2 r;
+    asm("ld.global.nc.L2::cache_hint.v2.f32 {%0,%1}, [%2], %3;" : "=f"(r.x), "=f"(r.y)
+        : "l"(ptr), "l"(pol));
+    return r;
+}
+
+template <int VW>
+__device__ __forceinline__ void ld_vec(const float* __restrict__ p, float (&v)[VW], uint64_t pol) {
+    if constexpr (VW == 4) {
+        const float4 t = ld_hot4(reinterpret_cast<const float4*>(p), pol);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else if constexpr (VW == 2) {
+        const float2 t = ld_hot2(reinterpret_cast<const float2*>(p), pol);
+        v[0] = t.x; v[1] = t.y;
     } else {
-#pragma unroll
-        for (int i = 0; i < BT; ++i) v[i] = ld_hot(p + i, pol);
+        v[0] = ld_hot(p, pol);
     }
 }
 
-template <int BT>
-__device__ __forceinline__ void scatter_add(float* __restrict__ p, float w, const float (&c)[BT]) {
-    if constexpr (BT % 4 == 0) {
-#pragma unroll
-        for (int i = 0; i < BT / 4; ++i)
-            atomicAdd(reinterpret_cast<float4*>(p) + i,
-                      make_float4(w * c[4 * i], w * c[4 * i + 1], w * c[4 * i + 2], w * c[4 * i + 3]));
+template <int VW>
+__device__ __forceinline__ void ld_plain(const float* __restrict__ p, float (&v)[VW]) {
+    if constexpr (VW == 4) {
+        const float4 t = *reinterpret_cast<const float4*>(p);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else if constexpr (VW == 2) {
+        const float2 t = *reinterpret_cast<const float2*>(p);
+        v[0] = t.x; v[1] = t.y;
     } else {
-#pragma unroll
-        for (int i = 0; i < BT; ++i) atomicAdd(p + i, w * c[i]);
+        v[0] = *p;
     }
 }
 
-// acc += v * vec[idx][f0 .. f0+BT) for the two elements of pair q, masking
-// elements outside [b, e).  k0 = global index of the pair's first element.
-// With p in [b>>1, (e+1)>>1): k0 < e and k0 + 1 >= b always hold.
-template <int BT>
-__device__ __forceinline__ void accum_pair(const uint4& q, uint64_t k0, uint64_t b, uint64_t e,
-                                           const float* __restrict__ vec, uint32_t B,
-                                           uint32_t f0, float (&acc)[BT], uint64_t pol) {
-    if (k0 >= b) {
-        float xv[BT];
-        gather<BT>(vec + (size_t)q.x * B + f0, xv, pol);
-        const float v = __uint_as_float(q.y);
-#pragma unroll
-        for (int i = 0; i < BT; ++i) acc[i] = fmaf(v, xv[i], acc[i]);
-    }
-    if (k0 + 1 < e) {
-        float xv[BT];
-        gather<BT>(vec + (size_t)q.z * B + f0, xv, pol);
-        const float v = __uint_as_float(q.w);
-#pragma unroll
-        for (int i = 0; i < BT; ++i) acc[i] = fmaf(v, xv[i], acc[i]);
+template <int VW>
+__device__ __forceinline__ void st_vec(float* __restrict__ p, const float (&v)[VW]) {
+    if constexpr (VW == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    else if constexpr (VW == 2) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    else *p = v[0];
+}
+
+template <int VW>
+__device__ __forceinline__ void ld_counts(const int32_t* __restrict__ p, int32_t (&v)[VW]) {
+    if constexpr (VW == 4) {
+        const int4 t = *reinterpret_cast<const int4*>(p);
+        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
+    } else if constexpr (VW == 2) {
+        const int2 t = *reinterpret_cast<const int2*>(p);
+        v[0] = t.x; v[1] = t.y;
+    } else {
+        v[0] = *p;
     }
 }
 
-// Dot products of one row (or column) against BT frames of `vec`.
+// u[...] += w * c[...] for VW floats (one vector reduction, 4..16 bytes).
+template <int VW>
+__device__ __forceinline__ void red_vec(float* __restrict__ p, float w, const float (&c)[VW]) {
+    if constexpr (VW == 4)
+        atomicAdd(reinterpret_cast<float4*>(p), make_float4(w * c[0], w * c[1], w * c[2], w * c[3]));
+    else if constexpr (VW == 2)
+        atomicAdd(reinterpret_cast<float2*>(p), make_float2(w * c[0], w * c[1]));
+    else
+        atomicAdd(p, w * c[0]);
+}
+
+// acc[0..VW) = sum over the row's elements of value * vec[col*B + off + ...].
 template <int G, int BT, bool KEEP>
-__device__ __forceinline__ void row_dot(const uint4* __restrict__ pairs, uint64_t b, uint64_t e,
+__device__ __forceinline__ void row_dot(const uint2* __restrict__ el, uint64_t b, uint64_t e,
                                         int lane, const float* __restrict__ vec, uint32_t B,
-                                        uint32_t f0, float (&acc)[BT], uint64_t ps,
+                                        uint32_t off, float (&acc)[Lanes<BT>::VW], uint64_t ps,
                                         uint64_t ph) {
+    constexpr int VW = Lanes<BT>::VW, FL = Lanes<BT>::FL, EPS = G / FL;
+    const float* base = vec + off;
 #pragma unroll
-    for (int i = 0; i < BT; ++i) acc[i] = 0.0f;
-    const uint64_t pend = (e + 1) >> 1;
-    uint64_t p = (b >> 1) + lane;
-    for (; p + 3 * G < pend; p += 4 * G) {
-        uint4 q[4];
+    for (int i = 0; i < VW; ++i) acc[i] = 0.0f;
+    uint64_t k = b + lane / FL;
+    for (; k + 3 * EPS < e; k += 4 * EPS) {
+        uint2 q[4];
 #pragma unroll
         for (int u = 0; u < 4; ++u)
-            q[u] = KEEP ? ld_keep(pairs + p + u * G, ps) : ld_stream(pairs + p + u * G, ps);
+            q[u] = KEEP ? ld_keep2(el + k + u * EPS, ps) : ld_stream2(el + k + u * EPS, ps);
 #pragma unroll
-        for (int u = 0; u < 4; ++u) accum_pair<BT>(q[u], 2 * (p + u * G), b, e, vec, B, f0, acc, ph);
+        for (int u = 0; u < 4; ++u) {
+            float xv[VW];
+            ld_vec<VW>(base + (size_t)q[u].x * B, xv, ph);
+            const float v = __uint_as_float(q[u].y);
+#pragma unroll
+            for (int i = 0; i < VW; ++i) acc[i] = fmaf(v, xv[i], acc[i]);
+        }
     }
-    for (; p < pend; p += G) {
-        uint4 q = KEEP ? ld_keep(pairs + p, ps) : ld_stream(pairs + p, ps);
-        accum_pair<BT>(q, 2 * p, b, e, vec, B, f0, acc, ph);
+    for (; k < e; k += EPS) {
+        const uint2 q = KEEP ? ld_keep2(el + k, ps) : ld_stream2(el + k, ps);
+        float xv[VW];
+        ld_vec<VW>(base + (size_t)q.x * B, xv, ph);
+        const float v = __uint_as_float(q.y);
+#pragma unroll
+        for (int i = 0; i < VW; ++i) acc[i] = fmaf(v, xv[i], acc[i]);
     }
 }
+
+// Sum over the element slots of the group: afterwards every lane holds the
+// row totals of its frames.  Every lane of the warp must call it.
+template <int G, int BT>
+__device__ __forceinline__ void slot_allreduce(float (&acc)[Lanes<BT>::VW]) {
+    constexpr int VW = Lanes<BT>::VW, FL = Lanes<BT>::FL;
+#pragma unroll
+    for (int o = FL; o < G; o <<= 1)
+#pragma unroll
+        for (int i = 0; i < VW; ++i) acc[i] += __shfl_xor_sync(MLEM_FULL_MASK, acc[i], o);
+}
+
+#define MLEM_WARP_LOOP_SETUP                                                     \
+    constexpr int RPW = 32 / G;                                                  \
+    constexpr int VW = Lanes<BT>::VW, FL = Lanes<BT>::FL;                        \
+    const int lw = threadIdx.x & 31;                                             \
+    const int lane = lw & (G - 1);                                               \
+    const int sub = lane % FL;                                                   \
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5; \
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;            \
+    const uint64_t ps = l2_evict_first(), ph = l2_evict_last();                  \
+    (void)VW;
 
 // ---------------------------------------------------------------------------
 // Forward projection (+ calcCorrel).
@@ -105,25 +162,27 @@ __global__ void __launch_bounds__(256) k_fwproj(SparseView csr, const float* __r
                                                 uint32_t B, uint32_t f0,
                                                 const int32_t* __restrict__ sino,
                                                 float* __restrict__ c, float* __restrict__ y) {
-    constexpr int RPW = 32 / G;
-    constexpr int SPAN = G / BT;
-    const int lw = threadIdx.x & 31;
-    const int lane = lw & (G - 1);
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    const uint64_t ps = l2_evict_first(), ph = l2_evict_last();
+    MLEM_WARP_LOOP_SETUP
+    const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
     for (uint64_t base = warp * RPW; base < csr.n; base += nwarps * RPW) {
         const uint64_t r = base + lw / G;
         const bool active = r < csr.n;
         uint64_t b = 0, e = 0;
         if (active) { b = csr.ptr[r]; e = csr.ptr[r + 1]; }
-        float acc[BT];
-        row_dot<G, BT, false>(csr.pairs, b, e, lane, x, B, f0, acc, ps, ph);
-        group_reduce_scatter<G, BT>(acc, lane);
-        if (active && (lane % SPAN) == 0) {
-            const uint64_t idx = r * B + f0 + lane / SPAN;
-            if (y) y[idx] = acc[0];
-            if (c) c[idx] = correl_of(sino[idx], acc[0]);
+        float acc[VW];
+        row_dot<G, BT, false>(el, b, e, lane, x, B, f0 + sub * VW, acc, ps, ph);
+        slot_allreduce<G, BT>(acc);
+        if (active && lane < FL) {
+            const uint64_t idx = r * B + f0 + sub * VW;
+            if (y) st_vec<VW>(y + idx, acc);
+            if (c) {
+                int32_t s[VW];
+                ld_counts<VW>(sino + idx, s);
+                float o[VW];
+#pragma unroll
+                for (int i = 0; i < VW; ++i) o[i] = correl_of(s[i], acc[i]);
+                st_vec<VW>(c + idx, o);
+            }
         }
     }
 }
@@ -136,25 +195,28 @@ __global__ void __launch_bounds__(256) k_bkproj_csc(SparseView csc, const float*
                                                     uint32_t B, uint32_t f0,
                                                     const float* __restrict__ norm,
                                                     float* __restrict__ x, float* __restrict__ u) {
-    constexpr int RPW = 32 / G;
-    constexpr int SPAN = G / BT;
-    const int lw = threadIdx.x & 31;
-    const int lane = lw & (G - 1);
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    const uint64_t ps = l2_evict_first(), ph = l2_evict_last();
+    MLEM_WARP_LOOP_SETUP
+    const uint2* el = reinterpret_cast<const uint2*>(csc.pairs);
     for (uint64_t base = warp * RPW; base < csc.n; base += nwarps * RPW) {
         const uint64_t col = base + lw / G;
         const bool active = col < csc.n;
         uint64_t b = 0, e = 0;
         if (active) { b = csc.ptr[col]; e = csc.ptr[col + 1]; }
-        float acc[BT];
-        row_dot<G, BT, false>(csc.pairs, b, e, lane, c, B, f0, acc, ps, ph);
-        group_reduce_scatter<G, BT>(acc, lane);
-        if (active && (lane % SPAN) == 0) {
-            const uint64_t idx = col * B + f0 + lane / SPAN;
-            if (norm) x[idx] *= update_factor(acc[0], norm[col]);
-            else u[idx] = acc[0];
+        float acc[VW];
+        row_dot<G, BT, false>(el, b, e, lane, c, B, f0 + sub * VW, acc, ps, ph);
+        slot_allreduce<G, BT>(acc);
+        if (active && lane < FL) {
+            const uint64_t idx = col * B + f0 + sub * VW;
+            if (norm) {
+                const float n = norm[col];
+                float xv[VW];
+                ld_plain<VW>(x + idx, xv);
+#pragma unroll
+                for (int i = 0; i < VW; ++i) xv[i] *= update_factor(acc[i], n);
+                st_vec<VW>(x + idx, xv);
+            } else {
+                st_vec<VW>(u + idx, acc);
+            }
         }
     }
 }
@@ -168,27 +230,23 @@ template <int G, int BT>
 __global__ void __launch_bounds__(256) k_bkproj_scatter(SparseView csr,
                                                         const float* __restrict__ c, uint32_t B,
                                                         uint32_t f0, float* __restrict__ u) {
-    constexpr int RPW = 32 / G;
-    const int lw = threadIdx.x & 31;
-    const int lane = lw & (G - 1);
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    const uint64_t ps = l2_evict_first(), ph = l2_evict_last();
+    MLEM_WARP_LOOP_SETUP
+    constexpr int EPS = G / FL;
+    const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
     for (uint64_t base = warp * RPW; base < csr.n; base += nwarps * RPW) {
         const uint64_t r = base + lw / G;
         if (r >= csr.n) continue;  // no shuffles in this kernel
         const uint64_t b = csr.ptr[r], e = csr.ptr[r + 1];
-        float cv[BT];
-        gather<BT>(c + r * B + f0, cv, ph);
+        float cv[VW];
+        ld_vec<VW>(c + r * B + f0 + sub * VW, cv, ph);
         bool any = false;
 #pragma unroll
-        for (int i = 0; i < BT; ++i) any |= (cv[i] != 0.0f);
+        for (int i = 0; i < VW; ++i) any |= (cv[i] != 0.0f);
         if (!any) continue;  // adding +0 changes no update entry
-        const uint64_t pend = (e + 1) >> 1;
-        for (uint64_t p = (b >> 1) + lane; p < pend; p += G) {
-            const uint4 q = ld_stream(csr.pairs + p, ps);
-            if (2 * p >= b) scatter_add<BT>(u + (size_t)q.x * B + f0, __uint_as_float(q.y), cv);
-            if (2 * p + 1 < e) scatter_add<BT>(u + (size_t)q.z * B + f0, __uint_as_float(q.w), cv);
+        float* ub = u + f0 + sub * VW;
+        for (uint64_t k = b + lane / FL; k < e; k += EPS) {
+            const uint2 q = ld_stream2(el + k, ps);
+            red_vec<VW>(ub + (size_t)q.x * B, __uint_as_float(q.y), cv);
         }
     }
 }
@@ -203,40 +261,38 @@ __global__ void __launch_bounds__(256) k_fused_row(SparseView csr, const float* 
                                                    uint32_t B, uint32_t f0,
                                                    const int32_t* __restrict__ sino,
                                                    float* __restrict__ u) {
-    constexpr int RPW = 32 / G;
-    constexpr int SPAN = G / BT;
-    const int lw = threadIdx.x & 31;
-    const int lane = lw & (G - 1);
-    const int gbase = lw & ~(G - 1);
-    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
-    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    const uint64_t ps = l2_evict_first(), ph = l2_evict_last();
+    MLEM_WARP_LOOP_SETUP
+    constexpr int EPS = G / FL;
+    const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
     for (uint64_t base = warp * RPW; base < csr.n; base += nwarps * RPW) {
         const uint64_t r = base + lw / G;
         const bool active = r < csr.n;
         uint64_t b = 0, e = 0;
         if (active) { b = csr.ptr[r]; e = csr.ptr[r + 1]; }
-        float acc[BT];
-        row_dot<G, BT, true>(csr.pairs, b, e, lane, x, B, f0, acc, ps, ph);
-        group_reduce_scatter<G, BT>(acc, lane);
-        float mine = 0.0f;
-        if (active && (lane % SPAN) == 0) mine = correl_of(sino[r * B + f0 + lane / SPAN], acc[0]);
-        float cv[BT];
+        float acc[VW];
+        row_dot<G, BT, true>(el, b, e, lane, x, B, f0 + sub * VW, acc, ps, ph);
+        slot_allreduce<G, BT>(acc);
+        if (!active) continue;
+        const uint64_t idx = r * B + f0 + sub * VW;
+        int32_t s[VW];
+        ld_counts<VW>(sino + idx, s);
+        float cv[VW];
         bool any = false;
 #pragma unroll
-        for (int i = 0; i < BT; ++i) {
-            cv[i] = __shfl_sync(MLEM_FULL_MASK, mine, gbase + i * SPAN);
+        for (int i = 0; i < VW; ++i) {
+            cv[i] = correl_of(s[i], acc[i]);
             any |= (cv[i] != 0.0f);
         }
         if (!any) continue;
-        const uint64_t pend = (e + 1) >> 1;
-        for (uint64_t p = (b >> 1) + lane; p < pend; p += G) {
-            const uint4 q = ld_keep(csr.pairs + p, ps);
-            if (2 * p >= b) scatter_add<BT>(u + (size_t)q.x * B + f0, __uint_as_float(q.y), cv);
-            if (2 * p + 1 < e) scatter_add<BT>(u + (size_t)q.z * B + f0, __uint_as_float(q.w), cv);
+        float* ub = u + f0 + sub * VW;
+        for (uint64_t k = b + lane / FL; k < e; k += EPS) {
+            const uint2 q = ld_keep2(el + k, ps);
+            red_vec<VW>(ub + (size_t)q.x * B, __uint_as_float(q.y), cv);
         }
     }
 }
+
+#undef MLEM_WARP_LOOP_SETUP
 
 template <bool ONE_FRAME>
 __global__ void k_apply_update(float* __restrict__ x, float* __restrict__ u,
@@ -367,10 +423,10 @@ cudaError_t dispatch_bt(const LaunchCfg& cfg, cudaStream_t st, Args... args) {
     const int grid = grid_for(cfg);
     switch (cfg.frame_tile) {
         case 1: K<G, 1>::run(grid, st, args...); break;
-        case 2: if constexpr (G >= 2) { K<G, 2>::run(grid, st, args...); break; } else return cudaErrorInvalidValue;
-        case 4: if constexpr (G >= 4) { K<G, 4>::run(grid, st, args...); break; } else return cudaErrorInvalidValue;
-        case 8: if constexpr (G >= 8) { K<G, 8>::run(grid, st, args...); break; } else return cudaErrorInvalidValue;
-        case 16: if constexpr (G >= 16) { K<G, 16>::run(grid, st, args...); break; } else return cudaErrorInvalidValue;
+        case 2: K<G, 2>::run(grid, st, args...); break;
+        case 4: K<G, 4>::run(grid, st, args...); break;
+        case 8: K<G, 8>::run(grid, st, args...); break;
+        case 16: K<G, 16>::run(grid, st, args...); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();
@@ -393,8 +449,8 @@ bool cfg_valid(const LaunchCfg& c) {
     const bool g = c.group == 4 || c.group == 8 || c.group == 16 || c.group == 32;
     const bool t = c.frame_tile == 1 || c.frame_tile == 2 || c.frame_tile == 4 ||
                    c.frame_tile == 8 || c.frame_tile == 16;
-    return g && t && c.frame_tile <= c.group && c.blocks_per_sm >= 1 && c.blocks_per_sm <= 8 &&
-           c.sm_count >= 1;
+    // lanes per element (frame_tile / min(frame_tile, 4)) never exceed the group
+    return g && t && c.blocks_per_sm >= 1 && c.blocks_per_sm <= 8 && c.sm_count >= 1;
 }
 
 cudaError_t fwproj(const SparseView& csr, const float* x, uint32_t B, uint32_t f0,

@@ -282,24 +282,46 @@ __global__ void k_correl(const float* __restrict__ f, const int32_t* __restrict_
 
 template <typename T>
 __global__ void k_interleave(const T* __restrict__ in, T* __restrict__ out, uint64_t n, uint32_t B,
-                             uint32_t Bp) {
+                             uint32_t Bp, const uint32_t* __restrict__ perm) {
     const uint64_t total = n * B;
     for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < total;
          j += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t b = j / n, i = j - b * n;
-        out[i * Bp + b] = in[j];
+        const uint64_t d = perm ? perm[i] : i;
+        out[d * Bp + b] = in[j];
     }
 }
 
 template <typename T>
 __global__ void k_deinterleave(const T* __restrict__ in, T* __restrict__ out, uint64_t n,
-                               uint32_t B, uint32_t Bp) {
+                               uint32_t B, uint32_t Bp, const uint32_t* __restrict__ perm) {
     const uint64_t total = n * B;
     for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < total;
          j += (uint64_t)gridDim.x * blockDim.x) {
         const uint64_t b = j / n, i = j - b * n;
-        out[j] = in[i * Bp + b];
+        const uint64_t d = perm ? perm[i] : i;
+        out[j] = in[d * Bp + b];
     }
+}
+
+template <bool TO_DEVICE>
+__global__ void k_permute(const float* __restrict__ in, float* __restrict__ out,
+                          const uint32_t* __restrict__ perm, uint64_t n, uint32_t B) {
+    const uint64_t total = n * B;
+    for (uint64_t j = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; j < total;
+         j += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t i = j / B, b = j - i * B;
+        const uint64_t d = (uint64_t)perm[i] * B + b;
+        if (TO_DEVICE) out[d] = in[j];
+        else out[j] = in[d];
+    }
+}
+
+__global__ void k_remap_columns(uint2* __restrict__ el, uint64_t nnz,
+                                const uint32_t* __restrict__ perm) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < nnz;
+         k += (uint64_t)gridDim.x * blockDim.x)
+        el[k].x = perm[el[k].x];
 }
 
 __global__ void k_fill(float* __restrict__ p, float v, uint64_t n) {
@@ -512,21 +534,41 @@ static unsigned elementwise_grid(uint64_t n) {
 cudaError_t interleave_i32(const int32_t* in, int32_t* out, uint64_t n, uint32_t B, uint32_t Bp,
                            cudaStream_t st) {
     if (n * B == 0) return cudaSuccess;
-    k_interleave<int32_t><<<elementwise_grid(n * B), 256, 0, st>>>(in, out, n, B, Bp);
+    k_interleave<int32_t><<<elementwise_grid(n * B), 256, 0, st>>>(in, out, n, B, Bp, nullptr);
     return cudaGetLastError();
 }
 
 cudaError_t interleave_f32(const float* in, float* out, uint64_t n, uint32_t B, uint32_t Bp,
-                           cudaStream_t st) {
+                           const uint32_t* perm, cudaStream_t st) {
     if (n * B == 0) return cudaSuccess;
-    k_interleave<float><<<elementwise_grid(n * B), 256, 0, st>>>(in, out, n, B, Bp);
+    k_interleave<float><<<elementwise_grid(n * B), 256, 0, st>>>(in, out, n, B, Bp, perm);
     return cudaGetLastError();
 }
 
 cudaError_t deinterleave_f32(const float* in, float* out, uint64_t n, uint32_t B, uint32_t Bp,
-                             cudaStream_t st) {
+                             const uint32_t* perm, cudaStream_t st) {
     if (n * B == 0) return cudaSuccess;
-    k_deinterleave<float><<<elementwise_grid(n * B), 256, 0, st>>>(in, out, n, B, Bp);
+    k_deinterleave<float><<<elementwise_grid(n * B), 256, 0, st>>>(in, out, n, B, Bp, perm);
+    return cudaGetLastError();
+}
+
+cudaError_t permute_to_device(const float* in, float* out, const uint32_t* perm, uint64_t n,
+                              uint32_t B, cudaStream_t st) {
+    if (n * B == 0) return cudaSuccess;
+    k_permute<true><<<elementwise_grid(n * B), 256, 0, st>>>(in, out, perm, n, B);
+    return cudaGetLastError();
+}
+
+cudaError_t permute_to_natural(const float* in, float* out, const uint32_t* perm, uint64_t n,
+                               uint32_t B, cudaStream_t st) {
+    if (n * B == 0) return cudaSuccess;
+    k_permute<false><<<elementwise_grid(n * B), 256, 0, st>>>(in, out, perm, n, B);
+    return cudaGetLastError();
+}
+
+cudaError_t remap_columns(uint2* elems, uint64_t nnz, const uint32_t* perm, cudaStream_t st) {
+    if (nnz == 0) return cudaSuccess;
+    k_remap_columns<<<elementwise_grid(nnz), 256, 0, st>>>(elems, nnz, perm);
     return cudaGetLastError();
 }
 

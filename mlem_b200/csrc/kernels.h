@@ -30,7 +30,7 @@ struct LaunchCfg {
     int sm_count = 148;
 };
 
-// Valid (group, frame_tile) pairs: frame_tile <= group.
+// Valid launch configuration (group 4..32, frame tile 1..16, 1..8 blocks/SM).
 bool cfg_valid(const LaunchCfg& c);
 
 // ---- forward projection -------------------------------------------------
@@ -80,14 +80,23 @@ cudaError_t image_stats(const float* x, uint32_t C, uint32_t B, uint32_t n_out, 
                         unsigned long long* subnormals, cudaStream_t st);
 
 // ---- layout helpers -------------------------------------------------------
-// out[i*Bp + b] = in[b*n + i] for b < B (n items per frame; pad frames
-// untouched), and back: out[b*n + i] = in[i*Bp + b].
+// out[p(i)*Bp + b] = in[b*n + i] for b < B (n items per frame; pad frames
+// untouched), and back: out[b*n + i] = in[p(i)*Bp + b], where p = perm
+// (natural -> device order) or the identity when perm is null.
 cudaError_t interleave_i32(const int32_t* in, int32_t* out, uint64_t n, uint32_t B, uint32_t Bp,
                            cudaStream_t st);
 cudaError_t interleave_f32(const float* in, float* out, uint64_t n, uint32_t B, uint32_t Bp,
-                           cudaStream_t st);
+                           const uint32_t* perm, cudaStream_t st);
 cudaError_t deinterleave_f32(const float* in, float* out, uint64_t n, uint32_t B, uint32_t Bp,
-                             cudaStream_t st);
+                             const uint32_t* perm, cudaStream_t st);
+// Interleaved [n][B] vectors between natural and device voxel order:
+// to_device: out[perm[i]*B + b] = in[i*B + b]; to_natural: out[i*B + b] = in[perm[i]*B + b].
+cudaError_t permute_to_device(const float* in, float* out, const uint32_t* perm, uint64_t n,
+                              uint32_t B, cudaStream_t st);
+cudaError_t permute_to_natural(const float* in, float* out, const uint32_t* perm, uint64_t n,
+                               uint32_t B, cudaStream_t st);
+// Relabel the column (voxel) index of every element: e.x = perm[e.x].
+cudaError_t remap_columns(uint2* elems, uint64_t nnz, const uint32_t* perm, cudaStream_t st);
 cudaError_t fill_f32(float* p, float v, uint64_t n, cudaStream_t st);
 // x[i][b] = b < B ? vals[b] : 0 for the Bp-interleaved image (vals: device, B floats).
 cudaError_t fill_frames(float* x, uint64_t n, uint32_t Bp, uint32_t B, const float* vals,

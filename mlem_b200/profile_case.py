@@ -26,10 +26,13 @@ def main(argv=None):
     ap.add_argument("--blocks-per-sm", type=int, default=8)
     ap.add_argument("--frames", type=int, default=1)
     ap.add_argument("--iters", type=int, default=3)
+    ap.add_argument("--natural", action="store_true", help="keep the natural voxel order")
     a = ap.parse_args(argv)
     nx, ny, nz = a.grid
     g = synth.Geometry(nx, ny, nz, a.rows, a.count[0], a.count[1], seed=a.seed)
     flags = api.FLAG_EXACT if a.mode == "exact" else 0
+    if a.natural:
+        flags |= api.FLAG_NATURAL_LAYOUT
     with api.Context.siddon(g, flags=flags) as ctx:
         w = synth.Workload("profile", g, a.frames, a.iters, 0, (3, 12), (1e6, 1e9), 9000)
         fr = synth.make_frames(w, ctx.project_f64)
@@ -41,6 +44,8 @@ def main(argv=None):
         ctx.init_images()
         ms, by, ln = ctx.profile_phases(a.iters)
         print(json.dumps({"nnz": int(ctx.nnz), "mode": a.mode, "frames": a.frames,
+                          "layout": "natural" if a.natural else "brick", "group": a.group,
+                          "frame_tile": a.frame_tile, "blocks_per_sm": a.blocks_per_sm,
                           "phase_ms": [round(float(x), 4) for x in ms],
                           "phase_GBps": [round(float(b / (t / 1e3) / 1e9), 1) if t > 0 else 0
                                          for b, t in zip(by, ms)]}))

@@ -226,3 +226,39 @@ def test_autotune_restores_images(ctxs):
     assert ctx.get_images().tobytes() == before.tobytes()
     ctx.iterate(iters)
     assert ob.rel_l2(ctx.get_images()[0], gold) <= TOL_MLEM
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_brick_layout_changes_no_result(golden, name):
+    """The device brick layout only relabels voxels: CSC-mode images, the
+    CSR/CSC copies and the column sums are bit-identical to natural order."""
+    m, sino, iters, gold, _ = golden.case(name)
+    out = []
+    for flags in (0, api.FLAG_NATURAL_LAYOUT):
+        with api.Context.from_matrix(m, flags=flags) as ctx:
+            ctx.set_sinograms(sino)
+            ctx.set_tuning(bk_mode=api.BK_CSC, group=32, frame_tile=1, blocks_per_sm=8)
+            ctx.init_images()
+            ctx.iterate(iters)
+            out.append((ctx.get_images().tobytes(), ctx.column_sums().tobytes(),
+                        ctx.csc()[1].tobytes(), ctx.csr()[1].tobytes()))
+    assert out[0] == out[1]
+
+
+def test_device_pointer_api_in_natural_order(small_ctx=None):
+    torch = pytest.importorskip("torch")
+    g = synth.Geometry(16, 16, 8, 3000, 5, 40, seed=3)
+    hm = synth.host_matrix(g)
+    x = torch.rand(hm.n_cols, device="cuda")
+    res = []
+    for flags in (0, api.FLAG_NATURAL_LAYOUT):
+        with api.Context.from_matrix(hm, flags=flags) as ctx:
+            y = torch.empty(hm.n_rows, device="cuda")
+            ctx.fwproj_d(x.data_ptr(), y.data_ptr(), 1, torch.cuda.current_stream().cuda_stream)
+            xb = torch.empty(hm.n_cols, device="cuda")
+            ctx.bkproj_d(y.data_ptr(), xb.data_ptr(), 1, torch.cuda.current_stream().cuda_stream)
+            torch.cuda.synchronize()
+            res.append((y.cpu().numpy().tobytes(), xb.cpu().numpy().tobytes()))
+    assert res[0] == res[1]
+    want = ob.fwproj(hm, x.cpu().numpy())
+    assert ob.rel_l2(np.frombuffer(res[0][0], np.float32), want) < TOL_PROJ
