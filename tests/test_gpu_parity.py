@@ -213,7 +213,9 @@ def test_invalid_inputs_raise():
             ctx.iterate(1)
         assert e.value.status == api.MLEM_ERR_STATE
         with pytest.raises(api.MlemError):
-            ctx.set_tuning(bk_mode=api.BK_CSC, group=4, frame_tile=8)
+            ctx.set_tuning(bk_mode=api.BK_CSC, group=6, frame_tile=1)
+        with pytest.raises(api.MlemError):
+            ctx.set_tuning(bk_mode=api.BK_CSC, group=32, frame_tile=3)
 
 
 def test_autotune_restores_images(ctxs):
