@@ -404,6 +404,20 @@ def mlem(matrix: Context, lmsino, image: Optional[np.ndarray] = None, nIteration
     return out, sums
 
 
+NOALLOC_MAX_VOXELS = 1048576
+
+
+def iterate_noalloc_d(row_ptr: int, elems: int, n_rows: int, n_cols: int, sino: int, norm: int,
+                      image: int, stream: int = 0) -> None:
+    """mlem_iterate_noalloc_d: one MLEM iteration on caller-owned device
+    buffers (integer device addresses) for callers that cannot let the
+    library allocate device memory; its update vector lives in a fixed
+    4 MiB static device array (at most NOALLOC_MAX_VOXELS voxels), shared by
+    all calls on a device, so overlapping calls race."""
+    _raise(core_lib().mlem_iterate_noalloc_d(row_ptr, elems, n_rows, n_cols, sino, norm, image,
+                                             stream or None))
+
+
 # ---------------------------------------------------------------------------
 # Host IO through the C ABI (the command-line driver's code path).
 # ---------------------------------------------------------------------------
