@@ -97,39 +97,60 @@ __device__ __forceinline__ void red_vec(float* __restrict__ p, float w, const fl
         atomicAdd(p, w * c[0]);
 }
 
+// Elements a lane loads before it gathers (memory-level parallelism).  A
+// full-warp group takes 8 (a 150-250-element row is one batch); narrower
+// groups take 4, which keeps their registers, and so their occupancy, lower
+// (measured on the plain-full workload).
+template <int G>
+constexpr int batch_depth() { return G == 32 ? 8 : 4; }
+
 // acc[0..VW) = sum over the row's elements of value * vec[col*B + off + ...].
+// Each batch issues all of its (predicated) element loads, then all of its
+// gathers, so a row costs about two memory latencies per batch instead of
+// two per element.  When `keep` is non-null and the whole row fits in one
+// batch, the lane's elements are left in keep[] (fused kernel) and true is
+// returned.
 template <int G, int BT, bool KEEP>
-__device__ __forceinline__ void row_dot(const uint2* __restrict__ el, uint64_t b, uint64_t e,
+__device__ __forceinline__ bool row_dot(const uint2* __restrict__ el, uint64_t b, uint64_t e,
                                         int lane, const float* __restrict__ vec, uint32_t B,
                                         uint32_t off, float (&acc)[Lanes<BT>::VW], uint64_t ps,
-                                        uint64_t ph) {
+                                        uint64_t ph, uint2* keep = nullptr) {
     constexpr int VW = Lanes<BT>::VW, FL = Lanes<BT>::FL, EPS = G / FL;
+    constexpr int kBatch = batch_depth<G>();
     const float* base = vec + off;
 #pragma unroll
     for (int i = 0; i < VW; ++i) acc[i] = 0.0f;
-    uint64_t k = b + lane / FL;
-    for (; k + 3 * EPS < e; k += 4 * EPS) {
-        uint2 q[4];
+    const bool one_batch = e - b <= (uint64_t)kBatch * EPS;
+    for (uint64_t k0 = b + lane / FL; k0 < e; k0 += (uint64_t)kBatch * EPS) {
+        uint2 q[kBatch];
 #pragma unroll
-        for (int u = 0; u < 4; ++u)
-            q[u] = KEEP ? ld_keep2(el + k + u * EPS, ps) : ld_stream2(el + k + u * EPS, ps);
+        for (int u = 0; u < kBatch; ++u) {
+            const uint64_t k = k0 + (uint64_t)u * EPS;
+            q[u] = make_uint2(0u, 0u);  // value 0: contributes nothing
+            if (k < e) q[u] = KEEP ? ld_keep2(el + k, ps) : ld_stream2(el + k, ps);
+        }
+        float xv[kBatch][VW];
 #pragma unroll
-        for (int u = 0; u < 4; ++u) {
-            float xv[VW];
-            ld_vec<VW>(base + (size_t)q[u].x * B, xv, ph);
+        for (int u = 0; u < kBatch; ++u) {
+            if (k0 + (uint64_t)u * EPS < e) {
+                ld_vec<VW>(base + (size_t)q[u].x * B, xv[u], ph);
+            } else {
+#pragma unroll
+                for (int i = 0; i < VW; ++i) xv[u][i] = 0.0f;
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
             const float v = __uint_as_float(q[u].y);
 #pragma unroll
-            for (int i = 0; i < VW; ++i) acc[i] = fmaf(v, xv[i], acc[i]);
+            for (int i = 0; i < VW; ++i) acc[i] = fmaf(v, xv[u][i], acc[i]);
+        }
+        if (keep && one_batch) {
+#pragma unroll
+            for (int u = 0; u < kBatch; ++u) keep[u] = q[u];
         }
     }
-    for (; k < e; k += EPS) {
-        const uint2 q = KEEP ? ld_keep2(el + k, ps) : ld_stream2(el + k, ps);
-        float xv[VW];
-        ld_vec<VW>(base + (size_t)q.x * B, xv, ph);
-        const float v = __uint_as_float(q.y);
-#pragma unroll
-        for (int i = 0; i < VW; ++i) acc[i] = fmaf(v, xv[i], acc[i]);
-    }
+    return one_batch;
 }
 
 // Sum over the element slots of the group: afterwards every lane holds the
@@ -270,7 +291,10 @@ __global__ void __launch_bounds__(256) k_fused_row(SparseView csr, const float* 
         uint64_t b = 0, e = 0;
         if (active) { b = csr.ptr[r]; e = csr.ptr[r + 1]; }
         float acc[VW];
-        row_dot<G, BT, true>(el, b, e, lane, x, B, f0 + sub * VW, acc, ps, ph);
+        constexpr int kBatch = batch_depth<G>();
+        uint2 kept[kBatch];
+        const bool in_regs =
+            row_dot<G, BT, true>(el, b, e, lane, x, B, f0 + sub * VW, acc, ps, ph, kept);
         slot_allreduce<G, BT>(acc);
         if (!active) continue;
         const uint64_t idx = r * B + f0 + sub * VW;
@@ -285,9 +309,17 @@ __global__ void __launch_bounds__(256) k_fused_row(SparseView csr, const float* 
         }
         if (!any) continue;
         float* ub = u + f0 + sub * VW;
-        for (uint64_t k = b + lane / FL; k < e; k += EPS) {
-            const uint2 q = ld_keep2(el + k, ps);
-            red_vec<VW>(ub + (size_t)q.x * B, __uint_as_float(q.y), cv);
+        if (in_regs) {
+            // the whole row is still in registers: scatter from there
+#pragma unroll
+            for (int q = 0; q < kBatch; ++q)
+                if (b + lane / FL + (uint64_t)q * EPS < e)
+                    red_vec<VW>(ub + (size_t)kept[q].x * B, __uint_as_float(kept[q].y), cv);
+        } else {
+            for (uint64_t k = b + lane / FL; k < e; k += EPS) {
+                const uint2 q = ld_keep2(el + k, ps);
+                red_vec<VW>(ub + (size_t)q.x * B, __uint_as_float(q.y), cv);
+            }
         }
     }
 }

@@ -242,22 +242,32 @@ __global__ void __launch_bounds__(kStatsThreads) k_stats(const float* __restrict
     }
 }
 
+// One warp per frame: lanes take the block partials in a fixed stride, then a
+// fixed butterfly combines the lanes -- the same order on every call.
 __global__ void k_stats_final(const double* __restrict__ ps, const unsigned long long* __restrict__ pz,
                               const unsigned long long* __restrict__ pn, uint32_t nblocks,
                               uint32_t B, uint32_t n_out, unsigned int* __restrict__ slot,
                               double* __restrict__ sums, unsigned long long* __restrict__ zeros,
                               unsigned long long* __restrict__ subn) {
-    // single block; frames strided over its threads
     const uint64_t row = slot ? *slot : 0;
-    for (uint32_t f = threadIdx.x; f < n_out; f += blockDim.x) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (uint32_t f = w; f < n_out; f += nw) {
         double a = 0.0;
         unsigned long long b = 0, c = 0;
-        for (uint32_t k = 0; k < nblocks; ++k) {
+        for (uint32_t k = lane; k < nblocks; k += 32) {
             a += ps[(uint64_t)k * B + f]; b += pz[(uint64_t)k * B + f]; c += pn[(uint64_t)k * B + f];
         }
-        if (sums) sums[row * n_out + f] = a;
-        if (zeros) zeros[row * n_out + f] = b;
-        if (subn) subn[row * n_out + f] = c;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            a += __shfl_xor_sync(MLEM_FULL_MASK, a, o);
+            b += __shfl_xor_sync(MLEM_FULL_MASK, b, o);
+            c += __shfl_xor_sync(MLEM_FULL_MASK, c, o);
+        }
+        if (lane == 0) {
+            if (sums) sums[row * n_out + f] = a;
+            if (zeros) zeros[row * n_out + f] = b;
+            if (subn) subn[row * n_out + f] = c;
+        }
     }
     __syncthreads();
     if (slot && threadIdx.x == 0) *slot = (unsigned int)row + 1;
@@ -522,7 +532,7 @@ cudaError_t image_stats(const float* x, uint32_t C, uint32_t B, uint32_t n_out, 
     }
     cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return err;
-    k_stats_final<<<1, 128, 0, st>>>(ps, pz, pn, kStatsBlocks, B, n_out, slot, sums, zeros,
+    k_stats_final<<<1, 512, 0, st>>>(ps, pz, pn, kStatsBlocks, B, n_out, slot, sums, zeros,
                                      subnormals);
     return cudaGetLastError();
 }
