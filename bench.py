@@ -46,7 +46,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--mode", choices=["auto", "csc", "atomic", "fused"], default="auto",
+    ap.add_argument("--mode", choices=["auto", "csc", "atomic", "fused", "region"], default="auto",
                     help="back-projection method; auto = autotuned")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -203,7 +203,8 @@ def run_ours(a, rank, world, local_rank):
     ctx.set_sinograms(frames.sinograms)
     ctx.init_images()
 
-    mode_map = {"csc": api.BK_CSC, "atomic": api.BK_ATOMIC, "fused": api.BK_FUSED}
+    mode_map = {"csc": api.BK_CSC, "atomic": api.BK_ATOMIC, "fused": api.BK_FUSED,
+                "region": api.BK_REGION}
     if a.mode == "auto":
         tuning = ctx.autotune()
     else:
@@ -270,6 +271,7 @@ def run_ours(a, rank, world, local_rank):
         api.BK_CSC: ("k_fwproj", "k_bkproj_csc", "-", "k_stats"),
         api.BK_ATOMIC: ("k_fwproj", "k_bkproj_scatter", "k_apply_update", "k_stats"),
         api.BK_FUSED: ("k_fused_row", "-", "k_apply_update", "k_stats"),
+        api.BK_REGION: ("k_rb_fwproj", "k_rb_bkproj", "-", "k_stats"),
     }[tuning["bk_mode"]]
     traffic = committed_traffic().get(kernel_names[dom])
     achieved = ph_bytes[dom] / (ph_ms[dom] / 1e3) / 1e9

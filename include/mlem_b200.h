@@ -63,6 +63,7 @@ extern "C" {
 #define MLEM_BK_CSC 1     /* gather over the device CSC copy, fused with calcUpdate (deterministic) */
 #define MLEM_BK_ATOMIC 2  /* atomic scatter over the CSR (reference GPU drivers' method) */
 #define MLEM_BK_FUSED 3   /* one pass per row: fwproj, correl and atomic scatter together */
+#define MLEM_BK_REGION 4  /* region-blocked copy: shared-memory image/update tiles per region */
 
 typedef struct mlem_ctx mlem_ctx;
 
@@ -79,9 +80,11 @@ typedef struct {
     uint64_t device_bytes; /* device memory held by the context */
 } mlem_info;
 
-/* Launch configuration chosen by the autotuner (or set by the caller). */
+/* Launch configuration chosen by the autotuner (or set by the caller).
+ * MLEM_BK_REGION builds its region-blocked copy of the matrix (about the
+ * size of the CSR) when it is first selected for a frame tile. */
 typedef struct {
-    int bk_mode;        /* MLEM_BK_CSC, MLEM_BK_ATOMIC or MLEM_BK_FUSED */
+    int bk_mode;        /* MLEM_BK_CSC, MLEM_BK_ATOMIC, MLEM_BK_FUSED or MLEM_BK_REGION */
     int group;          /* lanes per row/column: 4, 8, 16 or 32 */
     int frame_tile;     /* frames per pass over the matrix: 1, 2, 4, 8 or 16 */
     int blocks_per_sm;  /* 1..8 blocks of 256 threads per SM */
@@ -102,8 +105,9 @@ int mlem_create(mlem_ctx** out, const uint64_t* row_end, const void* elems, uint
                 uint32_t n_cols, uint64_t nnz, uint32_t flags, int device);
 
 /* Same, with the voxel grid (nx, ny, nz; nx*ny*nz == n_cols): the device
- * then stores the image in 8x8x8 bricks (Morton order inside), which keeps a
- * ray's voxels in few cache lines.  Only the device layout changes; every
+ * then stores the image along a Morton (Z-order) curve over the whole grid,
+ * which keeps a ray's voxels in few cache lines (every 2x2x2 cube in one
+ * 32-byte sector).  Only the device layout changes; every
  * host- and device-pointer interface keeps the natural voxel order
  * ix + nx*(iy + ny*iz) (helper_files_common/scannerconfig.cpp getVoxelNr)
  * and every result is unchanged.  grid == NULL: natural order. */
@@ -247,6 +251,59 @@ int mlem_project_f64(mlem_ctx* ctx, const float* x, double* out);
 int mlem_iterate_noalloc_d(const uint64_t* row_ptr, const void* elems, uint32_t n_rows,
                            uint32_t n_cols, const int32_t* sino, const float* norm, float* image,
                            void* stream);
+
+/* ---- uneven multi-matrix batches ----------------------------------------
+ * No counterpart in the reference, which reconstructs one matrix per process
+ * (seqcsr4mlem.cpp:137-189).  A batch iterates several contexts (different
+ * scanner matrices, different frame counts) together on one GPU.  Each
+ * iteration runs ONE kernel over the rows of all matrices, then a per-matrix
+ * calcUpdate and the image statistics; up to 64 iterations are captured as
+ * one graph.  Every row does the one-pass fwproj + correl + scatter for all
+ * frames of its matrix, in passes of one frame tile shared by the batch.  Two
+ * schedules share the rows out:
+ *   MLEM_BATCH_INTERLEAVED -- the rows of all matrices form one virtual row
+ *     space that the warps walk in grid-stride order, so every warp gets an
+ *     equal share of every matrix and a small matrix fills the tail of a
+ *     large one;
+ *   MLEM_BATCH_ITEMS -- the rows are cut into work items of about equal cost
+ *     (full items of the costliest matrix first, ragged remainders last,
+ *     heaviest first) that persistent blocks take from a shared counter.
+ *
+ * All contexts must live on the same device, be created without
+ * MLEM_FLAG_EXACT, and have sinograms and images set.  The batch enqueues on
+ * the first context's stream and waits for the others'; the contexts stay
+ * usable (mlem_get_images, ...) and must outlive the batch.  Results equal
+ * each context's own MLEM_BK_FUSED iterations up to float rounding (the
+ * scatter order differs). */
+typedef struct mlem_batch mlem_batch;
+#define MLEM_BATCH_MAX_MATRICES 64
+#define MLEM_BATCH_INTERLEAVED 0
+#define MLEM_BATCH_ITEMS 1
+int mlem_batch_create(mlem_batch** out, mlem_ctx* const* ctxs, uint32_t n_ctx);
+void mlem_batch_destroy(mlem_batch* b);
+const char* mlem_batch_last_error(const mlem_batch* b);
+/* policy: MLEM_BATCH_INTERLEAVED or MLEM_BATCH_ITEMS; items_per_block (1..1024,
+ * items schedule): about that many items for every resident block
+ * (blocks_per_sm x SMs); frame_tile in {1,2,4,8,16} dividing every context's
+ * padded frame count (0 keeps the current tile). */
+int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
+                            int blocks_per_sm, int frame_tile);
+/* Current schedule; any pointer may be NULL.  n_items: 0 for the interleaved
+ * schedule.  ms_per_iter: from the last autotune, else 0. */
+int mlem_batch_get_schedule(const mlem_batch* b, int* policy, uint32_t* items_per_block,
+                            int* blocks_per_sm, int* frame_tile, uint32_t* n_items,
+                            double* ms_per_iter);
+/* Time real iterations over schedules, frame tiles and resident blocks and
+ * keep the fastest; the images are restored afterwards. */
+int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter);
+/* n iterations of every context.  sums may be NULL, or hold n_ctx pointers
+ * (each NULL or n x n_frames doubles, iteration-major) for the image sums. */
+int mlem_batch_iterate(mlem_batch* b, int n, double* const* sums);
+/* Like mlem_profile_phases for the whole batch: ms[0] = the multi-matrix
+ * kernel, ms[2] = the calcUpdate launches, ms[3] = the statistics, averaged
+ * over n iterations; bytes[] are the algorithmic bytes of each phase summed
+ * over the contexts. */
+int mlem_batch_profile(mlem_batch* b, int n, double* ms, double* bytes, int* launches);
 
 /* ---- host IO: the reference's file formats ------------------------------ */
 typedef struct {

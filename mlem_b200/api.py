@@ -39,8 +39,10 @@ FLAG_NO_CSC = 0x2
 FLAG_CHECKED = 0x4
 FLAG_NATURAL_LAYOUT = 0x8
 
-BK_AUTO, BK_CSC, BK_ATOMIC, BK_FUSED = 0, 1, 2, 3
-BK_NAMES = {BK_CSC: "csc", BK_ATOMIC: "atomic", BK_FUSED: "fused"}
+BK_AUTO, BK_CSC, BK_ATOMIC, BK_FUSED, BK_REGION = 0, 1, 2, 3, 4
+BATCH_INTERLEAVED, BATCH_ITEMS = 0, 1
+BATCH_NAMES = {BATCH_INTERLEAVED: "interleaved", BATCH_ITEMS: "items"}
+BK_NAMES = {BK_CSC: "csc", BK_ATOMIC: "atomic", BK_FUSED: "fused", BK_REGION: "region"}
 
 ELEM_DTYPE = np.dtype([("index", "<u4"), ("value", "<f4")])
 
@@ -333,9 +335,87 @@ class Context:
 
 
 # ---------------------------------------------------------------------------
+# Uneven multi-matrix batches.
+class Batch:
+    """Several contexts (uneven matrices and frame counts) iterated together:
+    one persistent kernel per iteration takes row work items of all matrices
+    from a shared counter (mlem_batch_*; no counterpart in the reference,
+    which runs one matrix per process, mlem_seq/seqcsr4mlem.cpp:137-189).
+
+    The contexts keep their own images: read them with ctx.get_images().
+    They must outlive the batch."""
+
+    def __init__(self, contexts: Sequence[Context]):
+        self.contexts = list(contexts)
+        arr = (ctypes.c_void_p * len(self.contexts))(*[c.handle for c in self.contexts])
+        h = ctypes.c_void_p()
+        _raise(core_lib().mlem_batch_create(ctypes.byref(h), arr, len(self.contexts)))
+        self._h = h.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            core_lib().mlem_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _chk(self, st):
+        if st != MLEM_OK:
+            raise MlemError(st, core_lib().mlem_batch_last_error(self._h).decode(errors="replace"))
+
+    def set_schedule(self, policy: int = BATCH_INTERLEAVED, items_per_block: int = 4,
+                     blocks_per_sm: int = 4, frame_tile: int = 0) -> None:
+        self._chk(core_lib().mlem_batch_set_schedule(self._h, policy, items_per_block,
+                                                     blocks_per_sm, frame_tile))
+
+    def schedule(self) -> dict:
+        pol, ipb, bps = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_int()
+        tile, n, ms = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_double()
+        self._chk(core_lib().mlem_batch_get_schedule(self._h, ctypes.byref(pol), ctypes.byref(ipb),
+                                                     ctypes.byref(bps), ctypes.byref(tile),
+                                                     ctypes.byref(n), ctypes.byref(ms)))
+        return dict(policy=pol.value, items_per_block=ipb.value, blocks_per_sm=bps.value,
+                    frame_tile=tile.value, n_items=n.value, ms_per_iter=ms.value)
+
+    def autotune(self) -> dict:
+        ms = ctypes.c_double()
+        self._chk(core_lib().mlem_batch_autotune(self._h, ctypes.byref(ms)))
+        return self.schedule()
+
+    def iterate(self, n: int, stats: bool = True):
+        """n iterations of every context; returns one [n, B_i] array of image
+        sums per context (None without stats)."""
+        if not stats:
+            self._chk(core_lib().mlem_batch_iterate(self._h, n, None))
+            return None
+        sums = [np.zeros((n, c.n_frames), np.float64) for c in self.contexts]
+        ptrs = (ctypes.c_void_p * len(sums))(*[a.ctypes.data for a in sums])
+        self._chk(core_lib().mlem_batch_iterate(self._h, n, ptrs))
+        return sums
+
+    def profile(self, n: int):
+        """(ms[4], bytes[4], launches[4]) per iteration: the multi-matrix
+        kernel, -, the calcUpdate launches, the statistics."""
+        ms = np.zeros(4, np.float64)
+        by = np.zeros(4, np.float64)
+        ln = np.zeros(4, np.int32)
+        self._chk(core_lib().mlem_batch_profile(self._h, n, _p(ms), _p(by), _p(ln)))
+        return ms, by, ln
+
+
+# ---------------------------------------------------------------------------
 # The reference's functions (mlem_seq/seqcsr4mlem.cpp), same names and
 # argument meaning; `matrix` is a Context.
-# ---------------------------------------------------------------------------
 def _fill(dst, src, what):
     if dst.shape != src.shape:  # the reference asserts the sizes
         raise MlemError(MLEM_ERR_INVALID, f"{what}: size {dst.size} != {src.size}")

@@ -44,8 +44,8 @@ struct mlem_ctx {
     double sumnorm = 0.0;
 
     // Voxel order on the device.  With a known grid the columns are
-    // relabelled into 8x8x8 bricks with Morton order inside (see
-    // brick_order); perm maps a natural voxel index to its device index.
+    // relabelled along a Morton curve (see brick_order); perm maps a natural
+    // voxel index to its device index.
     bool bricked = false;
     uint32_t grid[3] = {0, 0, 0};
     uint32_t* perm = nullptr;
@@ -78,6 +78,10 @@ struct mlem_ctx {
     int32_t* tmp_sino = nullptr;
     double* tmp_d = nullptr;
     float* inits_dev = nullptr;
+
+    // region-blocked copy of the matrix (MLEM_BK_REGION), for one frame tile
+    RegionBlocks rb;
+    size_t rb_bytes = 0;
 
     mlem_tuning tuning{};
     cudaGraphExec_t graph = nullptr;
@@ -188,38 +192,47 @@ void default_tuning(mlem_ctx* c) {
 // ---------------------------------------------------------------------------
 // Device voxel order.  A ray's consecutive voxels are neighbours in 3-D; in
 // the natural order (ix + nx*(iy + ny*iz), scannerconfig.cpp getVoxelNr)
-// only its x-steps stay inside a 128-byte line.  Bricks of 8x8x8 voxels in
-// raster order with a Morton (Z-order) curve inside put every 2x2x2 cube in
-// one 32-byte sector and every 4x4x2 block in one 128-byte line, so the
-// image gathers and update scatters of a ray touch far fewer lines.  Grids
-// that are not multiples of 8 are padded conceptually and the codes ranked.
-// The relabelling changes no arithmetic: rows keep their element order and
-// columns keep their ascending row order.
+// only its x-steps stay inside a 128-byte line.  A Morton (Z-order) curve
+// over the whole grid puts every 2x2x2 cube in one 32-byte sector, every
+// 4x4x2 block in one 128-byte line, and every aligned block of 2^k voxels in
+// a compact box -- the regions of the region-blocked method.  Axes are
+// interleaved level by level while they have bits left (x lowest), so the
+// codes are dense when every dimension is a power of two; otherwise they
+// are ranked.  The relabelling changes no arithmetic: rows keep their
+// element order and columns keep their ascending row order.
 // ---------------------------------------------------------------------------
-uint32_t morton9(uint32_t x, uint32_t y, uint32_t z) {
-    uint32_t m = 0;
-    for (int b = 0; b < 3; ++b)
-        m |= (((x >> b) & 1u) << (3 * b)) | (((y >> b) & 1u) << (3 * b + 1)) |
-             (((z >> b) & 1u) << (3 * b + 2));
+uint64_t morton_code(uint32_t x, uint32_t y, uint32_t z, const int bits[3]) {
+    uint64_t m = 0;
+    int out = 0;
+    const int top = std::max(bits[0], std::max(bits[1], bits[2]));
+    for (int b = 0; b < top; ++b) {
+        if (b < bits[0]) m |= (uint64_t)((x >> b) & 1u) << out++;
+        if (b < bits[1]) m |= (uint64_t)((y >> b) & 1u) << out++;
+        if (b < bits[2]) m |= (uint64_t)((z >> b) & 1u) << out++;
+    }
     return m;
 }
 
 void brick_order(uint32_t nx, uint32_t ny, uint32_t nz, std::vector<uint32_t>& perm) {
     const uint64_t C = (uint64_t)nx * ny * nz;
-    const uint32_t bx = (nx + 7) / 8, by = (ny + 7) / 8;
+    int bits[3] = {0, 0, 0};
+    const uint32_t n[3] = {nx, ny, nz};
+    bool pow2 = true;
+    for (int i = 0; i < 3; ++i) {
+        while ((1ull << bits[i]) < n[i]) ++bits[i];
+        pow2 = pow2 && (1ull << bits[i]) == n[i];
+    }
     perm.resize(C);
-    std::vector<uint64_t> code(C);
+    std::vector<uint64_t> code(pow2 ? 0 : C);
     for (uint32_t iz = 0; iz < nz; ++iz)
         for (uint32_t iy = 0; iy < ny; ++iy)
             for (uint32_t ix = 0; ix < nx; ++ix) {
-                const uint64_t brick = (ix >> 3) + (uint64_t)bx * ((iy >> 3) + (uint64_t)by * (iz >> 3));
-                code[ix + (uint64_t)nx * (iy + (uint64_t)ny * iz)] =
-                    brick * 512 + morton9(ix & 7, iy & 7, iz & 7);
+                const uint64_t v = ix + (uint64_t)nx * (iy + (uint64_t)ny * iz);
+                const uint64_t m = morton_code(ix, iy, iz, bits);
+                if (pow2) perm[v] = (uint32_t)m;
+                else code[v] = m;
             }
-    if (nx % 8 == 0 && ny % 8 == 0 && nz % 8 == 0) {
-        for (uint64_t v = 0; v < C; ++v) perm[v] = (uint32_t)code[v];
-        return;
-    }
+    if (pow2) return;
     std::vector<uint32_t> order(C);
     for (uint64_t v = 0; v < C; ++v) order[v] = (uint32_t)v;
     std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return code[a] < code[b]; });
@@ -236,6 +249,33 @@ int perm_scratch(mlem_ctx* c, size_t floats) {
     c->pscratch_floats = 0;
     for (auto& p : c->pscratch) TRY(dev_alloc(c, &p, floats));
     c->pscratch_floats = floats;
+    return MLEM_OK;
+}
+
+// Region-blocked copy for the tile size `frame_tile` (built once per tile
+// size; rebuilding frees the previous copy).  Never called during capture.
+int ensure_region(mlem_ctx* c, int frame_tile) {
+    const int rlog = region_rlog(frame_tile, c->C);
+    if (c->rb.el && c->rb.rlog == rlog) return MLEM_OK;
+    if (c->rb.el) {
+        region_free(&c->rb);
+        c->device_bytes -= c->rb_bytes;
+        c->rb_bytes = 0;
+    }
+    size_t bytes = 0;
+    int line = 0;
+    const cudaError_t e =
+        region_build(SparseView{c->row_ptr, reinterpret_cast<const uint4*>(c->elems), c->R, c->Z},
+                     c->C, rlog, &c->rb, &bytes, &line, c->stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(c, e == cudaErrorMemoryAllocation ? MLEM_ERR_NOMEM : MLEM_ERR_CUDA,
+                    "region-blocked build (rlog %d) failed at k_region.cu:%d: %s", rlog, line,
+                    cudaGetErrorString(e));
+    }
+    c->rb_bytes = bytes;
+    c->device_bytes += bytes;
+    c->graph_dirty = true;
     return MLEM_OK;
 }
 
@@ -479,6 +519,19 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                 TRY(mark(c, pe, 2));
                 CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
                 break;
+            case MLEM_BK_REGION:
+                if (!c->rb.el || c->rb.rlog != region_rlog(t.frame_tile, c->C))
+                    return fail(c, MLEM_ERR_STATE, "region-blocked copy not built for this frame tile");
+                CK(c, cudaMemsetAsync(c->correl, 0, (size_t)c->R * Bp * 4, st));
+                for (uint32_t f0 = 0; f0 < Bp; f0 += T)
+                    CK(c, region_fwproj(c->rb, c->x, Bp, f0, c->C, c->correl, cfg, st));
+                CK(c, correl_inplace(c->correl, c->sino, (uint64_t)c->R * Bp, st));
+                TRY(mark(c, pe, 1));
+                for (uint32_t f0 = 0; f0 < Bp; f0 += T)
+                    CK(c, region_bkproj(c->rb, c->correl, Bp, f0, c->C, c->update, cfg, st));
+                TRY(mark(c, pe, 2));
+                CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
+                break;
             default:
                 return fail(c, MLEM_ERR_INVALID, "unknown back-projection mode %d", t.bk_mode);
         }
@@ -494,15 +547,30 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
 // Algorithmic bytes of each phase per iteration: every matrix element and
 // offset once per pass over the matrix (one pass per frame tile), every
 // vector entry once per read or write, for the B real frames.
-void phase_bytes(const mlem_ctx* c, double* bytes, int* launches) {
+void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* bytes,
+                     int* launches) {
     const double R = c->R, C = c->C, Z = (double)c->Z, B = c->B;
     const bool exact = (c->flags & MLEM_FLAG_EXACT) != 0;
-    const int mode = exact ? MLEM_BK_CSC : c->tuning.bk_mode;
-    const double tiles = exact ? 1.0 : (double)(c->Bp / (uint32_t)c->tuning.frame_tile);
+    const int mode = exact ? MLEM_BK_CSC : bk_mode;
+    const double tiles = exact ? 1.0 : (double)(c->Bp / (uint32_t)frame_tile);
     const double csr_pass = 8.0 * (R + 1) + 8.0 * Z;
     const double csc_pass = 8.0 * (C + 1) + 8.0 * Z;
     for (int p = 0; p < MLEM_N_PHASES; ++p) { bytes[p] = 0.0; launches[p] = 0; }
     const int nt = (int)tiles;
+    if (mode == MLEM_BK_REGION) {
+        // elements (padded to chunks), chunk segments, segment rows, per pass
+        const double NC = (double)c->rb.nchunks, S = (double)c->rb.nseg;
+        const double pass = 256.0 * NC + 4.0 * NC + 4.0 * S;
+        bytes[0] = tiles * pass + B * (4.0 * C + 4.0 * R) + B * 12.0 * R;  // x, f, correl pass
+        bytes[1] = tiles * pass + B * (4.0 * R + 4.0 * C);                  // c, update
+        bytes[2] = 4.0 * C + B * (4.0 * C + 8.0 * C + 4.0 * C);             // calcUpdate
+        launches[0] = nt + 1;
+        launches[1] = nt;
+        launches[2] = 1;
+        bytes[3] = 4.0 * C * B;
+        launches[3] = 2;
+        return;
+    }
     if (mode == MLEM_BK_FUSED) {
         bytes[0] = tiles * csr_pass + B * (4.0 * C + 4.0 * R + 4.0 * C);  // x, sino, update
         launches[0] = nt;
@@ -523,6 +591,10 @@ void phase_bytes(const mlem_ctx* c, double* bytes, int* launches) {
     }
     bytes[3] = 4.0 * C * B;
     launches[3] = 2;
+}
+
+void phase_bytes(const mlem_ctx* c, double* bytes, int* launches) {
+    phase_bytes_for(c, c->tuning.bk_mode, c->tuning.frame_tile, bytes, launches);
 }
 
 int ensure_history(mlem_ctx* c, int n) {
@@ -679,7 +751,7 @@ int mlem_create_siddon(mlem_ctx** out, uint32_t nx, uint32_t ny, uint32_t nz, ui
         if ((s = dev_alloc(c, &counts, std::max<uint32_t>(n_rows, 1))) != MLEM_OK) break;
         if ((s = dev_alloc(c, &scratch, sb)) != MLEM_OK) break;
         cudaError_t e = siddon_counts(spec, counts, c->stream);
-        if (e == cudaSuccess) e = exclusive_scan_u64(counts, c->row_ptr, n_rows, scratch, c->stream);
+        if (e == cudaSuccess) e = exclusive_scan_u64(counts, c->row_ptr, n_rows, scratch, sb, c->stream);
         uint64_t Z = 0;
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(&Z, c->row_ptr + n_rows, 8, cudaMemcpyDeviceToHost, c->stream);
@@ -718,6 +790,7 @@ void mlem_destroy(mlem_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     drop_graph(c);
     free_frames(c);
+    region_free(&c->rb);
     for (void* p : {(void*)c->row_ptr, (void*)c->elems, (void*)c->col_ptr, (void*)c->celems,
                     (void*)c->norm, c->stage, (void*)c->stats_slot, (void*)c->hist_sums,
                     (void*)c->hist_zeros, (void*)c->hist_subn, (void*)c->tmp_r[0],
@@ -762,6 +835,7 @@ int mlem_kernels_per_iteration(const mlem_ctx* c, int* n) {
     if (c->flags & MLEM_FLAG_EXACT) k += 2;
     else if (c->tuning.bk_mode == MLEM_BK_CSC) k += 2 * tiles;
     else if (c->tuning.bk_mode == MLEM_BK_ATOMIC) k += 2 * tiles + 1;
+    else if (c->tuning.bk_mode == MLEM_BK_REGION) k += 2 * tiles + 2;
     else k += tiles + 1;
     *n = k;
     return MLEM_OK;
@@ -942,6 +1016,8 @@ int mlem_iterate(mlem_ctx* c, int n, double* sums, uint64_t* zeros, uint64_t* su
     if (!c->images_ready) return fail(c, MLEM_ERR_STATE, "images not initialised");
     if (n == 0) return MLEM_OK;
     TRY(set_device(c));
+    if (c->tuning.bk_mode == MLEM_BK_REGION && !(c->flags & MLEM_FLAG_EXACT))
+        TRY(ensure_region(c, c->tuning.frame_tile));
     // Chunks of up to 64 iterations, each one graph launch.
     const int chunk = std::min(n, 64);
     TRY(ensure_history(c, chunk));
@@ -985,6 +1061,8 @@ int mlem_step_host(mlem_ctx* c, const int32_t* sino, float* images, uint32_t B) 
     TRY(upload_frames<int32_t>(c, sino, c->sino, c->R));
     TRY(upload_frames<float>(c, images, c->x, c->C));
     c->images_ready = true;
+    if (c->tuning.bk_mode == MLEM_BK_REGION && !(c->flags & MLEM_FLAG_EXACT))
+        TRY(ensure_region(c, c->tuning.frame_tile));
     if (c->graph_dirty || !c->graph || c->graph_iters != 1) {
         TRY(ensure_history(c, 1));
         TRY(capture(c, 1));
@@ -1000,6 +1078,8 @@ int mlem_profile_phases(mlem_ctx* c, int n, double* ms, double* bytes, int* laun
     if (!c->images_ready) return fail(c, MLEM_ERR_STATE, "images not initialised");
     TRY(set_device(c));
     TRY(ensure_history(c, 1));
+    if (c->tuning.bk_mode == MLEM_BK_REGION && !(c->flags & MLEM_FLAG_EXACT))
+        TRY(ensure_region(c, c->tuning.frame_tile));
     std::vector<PhaseEvents> evs((size_t)n);
     for (auto& pe : evs)
         for (auto& e : pe.ev) CK(c, cudaEventCreate(&e));
@@ -1047,7 +1127,7 @@ int mlem_set_tuning(mlem_ctx* c, const mlem_tuning* t) {
     if (n.bk_mode == MLEM_BK_AUTO) n.bk_mode = c->has_csc ? MLEM_BK_CSC : MLEM_BK_ATOMIC;
     if (n.bk_mode == MLEM_BK_CSC && !c->has_csc)
         return fail(c, MLEM_ERR_INVALID, "MLEM_BK_CSC needs the CSC copy");
-    if (n.bk_mode < MLEM_BK_CSC || n.bk_mode > MLEM_BK_FUSED)
+    if (n.bk_mode < MLEM_BK_CSC || n.bk_mode > MLEM_BK_REGION)
         return fail(c, MLEM_ERR_INVALID, "unknown back-projection mode %d", n.bk_mode);
     LaunchCfg cfg;
     cfg.group = n.group;
@@ -1059,6 +1139,10 @@ int mlem_set_tuning(mlem_ctx* c, const mlem_tuning* t) {
     if (c->Bp && (c->Bp % (uint32_t)n.frame_tile))
         return fail(c, MLEM_ERR_INVALID, "frame tile %d does not divide the padded frame count %u",
                     n.frame_tile, c->Bp);
+    if (n.bk_mode == MLEM_BK_REGION) {
+        TRY(set_device(c));
+        TRY(ensure_region(c, n.frame_tile));
+    }
     c->tuning = n;
     c->graph_dirty = true;
     return MLEM_OK;
@@ -1079,7 +1163,11 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
     CK(c, cudaMemcpyAsync(saved, c->x, xb, cudaMemcpyDeviceToDevice, c->stream));
     std::vector<int> modes;
     if (c->has_csc) modes.push_back(MLEM_BK_CSC);
-    if (!deterministic_only) { modes.push_back(MLEM_BK_ATOMIC); modes.push_back(MLEM_BK_FUSED); }
+    if (!deterministic_only) {
+        modes.push_back(MLEM_BK_ATOMIC);
+        modes.push_back(MLEM_BK_FUSED);
+        modes.push_back(MLEM_BK_REGION);
+    }
     cudaEvent_t e0, e1;
     CK(c, cudaEventCreate(&e0));
     CK(c, cudaEventCreate(&e1));
@@ -1090,7 +1178,12 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
         for (int group : {8, 16, 32})
             for (int tile : {1, 2, 4, 8, 16}) {
                 if (c->Bp % (uint32_t)tile) continue;
+                if (mode == MLEM_BK_REGION) {
+                    if (group != 32) continue;  // warp-wide kernels: the group is not used
+                    TRY(ensure_region(c, tile));
+                }
                 for (int bps : {4, 8}) {
+                    if (mode == MLEM_BK_REGION && bps == 4) continue;  // grid is fixed by the tile
                     mlem_tuning t{mode, group, tile, bps, 0.0};
                     // warm-up once, then time two iterations
                     int s = enqueue_iteration(c, t, false);
@@ -1113,6 +1206,7 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
     CK(c, cudaStreamSynchronize(c->stream));
     cudaFree(saved);
     c->device_bytes -= xb;
+    if (best.bk_mode == MLEM_BK_REGION) TRY(ensure_region(c, best.frame_tile));
     c->tuning = best;
     c->graph_dirty = true;
     if (best_out) *best_out = best;
@@ -1239,6 +1333,526 @@ int mlem_project_f64(mlem_ctx* c, const float* x, double* out) {
     CK(c, project_f64(csr_view(c), xd, c->tmp_d, c->stream));
     CK(c, cudaMemcpyAsync(out, c->tmp_d, (size_t)c->R * 8, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
+    return MLEM_OK;
+}
+
+}  // extern "C"
+
+// ===========================================================================
+// Multi-matrix batches (mlem_batch_*): several contexts, one persistent
+// kernel per iteration over work items cut from all their rows.
+// ===========================================================================
+struct mlem_batch {
+    std::vector<mlem_ctx*> ctx;
+    int device = 0;
+    int n_sm = 148;
+    cudaStream_t stream = nullptr;               // the first context's stream
+    std::vector<std::vector<uint64_t>> row_ptr;  // host copies, for cutting items
+    int policy = MLEM_BATCH_INTERLEAVED;
+    int tile = 0;  // frames per pass, shared by the batch
+    uint32_t items_per_block = 4;
+    int blocks_per_sm = 4;  // k_batch_fused is bounded to 64 registers: 4 x 256 threads per SM
+    double ms_per_iter = 0.0;
+
+    std::vector<BatchItem> items;
+    BatchTable table{};  // the kernels' parameter
+    BatchItem* items_d = nullptr;
+    size_t items_cap = 0;
+    unsigned int* counter = nullptr;
+    bool scheduled = false;
+
+    cudaGraphExec_t graph = nullptr;
+    int graph_iters = 0;
+    bool graph_dirty = true;
+    std::vector<const void*> graph_sig;  // context pointers the graph holds
+
+    std::string err;
+};
+
+namespace {
+
+int bfail(mlem_batch* b, int status, const char* fmt, ...) __attribute__((format(printf, 3, 4)));
+int bfail(mlem_batch* b, int status, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    return set_error(b ? &b->err : nullptr, status, "%s", buf);
+}
+
+#define BCK(b, call)                                                                        \
+    do {                                                                                    \
+        cudaError_t e_ = (call);                                                            \
+        if (e_ != cudaSuccess)                                                              \
+            return bfail((b), e_ == cudaErrorMemoryAllocation ? MLEM_ERR_NOMEM : MLEM_ERR_CUDA, \
+                         "%s: %s (%s:%d)", cudaGetErrorName(e_), cudaGetErrorString(e_),   \
+                         __FILE__, __LINE__);                                               \
+    } while (0)
+
+// A context's status, carried over into the batch's message.
+int bctx(mlem_batch* b, mlem_ctx* c, int s) {
+    if (s == MLEM_OK) return s;
+    return bfail(b, s, "%s", c->err.c_str());
+}
+
+bool tile_ok(int t, uint32_t Bp) {
+    return (t == 1 || t == 2 || t == 4 || t == 8 || t == 16) && Bp % (uint32_t)t == 0;
+}
+
+bool tile_ok_all(const mlem_batch* b, int t) {
+    for (const mlem_ctx* c : b->ctx)
+        if (!tile_ok(t, c->Bp)) return false;
+    return true;
+}
+
+// Widest tile (<= 16) dividing every padded frame count.
+int batch_default_tile(const mlem_batch* b) {
+    for (int t : {16, 8, 4, 2})
+        if (tile_ok_all(b, t)) return t;
+    return 1;
+}
+
+// Cost of rows [r0, r1) of context i: element bytes once per frame-tile
+// pass, one gather and one scatter of 4 bytes per element and frame, and the
+// row's offsets, sinogram entries and sums.
+double item_cost(const mlem_batch* b, size_t i, uint32_t r0, uint32_t r1) {
+    const mlem_ctx* c = b->ctx[i];
+    const double nnz = (double)(b->row_ptr[i][r1] - b->row_ptr[i][r0]);
+    const double passes = (double)(c->Bp / (uint32_t)b->tile);
+    return nnz * (8.0 * passes + 8.0 * c->Bp) + (double)(r1 - r0) * (16.0 + 8.0 * c->Bp);
+}
+
+// Cut the rows of every matrix into items of about total / (resident blocks x
+// items_per_block) cost; full items of the costliest matrix first in row
+// order (neighbouring rows share image voxels in L2), then the ragged
+// remainders, heaviest first.
+int batch_schedule(mlem_batch* b) {
+    const size_t n = b->ctx.size();
+    if (b->policy != MLEM_BATCH_ITEMS) {  // the interleaved schedule needs no items
+        b->items.clear();
+        b->scheduled = true;
+        b->graph_dirty = true;
+        return MLEM_OK;
+    }
+    std::vector<double> total(n, 0.0);
+    double all = 0.0;
+    for (size_t i = 0; i < n; ++i) {
+        total[i] = item_cost(b, i, 0, b->ctx[i]->R);
+        all += total[i];
+    }
+    const double resident = (double)b->n_sm * (double)b->blocks_per_sm;
+    const double target = std::max(all / (resident * (double)b->items_per_block), 1.0);
+    std::vector<size_t> order(n);
+    for (size_t i = 0; i < n; ++i) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t a, size_t c) { return total[a] > total[c]; });
+    std::vector<BatchItem> full;
+    std::vector<std::pair<double, BatchItem>> tail;
+    for (size_t i : order) {
+        const uint32_t R = b->ctx[i]->R;
+        uint32_t r0 = 0;
+        while (r0 < R) {
+            uint32_t lo = r0 + 1, hi = R;  // smallest r1 whose cost reaches the target
+            while (lo < hi) {
+                const uint32_t mid = lo + (hi - lo) / 2;
+                if (item_cost(b, i, r0, mid) >= target) hi = mid;
+                else lo = mid + 1;
+            }
+            const BatchItem it{(uint32_t)i, r0, lo, 0u};
+            const double cost = item_cost(b, i, r0, lo);
+            if (cost >= 0.5 * target) full.push_back(it);
+            else tail.emplace_back(cost, it);
+            r0 = lo;
+        }
+    }
+    std::stable_sort(tail.begin(), tail.end(),
+                     [](const std::pair<double, BatchItem>& a,
+                        const std::pair<double, BatchItem>& c) { return a.first > c.first; });
+    b->items = std::move(full);
+    for (auto& t : tail) b->items.push_back(t.second);
+    if (b->items.size() > 0xffffffffull)
+        return bfail(b, MLEM_ERR_INVALID, "too many work items (%zu)", b->items.size());
+    if (b->items.size() > b->items_cap) {
+        dev_free(b->items_d);
+        b->items_d = nullptr;
+        b->items_cap = 0;
+        BCK(b, cudaMalloc(&b->items_d, b->items.size() * sizeof(BatchItem)));
+        b->items_cap = b->items.size();
+    }
+    if (!b->items.empty())
+        BCK(b, cudaMemcpyAsync(b->items_d, b->items.data(), b->items.size() * sizeof(BatchItem),
+                               cudaMemcpyHostToDevice, b->stream));
+    BCK(b, cudaStreamSynchronize(b->stream));
+    b->scheduled = true;
+    b->graph_dirty = true;
+    return MLEM_OK;
+}
+
+// Check the contexts, make room for `chunk` iterations of statistics, fill
+// the matrix table and (re)schedule when a context changed.
+int batch_refresh(mlem_batch* b, int chunk) {
+    bool reschedule = !b->scheduled;
+    std::vector<const void*> sig;
+    BatchTable& t = b->table;
+    t.n = (uint32_t)b->ctx.size();
+    t.row_base[0] = 0;
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+        mlem_ctx* c = b->ctx[i];
+        if (!c->B || !c->images_ready)
+            return bfail(b, MLEM_ERR_STATE, "context %zu: sinograms and images not set", i);
+        if (c->stream != b->stream) BCK(b, cudaStreamSynchronize(c->stream));
+        TRY(bctx(b, c, ensure_history(c, chunk)));
+        if (t.mats[i].Bp != c->Bp) reschedule = true;
+        t.mats[i] = BatchMat{csr_view(c), c->x, c->sino, c->update, c->Bp, 0u};
+        t.row_base[i + 1] = t.row_base[i] + c->R;
+        for (const void* p : {(const void*)c->x, (const void*)c->sino, (const void*)c->update,
+                              (const void*)c->norm, (const void*)c->stats_scratch,
+                              (const void*)c->stats_slot, (const void*)c->hist_sums,
+                              (const void*)c->hist_zeros, (const void*)c->hist_subn})
+            sig.push_back(p);
+        sig.push_back(reinterpret_cast<const void*>((uintptr_t)c->Bp));
+        sig.push_back(reinterpret_cast<const void*>((uintptr_t)c->B));
+    }
+    if (!tile_ok_all(b, b->tile)) {
+        b->tile = batch_default_tile(b);
+        reschedule = true;
+    }
+    if (sig != b->graph_sig) {
+        b->graph_dirty = true;
+        b->graph_sig = sig;
+    }
+    if (reschedule) TRY(batch_schedule(b));
+    return MLEM_OK;
+}
+
+int bmark(mlem_batch* b, const PhaseEvents* pe, int i) {
+    if (pe) BCK(b, cudaEventRecord(pe->ev[i], b->stream));
+    return MLEM_OK;
+}
+
+// One iteration of every context: the multi-matrix pass, then per context
+// calcUpdate (zeroing its update vector) and the image statistics.
+int batch_enqueue(mlem_batch* b, bool stats, const PhaseEvents* pe = nullptr) {
+    cudaStream_t st = b->stream;
+    TRY(bmark(b, pe, 0));
+    if (b->policy == MLEM_BATCH_ITEMS)
+        BCK(b, batch_fused(b->table, b->items_d, (uint32_t)b->items.size(), b->counter, b->tile,
+                           b->n_sm, b->blocks_per_sm, st));
+    else
+        BCK(b, batch_interleaved(b->table, b->tile, b->n_sm, b->blocks_per_sm, st));
+    TRY(bmark(b, pe, 1));
+    TRY(bmark(b, pe, 2));
+    for (mlem_ctx* c : b->ctx) BCK(b, apply_update(c->x, c->update, c->norm, c->C, c->Bp, true, st));
+    TRY(bmark(b, pe, 3));
+    if (stats)
+        for (mlem_ctx* c : b->ctx)
+            BCK(b, image_stats(c->x, c->C, c->Bp, c->B, c->stats_scratch, c->stats_slot,
+                               c->hist_sums, c->hist_zeros, c->hist_subn, st));
+    TRY(bmark(b, pe, 4));
+    return MLEM_OK;
+}
+
+int batch_reset_slots(mlem_batch* b) {
+    for (mlem_ctx* c : b->ctx) BCK(b, cudaMemsetAsync(c->stats_slot, 0, 4, b->stream));
+    return MLEM_OK;
+}
+
+void batch_drop_graph(mlem_batch* b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->graph_iters = 0;
+}
+
+int batch_capture(mlem_batch* b, int n) {
+    batch_drop_graph(b);
+    BCK(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    int s = batch_reset_slots(b);
+    for (int i = 0; i < n && s == MLEM_OK; ++i) s = batch_enqueue(b, true);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(b->stream, &g);
+    if (s != MLEM_OK) { if (g) cudaGraphDestroy(g); return s; }
+    if (e != cudaSuccess) return bfail(b, MLEM_ERR_CUDA, "end capture: %s", cudaGetErrorString(e));
+    e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) return bfail(b, MLEM_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e));
+    b->graph_iters = n;
+    b->graph_dirty = false;
+    return MLEM_OK;
+}
+
+// Average ms of `reps` iterations (after one warm-up) with the current schedule.
+int batch_time(mlem_batch* b, int reps, cudaEvent_t e0, cudaEvent_t e1, double* ms) {
+    TRY(batch_enqueue(b, false));
+    BCK(b, cudaEventRecord(e0, b->stream));
+    for (int i = 0; i < reps; ++i) TRY(batch_enqueue(b, false));
+    BCK(b, cudaEventRecord(e1, b->stream));
+    BCK(b, cudaEventSynchronize(e1));
+    float t = 0.0f;
+    BCK(b, cudaEventElapsedTime(&t, e0, e1));
+    *ms = t / reps;
+    return MLEM_OK;
+}
+
+void batch_free(mlem_batch* b) {
+    batch_drop_graph(b);
+    dev_free(b->items_d);
+    dev_free(b->counter);
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* mlem_batch_last_error(const mlem_batch* b) {
+    return b ? b->err.c_str() : global_error().c_str();
+}
+
+int mlem_batch_create(mlem_batch** out, mlem_ctx* const* ctxs, uint32_t n_ctx) {
+    if (!out || !ctxs) return bfail(nullptr, MLEM_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (n_ctx == 0 || n_ctx > MLEM_BATCH_MAX_MATRICES)
+        return bfail(nullptr, MLEM_ERR_INVALID, "a batch holds 1..%d contexts (got %u)",
+                     MLEM_BATCH_MAX_MATRICES, n_ctx);
+    for (uint32_t i = 0; i < n_ctx; ++i) {
+        const mlem_ctx* c = ctxs[i];
+        if (!c) return bfail(nullptr, MLEM_ERR_INVALID, "context %u is null", i);
+        for (uint32_t j = 0; j < i; ++j)
+            if (ctxs[j] == c) return bfail(nullptr, MLEM_ERR_INVALID, "context %u repeats %u", i, j);
+        if (c->device != ctxs[0]->device)
+            return bfail(nullptr, MLEM_ERR_INVALID, "context %u is on device %d, not %d", i,
+                         c->device, ctxs[0]->device);
+        if (c->flags & MLEM_FLAG_EXACT)
+            return bfail(nullptr, MLEM_ERR_INVALID,
+                         "context %u was created with MLEM_FLAG_EXACT (bit-exact kernels)", i);
+        if (!c->B || !c->images_ready)
+            return bfail(nullptr, MLEM_ERR_STATE, "context %u: sinograms and images not set", i);
+    }
+    mlem_batch* b = new mlem_batch();
+    b->ctx.assign(ctxs, ctxs + n_ctx);
+    b->device = ctxs[0]->device;
+    b->n_sm = ctxs[0]->n_sm;
+    b->stream = ctxs[0]->stream;
+    int s = MLEM_OK;
+    auto bail = [&](int status) {
+        batch_free(b);
+        global_error() = b->err;
+        delete b;
+        return status;
+    };
+    if (cudaSetDevice(b->device) != cudaSuccess)
+        return bail(bfail(b, MLEM_ERR_CUDA, "cudaSetDevice(%d) failed", b->device));
+    b->row_ptr.resize(n_ctx);
+    for (uint32_t i = 0; i < n_ctx; ++i) {
+        mlem_ctx* c = ctxs[i];
+        b->row_ptr[i].resize((size_t)c->R + 1);
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(b->row_ptr[i].data(), c->row_ptr, ((size_t)c->R + 1) * 8,
+                           cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess)
+            return bail(bfail(b, MLEM_ERR_CUDA, "row offsets of context %u: %s", i,
+                              cudaGetErrorString(e)));
+    }
+    if (cudaMalloc(&b->counter, 256) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(bfail(b, MLEM_ERR_NOMEM, "batch descriptors: cudaMalloc failed"));
+    }
+    s = batch_refresh(b, 1);
+    if (s != MLEM_OK) return bail(s);
+    *out = b;
+    return MLEM_OK;
+}
+
+void mlem_batch_destroy(mlem_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    batch_free(b);
+    delete b;
+}
+
+int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
+                            int blocks_per_sm, int frame_tile) {
+    if (!b) return bfail(nullptr, MLEM_ERR_INVALID, "null batch");
+    if (policy != MLEM_BATCH_INTERLEAVED && policy != MLEM_BATCH_ITEMS)
+        return bfail(b, MLEM_ERR_INVALID, "unknown batch schedule %d", policy);
+    if (items_per_block < 1 || items_per_block > 1024)
+        return bfail(b, MLEM_ERR_INVALID, "items_per_block must be 1..1024 (got %u)", items_per_block);
+    if (blocks_per_sm < 1 || blocks_per_sm > 32)
+        return bfail(b, MLEM_ERR_INVALID, "blocks_per_sm must be 1..32 (got %d)", blocks_per_sm);
+    if (frame_tile != 0 && !tile_ok_all(b, frame_tile))
+        return bfail(b, MLEM_ERR_INVALID,
+                     "frame tile %d: must be 1, 2, 4, 8 or 16 and divide every context's padded "
+                     "frame count", frame_tile);
+    BCK(b, cudaSetDevice(b->device));
+    b->policy = policy;
+    b->items_per_block = items_per_block;
+    b->blocks_per_sm = blocks_per_sm;
+    if (frame_tile != 0) b->tile = frame_tile;
+    b->scheduled = false;
+    b->graph_dirty = true;
+    return batch_refresh(b, 1);
+}
+
+int mlem_batch_get_schedule(const mlem_batch* b, int* policy, uint32_t* items_per_block,
+                            int* blocks_per_sm, int* frame_tile, uint32_t* n_items,
+                            double* ms_per_iter) {
+    if (!b) return bfail(nullptr, MLEM_ERR_INVALID, "null batch");
+    if (policy) *policy = b->policy;
+    if (items_per_block) *items_per_block = b->items_per_block;
+    if (blocks_per_sm) *blocks_per_sm = b->blocks_per_sm;
+    if (frame_tile) *frame_tile = b->tile;
+    if (n_items) *n_items = (uint32_t)b->items.size();
+    if (ms_per_iter) *ms_per_iter = b->ms_per_iter;
+    return MLEM_OK;
+}
+
+int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter) {
+    if (!b) return bfail(nullptr, MLEM_ERR_INVALID, "null batch");
+    BCK(b, cudaSetDevice(b->device));
+    TRY(batch_refresh(b, 1));
+    // Tuning runs real iterations: save the images.
+    std::vector<float*> saved(b->ctx.size(), nullptr);
+    auto release = [&]() {
+        for (float* p : saved) dev_free(p);
+    };
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+        mlem_ctx* c = b->ctx[i];
+        if (cudaMalloc(&saved[i], (size_t)c->C * c->Bp * 4) != cudaSuccess) {
+            cudaGetLastError();
+            release();
+            return bfail(b, MLEM_ERR_NOMEM, "autotune: no room to save the images of context %zu", i);
+        }
+        if (cudaMemcpyAsync(saved[i], c->x, (size_t)c->C * c->Bp * 4, cudaMemcpyDeviceToDevice,
+                            b->stream) != cudaSuccess) {
+            release();
+            return bfail(b, MLEM_ERR_CUDA, "autotune: saving images failed");
+        }
+    }
+    auto restore = [&]() -> int {
+        for (size_t i = 0; i < b->ctx.size(); ++i) {
+            mlem_ctx* c = b->ctx[i];
+            BCK(b, cudaMemcpyAsync(c->x, saved[i], (size_t)c->C * c->Bp * 4,
+                                   cudaMemcpyDeviceToDevice, b->stream));
+        }
+        return MLEM_OK;
+    };
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    int s = MLEM_OK;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        s = bfail(b, MLEM_ERR_CUDA, "event creation failed");
+    uint32_t best_ipb = b->items_per_block;
+    int best_bps = b->blocks_per_sm, best_tile = b->tile, best_policy = b->policy;
+    double best = 1e30;
+    auto trial = [&](int policy, uint32_t ipb, int bps, int tile) -> int {
+        TRY(mlem_batch_set_schedule(b, policy, ipb, bps, tile));
+        double ms = 0.0;
+        TRY(batch_time(b, 2, e0, e1, &ms));
+        TRY(restore());
+        if (ms < best) {
+            best = ms;
+            best_policy = policy;
+            best_ipb = ipb;
+            best_bps = bps;
+            best_tile = tile;
+        }
+        return MLEM_OK;
+    };
+    // The frame tile with the interleaved schedule first, then the resident
+    // blocks, then the items schedule's granularity with that tile.
+    for (int t : {16, 8, 4, 2, 1})
+        if (s == MLEM_OK && tile_ok_all(b, t)) s = trial(MLEM_BATCH_INTERLEAVED, best_ipb, 4, t);
+    for (int bps : {3, 8})
+        if (s == MLEM_OK) s = trial(MLEM_BATCH_INTERLEAVED, best_ipb, bps, best_tile);
+    for (uint32_t ipb : {1u, 4u, 16u, 64u})
+        if (s == MLEM_OK) s = trial(MLEM_BATCH_ITEMS, ipb, 4, best_tile);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (s == MLEM_OK) s = restore();
+    if (s == MLEM_OK && cudaStreamSynchronize(b->stream) != cudaSuccess)
+        s = bfail(b, MLEM_ERR_CUDA, "autotune: synchronize failed");
+    release();
+    if (s != MLEM_OK) return s;
+    TRY(mlem_batch_set_schedule(b, best_policy, best_ipb, best_bps, best_tile));
+    b->ms_per_iter = best;
+    if (ms_per_iter) *ms_per_iter = best;
+    return MLEM_OK;
+}
+
+int mlem_batch_iterate(mlem_batch* b, int n, double* const* sums) {
+    if (!b) return bfail(nullptr, MLEM_ERR_INVALID, "null batch");
+    if (n < 0) return bfail(b, MLEM_ERR_INVALID, "negative iteration count");
+    if (n == 0) return MLEM_OK;
+    BCK(b, cudaSetDevice(b->device));
+    const int chunk = std::min(n, 64);
+    TRY(batch_refresh(b, chunk));
+    if (b->graph_dirty || !b->graph || b->graph_iters != chunk) TRY(batch_capture(b, chunk));
+    int done = 0;
+    while (done < n) {
+        const int k = std::min(chunk, n - done);
+        if (k == chunk) {
+            BCK(b, cudaGraphLaunch(b->graph, b->stream));
+        } else {
+            TRY(batch_reset_slots(b));
+            for (int i = 0; i < k; ++i) TRY(batch_enqueue(b, true));
+        }
+        bool any = false;
+        for (size_t i = 0; sums && i < b->ctx.size(); ++i) {
+            if (!sums[i]) continue;
+            const mlem_ctx* c = b->ctx[i];
+            BCK(b, cudaMemcpyAsync(sums[i] + (size_t)done * c->B, c->hist_sums,
+                                   (size_t)k * c->B * 8, cudaMemcpyDeviceToHost, b->stream));
+            any = true;
+        }
+        if (any) BCK(b, cudaStreamSynchronize(b->stream));
+        done += k;
+    }
+    BCK(b, cudaStreamSynchronize(b->stream));
+    return MLEM_OK;
+}
+
+int mlem_batch_profile(mlem_batch* b, int n, double* ms, double* bytes, int* launches) {
+    if (!b || n <= 0) return bfail(b, MLEM_ERR_INVALID, "bad argument");
+    BCK(b, cudaSetDevice(b->device));
+    TRY(batch_refresh(b, 1));
+    std::vector<PhaseEvents> evs((size_t)n);
+    for (auto& pe : evs)
+        for (auto& e : pe.ev) BCK(b, cudaEventCreate(&e));
+    int s = MLEM_OK;
+    for (int i = 0; i < n && s == MLEM_OK; ++i) {
+        s = batch_reset_slots(b);
+        if (s == MLEM_OK) s = batch_enqueue(b, true, &evs[(size_t)i]);
+    }
+    if (s == MLEM_OK && cudaStreamSynchronize(b->stream) != cudaSuccess)
+        s = bfail(b, MLEM_ERR_CUDA, "synchronize");
+    double acc[MLEM_N_PHASES] = {0, 0, 0, 0};
+    for (auto& pe : evs)
+        for (int p = 0; p < MLEM_N_PHASES && s == MLEM_OK; ++p) {
+            float t = 0.0f;
+            if (cudaEventElapsedTime(&t, pe.ev[p], pe.ev[p + 1]) != cudaSuccess)
+                s = bfail(b, MLEM_ERR_CUDA, "event timing");
+            acc[p] += t;
+        }
+    for (auto& pe : evs)
+        for (auto& e : pe.ev) cudaEventDestroy(e);
+    if (s != MLEM_OK) return s;
+    double tb[MLEM_N_PHASES] = {0, 0, 0, 0};
+    int tl[MLEM_N_PHASES] = {0, 0, 0, 0};
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+        double pb[MLEM_N_PHASES];
+        int pl[MLEM_N_PHASES];
+        phase_bytes_for(b->ctx[i], MLEM_BK_FUSED, b->tile, pb, pl);
+        for (int p = 0; p < MLEM_N_PHASES; ++p) {
+            tb[p] += pb[p];
+            tl[p] += pl[p];
+        }
+    }
+    tl[MLEM_PHASE_PROJECT] = 1;  // one kernel for all matrices and frame tiles
+    for (int p = 0; p < MLEM_N_PHASES; ++p) {
+        if (ms) ms[p] = acc[p] / n;
+        if (bytes) bytes[p] = tb[p];
+        if (launches) launches[p] = tl[p];
+    }
     return MLEM_OK;
 }
 

@@ -1,0 +1,117 @@
+// k_batch.cu -- one kernel per iteration for reconstructions over several
+// matrices of uneven size (different scanners, different frame counts).
+//
+// Each matrix keeps its own context (CSR, image, sinograms, update vector).
+// Two schedules run the one-pass per-row work (fused_row_range, row_dev.cuh)
+// over the rows of all matrices in one launch, so a small matrix fills the
+// tail of a large one instead of running in a launch of its own:
+//   items       -- the rows are cut into work items of about equal cost
+//                  (rows x elements per row x frames) that a persistent grid
+//                  pulls from a global counter, heaviest first;
+//   interleaved -- one virtual row space over all matrices, walked in
+//                  grid-stride order.
+//
+// BT is one template parameter for the whole batch: dispatching several tile
+// widths inside one kernel makes the compiler allocate their registers side
+// by side (72-80 registers for one width, 167 for five), which would halve
+// the resident warps of a latency-bound gather kernel.
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.h"
+#include "row_dev.cuh"
+
+namespace mlem {
+
+namespace {
+
+constexpr int kBatchThreads = 256;
+
+template <int BT>
+__global__ void __launch_bounds__(kBatchThreads, 4) k_batch_fused(const BatchTable t,
+                                                                   const BatchItem* __restrict__ items,
+                                                                   uint32_t n_items,
+                                                                   unsigned int* __restrict__ counter) {
+    __shared__ BatchItem s_item;
+    const uint64_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint32_t it = atomicAdd(counter, 1u);
+            s_item = it < n_items ? items[it] : BatchItem{0u, 0u, 0u, 1u};
+        }
+        __syncthreads();
+        const BatchItem item = s_item;
+        __syncthreads();                 // s_item is rewritten by the next grab
+        if (item.pad) return;            // block-uniform: no items left
+        const BatchMat& m = t.mats[item.mat];
+        const uint32_t Bp = m.Bp;
+#pragma unroll 1
+        for (uint32_t f0 = 0; f0 < Bp; f0 += BT)
+            fused_row_range<32, BT>(m.csr, m.x, Bp, f0, m.sino, m.u, item.row0, item.row1, warp,
+                                    nwarps);
+    }
+}
+
+// Interleaved schedule: the rows of all matrices form one virtual row space
+// (matrix i owns [row_base[i], row_base[i+1])), and global warp w takes
+// virtual rows w, w + W, w + 2W, ... -- the grid-stride order of k_fused_row,
+// so at any moment the whole grid works on one window of neighbouring rows,
+// and a warp that finishes one matrix's rows goes straight on to the next
+// matrix's.  Each row does all its frame tiles back to back.  The table is a
+// kernel parameter: it lives in the constant bank like k_fused_row's
+// arguments instead of taking registers.
+template <int BT>
+__global__ void __launch_bounds__(kBatchThreads, 4) k_batch_interleaved(const BatchTable t) {
+    const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const uint64_t total = t.row_base[t.n];
+    uint32_t mi = 0;
+    for (; v < total; v += nw) {
+        while (v >= t.row_base[mi + 1]) ++mi;  // warp-uniform, monotone
+        const uint64_t r = v - t.row_base[mi];
+        const uint32_t Bp = t.mats[mi].Bp;
+#pragma unroll 1
+        for (uint32_t f0 = 0; f0 < Bp; f0 += BT)
+            fused_row_range<32, BT>(t.mats[mi].csr, t.mats[mi].x, Bp, f0, t.mats[mi].sino,
+                                    t.mats[mi].u, r, r + 1, 0, 1);
+    }
+}
+
+}  // namespace
+
+cudaError_t batch_interleaved(const BatchTable& t, int frame_tile, int sm_count,
+                              int blocks_per_sm, cudaStream_t st) {
+    if (t.n == 0 || t.n > kBatchTableMax) return cudaErrorInvalidValue;
+    const int grid = std::max(1, sm_count * blocks_per_sm);
+    switch (frame_tile) {
+        case 1: k_batch_interleaved<1><<<grid, kBatchThreads, 0, st>>>(t); break;
+        case 2: k_batch_interleaved<2><<<grid, kBatchThreads, 0, st>>>(t); break;
+        case 4: k_batch_interleaved<4><<<grid, kBatchThreads, 0, st>>>(t); break;
+        case 8: k_batch_interleaved<8><<<grid, kBatchThreads, 0, st>>>(t); break;
+        case 16: k_batch_interleaved<16><<<grid, kBatchThreads, 0, st>>>(t); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t batch_fused(const BatchTable& t, const BatchItem* items, uint32_t n_items,
+                        unsigned int* counter, int frame_tile, int sm_count, int blocks_per_sm,
+                        cudaStream_t st) {
+    if (n_items == 0) return cudaSuccess;
+    if (t.n == 0 || t.n > kBatchTableMax) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
+    if (e != cudaSuccess) return e;
+    const int grid = std::max(1, std::min<int>((int)std::min<uint32_t>(n_items, 1u << 30),
+                                               sm_count * blocks_per_sm));
+    switch (frame_tile) {
+        case 1: k_batch_fused<1><<<grid, kBatchThreads, 0, st>>>(t, items, n_items, counter); break;
+        case 2: k_batch_fused<2><<<grid, kBatchThreads, 0, st>>>(t, items, n_items, counter); break;
+        case 4: k_batch_fused<4><<<grid, kBatchThreads, 0, st>>>(t, items, n_items, counter); break;
+        case 8: k_batch_fused<8><<<grid, kBatchThreads, 0, st>>>(t, items, n_items, counter); break;
+        case 16: k_batch_fused<16><<<grid, kBatchThreads, 0, st>>>(t, items, n_items, counter); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace mlem

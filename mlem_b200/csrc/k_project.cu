@@ -22,147 +22,11 @@
 
 #include "common.cuh"
 #include "kernels.h"
+#include "row_dev.cuh"
 
 namespace mlem {
 
 namespace {
-
-template <int BT>
-struct Lanes {
-    static constexpr int VW = BT < 4 ? BT : 4;  // floats per lane
-    static constexpr int FL = BT / VW;          // lanes per element
-};
-
-__device__ __forceinline__ float2 ld_hot2(const float2* ptr, uint64_t pol) {
-    float2 r;
-    asm("ld.global.nc.L2::cache_hint.v2.f32 {%0,%1}, [%2], %3;" : "=f"(r.x), "=f"(r.y)
-        : "l"(ptr), "l"(pol));
-    return r;
-}
-
-template <int VW>
-__device__ __forceinline__ void ld_vec(const float* __restrict__ p, float (&v)[VW], uint64_t pol) {
-    if constexpr (VW == 4) {
-        const float4 t = ld_hot4(reinterpret_cast<const float4*>(p), pol);
-        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-    } else if constexpr (VW == 2) {
-        const float2 t = ld_hot2(reinterpret_cast<const float2*>(p), pol);
-        v[0] = t.x; v[1] = t.y;
-    } else {
-        v[0] = ld_hot(p, pol);
-    }
-}
-
-template <int VW>
-__device__ __forceinline__ void ld_plain(const float* __restrict__ p, float (&v)[VW]) {
-    if constexpr (VW == 4) {
-        const float4 t = *reinterpret_cast<const float4*>(p);
-        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-    } else if constexpr (VW == 2) {
-        const float2 t = *reinterpret_cast<const float2*>(p);
-        v[0] = t.x; v[1] = t.y;
-    } else {
-        v[0] = *p;
-    }
-}
-
-template <int VW>
-__device__ __forceinline__ void st_vec(float* __restrict__ p, const float (&v)[VW]) {
-    if constexpr (VW == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-    else if constexpr (VW == 2) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
-    else *p = v[0];
-}
-
-template <int VW>
-__device__ __forceinline__ void ld_counts(const int32_t* __restrict__ p, int32_t (&v)[VW]) {
-    if constexpr (VW == 4) {
-        const int4 t = *reinterpret_cast<const int4*>(p);
-        v[0] = t.x; v[1] = t.y; v[2] = t.z; v[3] = t.w;
-    } else if constexpr (VW == 2) {
-        const int2 t = *reinterpret_cast<const int2*>(p);
-        v[0] = t.x; v[1] = t.y;
-    } else {
-        v[0] = *p;
-    }
-}
-
-// u[...] += w * c[...] for VW floats (one vector reduction, 4..16 bytes).
-template <int VW>
-__device__ __forceinline__ void red_vec(float* __restrict__ p, float w, const float (&c)[VW]) {
-    if constexpr (VW == 4)
-        atomicAdd(reinterpret_cast<float4*>(p), make_float4(w * c[0], w * c[1], w * c[2], w * c[3]));
-    else if constexpr (VW == 2)
-        atomicAdd(reinterpret_cast<float2*>(p), make_float2(w * c[0], w * c[1]));
-    else
-        atomicAdd(p, w * c[0]);
-}
-
-// Elements a lane loads before it gathers (memory-level parallelism).  A
-// full-warp group takes 8 (a 150-250-element row is one batch); narrower
-// groups take 4, which keeps their registers, and so their occupancy, lower
-// (measured on the plain-full workload).
-template <int G>
-constexpr int batch_depth() { return G == 32 ? 8 : 4; }
-
-// acc[0..VW) = sum over the row's elements of value * vec[col*B + off + ...].
-// Each batch issues all of its (predicated) element loads, then all of its
-// gathers, so a row costs about two memory latencies per batch instead of
-// two per element.  When `keep` is non-null and the whole row fits in one
-// batch, the lane's elements are left in keep[] (fused kernel) and true is
-// returned.
-template <int G, int BT, bool KEEP>
-__device__ __forceinline__ bool row_dot(const uint2* __restrict__ el, uint64_t b, uint64_t e,
-                                        int lane, const float* __restrict__ vec, uint32_t B,
-                                        uint32_t off, float (&acc)[Lanes<BT>::VW], uint64_t ps,
-                                        uint64_t ph, uint2* keep = nullptr) {
-    constexpr int VW = Lanes<BT>::VW, FL = Lanes<BT>::FL, EPS = G / FL;
-    constexpr int kBatch = batch_depth<G>();
-    const float* base = vec + off;
-#pragma unroll
-    for (int i = 0; i < VW; ++i) acc[i] = 0.0f;
-    const bool one_batch = e - b <= (uint64_t)kBatch * EPS;
-    for (uint64_t k0 = b + lane / FL; k0 < e; k0 += (uint64_t)kBatch * EPS) {
-        uint2 q[kBatch];
-#pragma unroll
-        for (int u = 0; u < kBatch; ++u) {
-            const uint64_t k = k0 + (uint64_t)u * EPS;
-            q[u] = make_uint2(0u, 0u);  // value 0: contributes nothing
-            if (k < e) q[u] = KEEP ? ld_keep2(el + k, ps) : ld_stream2(el + k, ps);
-        }
-        float xv[kBatch][VW];
-#pragma unroll
-        for (int u = 0; u < kBatch; ++u) {
-            if (k0 + (uint64_t)u * EPS < e) {
-                ld_vec<VW>(base + (size_t)q[u].x * B, xv[u], ph);
-            } else {
-#pragma unroll
-                for (int i = 0; i < VW; ++i) xv[u][i] = 0.0f;
-            }
-        }
-#pragma unroll
-        for (int u = 0; u < kBatch; ++u) {
-            const float v = __uint_as_float(q[u].y);
-#pragma unroll
-            for (int i = 0; i < VW; ++i) acc[i] = fmaf(v, xv[u][i], acc[i]);
-        }
-        if (keep && one_batch) {
-#pragma unroll
-            for (int u = 0; u < kBatch; ++u) keep[u] = q[u];
-        }
-    }
-    return one_batch;
-}
-
-// Sum over the element slots of the group: afterwards every lane holds the
-// row totals of its frames.  Every lane of the warp must call it.
-template <int G, int BT>
-__device__ __forceinline__ void slot_allreduce(float (&acc)[Lanes<BT>::VW]) {
-    constexpr int VW = Lanes<BT>::VW, FL = Lanes<BT>::FL;
-#pragma unroll
-    for (int o = FL; o < G; o <<= 1)
-#pragma unroll
-        for (int i = 0; i < VW; ++i) acc[i] += __shfl_xor_sync(MLEM_FULL_MASK, acc[i], o);
-}
 
 #define MLEM_WARP_LOOP_SETUP                                                     \
     constexpr int RPW = 32 / G;                                                  \
@@ -274,54 +138,19 @@ __global__ void __launch_bounds__(256) k_bkproj_scatter(SparseView csr,
 
 // ---------------------------------------------------------------------------
 // One pass per row: forward projection, calcCorrel, and the back-projection
-// scatter of the same row while its elements are still on chip (the row is
-// re-read from L1).  The matrix streams from HBM once per iteration.
+// scatter of the same row while its elements are still on chip (in
+// registers when the row fits one load batch, else re-read from L1).  The
+// matrix streams from HBM once per iteration.  The per-row work is in
+// fused_row_range (row_dev.cuh), shared with the multi-matrix kernel.
 // ---------------------------------------------------------------------------
 template <int G, int BT>
 __global__ void __launch_bounds__(256) k_fused_row(SparseView csr, const float* __restrict__ x,
                                                    uint32_t B, uint32_t f0,
                                                    const int32_t* __restrict__ sino,
                                                    float* __restrict__ u) {
-    MLEM_WARP_LOOP_SETUP
-    constexpr int EPS = G / FL;
-    const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
-    for (uint64_t base = warp * RPW; base < csr.n; base += nwarps * RPW) {
-        const uint64_t r = base + lw / G;
-        const bool active = r < csr.n;
-        uint64_t b = 0, e = 0;
-        if (active) { b = csr.ptr[r]; e = csr.ptr[r + 1]; }
-        float acc[VW];
-        constexpr int kBatch = batch_depth<G>();
-        uint2 kept[kBatch];
-        const bool in_regs =
-            row_dot<G, BT, true>(el, b, e, lane, x, B, f0 + sub * VW, acc, ps, ph, kept);
-        slot_allreduce<G, BT>(acc);
-        if (!active) continue;
-        const uint64_t idx = r * B + f0 + sub * VW;
-        int32_t s[VW];
-        ld_counts<VW>(sino + idx, s);
-        float cv[VW];
-        bool any = false;
-#pragma unroll
-        for (int i = 0; i < VW; ++i) {
-            cv[i] = correl_of(s[i], acc[i]);
-            any |= (cv[i] != 0.0f);
-        }
-        if (!any) continue;
-        float* ub = u + f0 + sub * VW;
-        if (in_regs) {
-            // the whole row is still in registers: scatter from there
-#pragma unroll
-            for (int q = 0; q < kBatch; ++q)
-                if (b + lane / FL + (uint64_t)q * EPS < e)
-                    red_vec<VW>(ub + (size_t)kept[q].x * B, __uint_as_float(kept[q].y), cv);
-        } else {
-            for (uint64_t k = b + lane / FL; k < e; k += EPS) {
-                const uint2 q = ld_keep2(el + k, ps);
-                red_vec<VW>(ub + (size_t)q.x * B, __uint_as_float(q.y), cv);
-            }
-        }
-    }
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    fused_row_range<G, BT>(csr, x, B, f0, sino, u, 0, csr.n, warp, nwarps);
 }
 
 #undef MLEM_WARP_LOOP_SETUP

@@ -415,7 +415,8 @@ static cudaError_t scan_impl(const uint64_t* in, uint64_t* out, uint64_t n, char
 }
 
 cudaError_t exclusive_scan_u64(const uint64_t* in, uint64_t* out, uint64_t n, void* scratch,
-                               cudaStream_t st) {
+                               size_t scratch_bytes, cudaStream_t st) {
+    if (scratch_bytes < scan_scratch_bytes(n)) return cudaErrorInvalidValue;
     return scan_impl(in, out, n, static_cast<char*>(scratch), st);
 }
 
@@ -449,7 +450,8 @@ cudaError_t transpose(const SparseView& csr, uint32_t C, uint64_t* col_ptr, uint
         k_count_cols<<<grid, 256, 0, st>>>(csr, cnt);
         MLEM_TRY(cudaGetLastError());
     }
-    MLEM_TRY(exclusive_scan_u64(reinterpret_cast<const uint64_t*>(cnt), col_ptr, C, scan_scratch, st));
+    MLEM_TRY(exclusive_scan_u64(reinterpret_cast<const uint64_t*>(cnt), col_ptr, C, scan_scratch,
+                                scan_scratch_bytes(C), st));
     if (csr.nnz == 0) {
         if (max_col_len) *max_col_len = 0;
         return cudaStreamSynchronize(st);

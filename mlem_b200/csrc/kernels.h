@@ -108,8 +108,10 @@ cudaError_t correl_elementwise(const float* f, const int32_t* s, float* c, uint6
 // ---- prefix sums ----------------------------------------------------------
 // out[0] = 0, out[i+1] = in[0] + ... + in[i]  (n+1 outputs).
 size_t scan_scratch_bytes(uint64_t n);
+// `scratch` must hold scan_scratch_bytes(n) bytes; scratch_bytes is checked
+// (cudaErrorInvalidValue, nothing launched, when it is too small).
 cudaError_t exclusive_scan_u64(const uint64_t* in, uint64_t* out, uint64_t n, void* scratch,
-                               cudaStream_t st);
+                               size_t scratch_bytes, cudaStream_t st);
 
 // ---- deterministic CSR -> CSC transpose -----------------------------------
 // col_ptr: C+1 entries; celems: Z (+ padding) 8-byte elements.  scratch is
@@ -134,5 +136,91 @@ cudaError_t siddon_fill(const SiddonSpec& s, const uint64_t* row_ptr, uint2* ele
                         cudaStream_t st);
 // out[r] = sequential double sum of v_k * x[col_k] (bit-identical to the host).
 cudaError_t project_f64(const SparseView& csr, const float* x, double* out, cudaStream_t st);
+
+// ---- region-blocked method (k_region.cu) -----------------------------------
+// Rows cut into segments, one per region (aligned block of 2^rlog device
+// voxels); elements stored region by region, each region padded to whole
+// 32-element chunks: {voxel index inside the region | head flag (bit 31) on
+// a segment's first element, value}.  seg_row[s]: row of segment s;
+// chunk_seg[c]: segment of chunk c's first element.
+struct RegionView {
+    const uint64_t* reg_chunk_ptr;  // nreg+1 chunk ranges
+    const uint2* el;
+    const uint32_t* seg_row;
+    const uint32_t* chunk_seg;
+    uint64_t nchunks;
+    uint32_t nreg;
+    int rlog;
+};
+
+struct RegionBlocks {
+    uint64_t* reg_chunk_ptr = nullptr;
+    uint2* el = nullptr;
+    uint32_t* seg_row = nullptr;
+    uint32_t* chunk_seg = nullptr;
+    uint64_t nchunks = 0;
+    uint32_t nreg = 0;
+    int rlog = 0;
+    uint64_t nseg = 0;
+    RegionView view() const {
+        return RegionView{reg_chunk_ptr, el, seg_row, chunk_seg, nchunks, nreg, rlog};
+    }
+};
+
+// Shared memory of one region tile: 2^rlog voxels x frame_tile floats.
+constexpr size_t kRegionTileBytes = 65536;
+// Region size (log2 voxels) for a frame tile and C voxels.
+int region_rlog(int frame_tile, uint32_t C);
+// failed_line (nullable) receives the k_region.cu line of a failing step.
+cudaError_t region_build(const SparseView& csr, uint32_t C, int rlog, RegionBlocks* out,
+                         size_t* bytes, int* failed_line, cudaStream_t st);
+void region_free(RegionBlocks* rb);
+// fw[row][f] += segment partial projections (fw zeroed by the caller).
+cudaError_t region_fwproj(const RegionBlocks& rb, const float* x, uint32_t B, uint32_t f0,
+                          uint32_t C, float* fw, const LaunchCfg& cfg, cudaStream_t st);
+// u[col][f] += (A^T c)[col][f] (u zeroed by the caller).
+cudaError_t region_bkproj(const RegionBlocks& rb, const float* c, uint32_t B, uint32_t f0,
+                          uint32_t C, float* u, const LaunchCfg& cfg, cudaStream_t st);
+// f[i] = calcCorrel(s[i], f[i]).
+cudaError_t correl_inplace(float* f, const int32_t* s, uint64_t n, cudaStream_t st);
+
+// ---- multi-matrix batches (k_batch.cu) ---------------------------------------
+// One matrix of a batch: its CSR and interleaved images / sinograms / update
+// vector (stride Bp).
+struct BatchMat {
+    SparseView csr;
+    const float* x;
+    const int32_t* sino;
+    float* u;
+    uint32_t Bp;
+    uint32_t pad;
+};
+// Rows [row0, row1) of matrix `mat` (pad: 0).
+struct BatchItem {
+    uint32_t mat;
+    uint32_t row0, row1;
+    uint32_t pad;
+};
+// The matrices of a batch, passed by value as the kernels' parameter (it
+// lives in the constant bank, like a single-matrix kernel's arguments, and
+// takes no registers): matrix i owns virtual rows [row_base[i], row_base[i+1]).
+constexpr uint32_t kBatchTableMax = 64;
+struct BatchTable {
+    BatchMat mats[kBatchTableMax];
+    uint64_t row_base[kBatchTableMax + 1];
+    uint32_t n;
+};
+static_assert(sizeof(BatchTable) <= 32764, "kernel parameter space (CUDA >= 12.1)");
+
+// Items schedule: every item does u[mat] += A^T correl(A x) over its rows,
+// all frames of its matrix in passes of frame_tile (1, 2, 4, 8 or 16;
+// divides every Bp).  `counter` (one uint) is reset on the stream first.
+cudaError_t batch_fused(const BatchTable& t, const BatchItem* items, uint32_t n_items,
+                        unsigned int* counter, int frame_tile, int sm_count, int blocks_per_sm,
+                        cudaStream_t st);
+// Interleaved schedule: the same work in grid-stride order over the virtual
+// row space.
+cudaError_t batch_interleaved(const BatchTable& t, int frame_tile, int sm_count,
+                              int blocks_per_sm, cudaStream_t st);
 
 }  // namespace mlem

@@ -20,7 +20,7 @@ def main(argv=None):
     ap.add_argument("--rows", type=int, default=1 << 20)
     ap.add_argument("--count", type=int, nargs=2, default=[150, 250])
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--mode", choices=["csc", "atomic", "fused", "exact"], default="csc")
+    ap.add_argument("--mode", choices=["csc", "atomic", "fused", "region", "exact"], default="csc")
     ap.add_argument("--group", type=int, default=32)
     ap.add_argument("--frame-tile", type=int, default=1)
     ap.add_argument("--blocks-per-sm", type=int, default=8)
@@ -38,7 +38,8 @@ def main(argv=None):
         fr = synth.make_frames(w, ctx.project_f64)
         ctx.set_sinograms(fr.sinograms)
         if a.mode != "exact":
-            mode = {"csc": api.BK_CSC, "atomic": api.BK_ATOMIC, "fused": api.BK_FUSED}[a.mode]
+            mode = {"csc": api.BK_CSC, "atomic": api.BK_ATOMIC, "fused": api.BK_FUSED,
+                    "region": api.BK_REGION}[a.mode]
             ctx.set_tuning(bk_mode=mode, group=a.group, frame_tile=a.frame_tile,
                            blocks_per_sm=a.blocks_per_sm)
         ctx.init_images()

@@ -1,0 +1,169 @@
+"""Uneven multi-matrix batches (mlem_batch_*): several matrices of different
+size and frame count iterated by one persistent kernel per iteration.
+
+Every frame of every context must match the oracle's own run of that
+(matrix, sinogram) within relative L2 1e-4, whatever the schedule (work-item
+granularity, resident blocks, frame tile).
+"""
+import numpy as np
+import pytest
+
+from mlem_b200 import api
+
+import oracle_bind as ob
+
+pytestmark = pytest.mark.gpu
+
+TOL_MLEM = 1e-4
+ITERS = 10
+# (golden case, frames): padded frame counts 16, 8 and 4 -- three matrices of
+# different size, like a batch over three scanner geometries
+MEMBERS = (("plain_small_it10", 4), ("tiny_it10", 12), ("edge_it7", 8))
+
+
+def _frames(sino, B, seed):
+    rng = np.random.default_rng(seed)
+    return np.stack([sino if b == 0 else rng.permutation(sino) for b in range(B)]).astype(np.int32)
+
+
+@pytest.fixture(scope="module")
+def members(golden):
+    out = []
+    for i, (name, B) in enumerate(MEMBERS):
+        m, sino, _, _, _ = golden.case(name)
+        sinos = _frames(sino, B, 17 + i)
+        want = np.stack([ob.mlem(m, sinos[b], ITERS)[0] for b in range(B)])
+        out.append((m, sinos, want))
+    return out
+
+
+def _contexts(members, flags=0):
+    ctxs = []
+    for m, sinos, _ in members:
+        c = api.Context.from_matrix(m, flags=flags)
+        c.set_sinograms(sinos)
+        c.init_images()
+        ctxs.append(c)
+    return ctxs
+
+
+def _check(ctxs, members):
+    for c, (m, sinos, want) in zip(ctxs, members):
+        got = c.get_images()
+        for b in range(sinos.shape[0]):
+            assert ob.rel_l2(got[b], want[b]) <= TOL_MLEM, (m.n_rows, b)
+
+
+@pytest.mark.parametrize("policy,items_per_block,blocks_per_sm,tile", [
+    (api.BATCH_INTERLEAVED, 4, 4, 0), (api.BATCH_INTERLEAVED, 1, 3, 1),
+    (api.BATCH_INTERLEAVED, 1, 8, 4), (api.BATCH_ITEMS, 4, 4, 0), (api.BATCH_ITEMS, 1, 3, 4),
+    (api.BATCH_ITEMS, 32, 4, 2), (api.BATCH_ITEMS, 2, 1, 1), (api.BATCH_ITEMS, 1024, 8, 4)])
+def test_batch_matches_oracle(members, policy, items_per_block, blocks_per_sm, tile):
+    ctxs = _contexts(members)
+    try:
+        with api.Batch(ctxs) as b:
+            b.set_schedule(policy, items_per_block, blocks_per_sm, tile)
+            sched = b.schedule()
+            assert sched["policy"] == policy
+            if policy == api.BATCH_ITEMS:
+                assert sched["n_items"] >= len(ctxs)
+            if tile:
+                assert sched["frame_tile"] == tile
+            b.iterate(ITERS)
+        _check(ctxs, members)
+    finally:
+        for c in ctxs:
+            c.close()
+
+
+def test_batch_sums_and_chunking(members):
+    """70 iterations (one 64-iteration graph plus 6 single launches) give
+    the same images as 70 iterations of each context on its own, and the
+    returned sums are the image sums."""
+    ctxs = _contexts(members)
+    solo = _contexts(members)
+    try:
+        with api.Batch(ctxs) as b:
+            sums = b.iterate(70)
+        for c, s, own in zip(ctxs, sums, solo):
+            own.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=4, blocks_per_sm=8)
+            own_sums, _, _ = own.iterate(70)
+            a, w = c.get_images(), own.get_images()
+            assert s.shape == (70, c.n_frames)
+            for f in range(c.n_frames):
+                assert ob.rel_l2(a[f], w[f]) <= TOL_MLEM
+                np.testing.assert_allclose(s[:, f], own_sums[:, f], rtol=1e-4)
+                assert abs(s[-1, f] - a[f].astype(np.float64).sum()) <= 1e-6 * abs(s[-1, f])
+    finally:
+        for c in ctxs + solo:
+            c.close()
+
+
+def test_batch_autotune_restores_images(members):
+    ctxs = _contexts(members)
+    try:
+        before = [c.get_images() for c in ctxs]
+        with api.Batch(ctxs) as b:
+            sched = b.autotune()
+            assert sched["ms_per_iter"] > 0
+            assert sched["frame_tile"] in (1, 2, 4)  # must divide 4, 8 and 16
+            for c, x in zip(ctxs, before):
+                assert c.get_images().tobytes() == x.tobytes()
+            b.iterate(ITERS)
+        _check(ctxs, members)
+    finally:
+        for c in ctxs:
+            c.close()
+
+
+def test_batch_follows_new_sinograms(members):
+    """A context given other frames after the batch was made is picked up
+    (new buffers, new frame count, new schedule) at the next iterate."""
+    ctxs = _contexts(members)
+    try:
+        with api.Batch(ctxs) as b:
+            b.iterate(2)
+            m, sinos, want = members[0]
+            ctxs[0].set_sinograms(sinos[:2])
+            ctxs[0].init_images()
+            b.iterate(ITERS)
+            got = ctxs[0].get_images()
+            for f in range(2):
+                assert ob.rel_l2(got[f], want[f]) <= TOL_MLEM
+    finally:
+        for c in ctxs:
+            c.close()
+
+
+def test_batch_rejects_bad_input(members):
+    ctxs = _contexts(members)
+    m = members[0][0]
+    exact = api.Context.from_matrix(m, flags=api.FLAG_EXACT)
+    exact.set_sinograms(members[0][1])
+    exact.init_images()
+    bare = api.Context.from_matrix(m)
+    try:
+        with pytest.raises(api.MlemError):
+            api.Batch([ctxs[0], exact])
+        with pytest.raises(api.MlemError):
+            api.Batch([ctxs[0], bare])  # no sinograms
+        with pytest.raises(api.MlemError):
+            api.Batch([ctxs[0], ctxs[0]])
+        with pytest.raises(api.MlemError):
+            api.Batch([])
+        with api.Batch(ctxs) as b:
+            with pytest.raises(api.MlemError):
+                b.set_schedule(api.BATCH_ITEMS, 4, 4, 8)  # does not divide the padded count 4
+            with pytest.raises(api.MlemError):
+                b.set_schedule(api.BATCH_ITEMS, 0, 4, 0)
+            with pytest.raises(api.MlemError):
+                b.set_schedule(api.BATCH_INTERLEAVED, 4, 0, 0)
+            with pytest.raises(api.MlemError):
+                b.set_schedule(api.BATCH_INTERLEAVED, 4, 4, 3)
+            with pytest.raises(api.MlemError):
+                b.set_schedule(7, 4, 4, 0)
+            b.iterate(ITERS)  # still usable after the rejected calls
+        _check(ctxs, members)
+    finally:
+        for c in ctxs + [exact, bare]:
+            c.close()

@@ -71,8 +71,11 @@ def test_pieces_against_oracle(ctxs, name):
     assert ctx.init_value(sino) == ob.init_value(norm, sino)
 
 
+MODES = [api.BK_CSC, api.BK_ATOMIC, api.BK_FUSED, api.BK_REGION]
+
+
 @pytest.mark.parametrize("name", CASES)
-@pytest.mark.parametrize("mode", [api.BK_CSC, api.BK_ATOMIC, api.BK_FUSED])
+@pytest.mark.parametrize("mode", MODES)
 def test_mlem_matches_reference_image(ctxs, name, mode):
     ctx, m, sino, iters, gold = ctxs[name]
     ctx.set_sinograms(sino)
@@ -115,8 +118,8 @@ def test_csc_mode_is_deterministic(ctxs):
     assert a.tobytes() == b.tobytes()
 
 
-@pytest.mark.parametrize("group,tile", [(8, 1), (16, 4), (32, 8), (32, 16), (16, 16)])
-@pytest.mark.parametrize("mode", [api.BK_CSC, api.BK_ATOMIC, api.BK_FUSED])
+@pytest.mark.parametrize("group,tile", [(8, 1), (16, 4), (32, 8), (32, 16), (16, 16), (4, 16)])
+@pytest.mark.parametrize("mode", MODES)
 def test_batched_frames_match_separate_runs(golden, group, tile, mode):
     m, sino, iters, gold, _ = golden.case("tiny_it10")
     rng = np.random.default_rng(group * 100 + tile)
@@ -189,7 +192,7 @@ def test_skewed_matrix_long_rows_and_columns():
         cp_o, ce_o = ob.transpose(m)
         assert np.array_equal(cp, cp_o) and ce.tobytes() == ce_o.tobytes()
         assert ctx.column_sums().tobytes() == ob.column_sums(m).tobytes()
-        for mode in (api.BK_CSC, api.BK_ATOMIC, api.BK_FUSED):
+        for mode in MODES:
             ctx.set_sinograms(sino)
             ctx.set_tuning(bk_mode=mode, group=32, frame_tile=1, blocks_per_sm=8)
             ctx.init_images()
