@@ -56,7 +56,8 @@ extern "C" {
 #define MLEM_FLAG_EXACT 0x1u    /* bit-exact kernels: the float operation order of seqcsr4mlem */
 #define MLEM_FLAG_NO_CSC 0x2u   /* do not build the CSC copy (atomic back projection only) */
 #define MLEM_FLAG_CHECKED 0x4u  /* accepted for compatibility: offsets and column indices are always validated */
-#define MLEM_FLAG_NATURAL_LAYOUT 0x8u /* keep the natural voxel order on the device (no brick layout) */
+#define MLEM_FLAG_NATURAL_LAYOUT 0x8u /* keep the natural voxel order on the device (no Morton layout) */
+#define MLEM_FLAG_NO_ROW_ORDER 0x10u  /* visit rows in file order (no entry/exit-voxel sort of the rows) */
 
 /* ---- back-projection strategies ---------------------------------------- */
 #define MLEM_BK_AUTO 0    /* the autotuner's choice (CSC when not tuned) */
@@ -88,8 +89,16 @@ typedef struct {
     int group;          /* lanes per row/column: 4, 8, 16 or 32 */
     int frame_tile;     /* frames per pass over the matrix: 1, 2, 4, 8 or 16 */
     int blocks_per_sm;  /* 1..8 blocks of 256 threads per SM */
+    int visit;          /* row visiting order: MLEM_VISIT_FILE, _SORTED or _SORTED_BLOCKED */
     double ms_per_iter; /* measured by mlem_autotune; 0 when set by hand */
 } mlem_tuning;
+
+/* Row visiting orders (mlem_tuning.visit).  The sorted orders need the row
+ * order built at creation (not MLEM_FLAG_NO_ROW_ORDER); results change only
+ * by the order of the scatter atomics. */
+#define MLEM_VISIT_FILE 0           /* file order, grid stride */
+#define MLEM_VISIT_SORTED 1         /* rows sorted by entry/exit voxel, grid stride */
+#define MLEM_VISIT_SORTED_BLOCKED 2 /* sorted; each warp walks one contiguous run (one-pass kernel) */
 
 /* ---- errors ------------------------------------------------------------- */
 const char* mlem_last_error(const mlem_ctx* ctx);
@@ -285,13 +294,15 @@ const char* mlem_batch_last_error(const mlem_batch* b);
 /* policy: MLEM_BATCH_INTERLEAVED or MLEM_BATCH_ITEMS; items_per_block (1..1024,
  * items schedule): about that many items for every resident block
  * (blocks_per_sm x SMs); frame_tile in {1,2,4,8,16} dividing every context's
- * padded frame count (0 keeps the current tile). */
+ * padded frame count (0 keeps the current tile); visit: MLEM_VISIT_* row
+ * order of every matrix (the sorted ones need every context's row order;
+ * MLEM_VISIT_SORTED_BLOCKED walks runs only in the items schedule). */
 int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
-                            int blocks_per_sm, int frame_tile);
+                            int blocks_per_sm, int frame_tile, int visit);
 /* Current schedule; any pointer may be NULL.  n_items: 0 for the interleaved
  * schedule.  ms_per_iter: from the last autotune, else 0. */
 int mlem_batch_get_schedule(const mlem_batch* b, int* policy, uint32_t* items_per_block,
-                            int* blocks_per_sm, int* frame_tile, uint32_t* n_items,
+                            int* blocks_per_sm, int* frame_tile, int* visit, uint32_t* n_items,
                             double* ms_per_iter);
 /* Time real iterations over schedules, frame tiles and resident blocks and
  * keep the fastest; the images are restored afterwards. */

@@ -21,7 +21,7 @@ class MlemInfo(ctypes.Structure):
 class MlemTuning(ctypes.Structure):
     _fields_ = [("bk_mode", ctypes.c_int), ("group", ctypes.c_int),
                 ("frame_tile", ctypes.c_int), ("blocks_per_sm", ctypes.c_int),
-                ("ms_per_iter", ctypes.c_double)]
+                ("visit", ctypes.c_int), ("ms_per_iter", ctypes.c_double)]
 
 
 class MlemCsr4Header(ctypes.Structure):

@@ -38,9 +38,12 @@ FLAG_EXACT = 0x1
 FLAG_NO_CSC = 0x2
 FLAG_CHECKED = 0x4
 FLAG_NATURAL_LAYOUT = 0x8
+FLAG_NO_ROW_ORDER = 0x10
 
 BK_AUTO, BK_CSC, BK_ATOMIC, BK_FUSED, BK_REGION = 0, 1, 2, 3, 4
 BATCH_INTERLEAVED, BATCH_ITEMS = 0, 1
+VISIT_FILE, VISIT_SORTED, VISIT_SORTED_BLOCKED = 0, 1, 2
+VISIT_NAMES = {VISIT_FILE: "file", VISIT_SORTED: "sorted", VISIT_SORTED_BLOCKED: "sorted-blocked"}
 BATCH_NAMES = {BATCH_INTERLEAVED: "interleaved", BATCH_ITEMS: "items"}
 BK_NAMES = {BK_CSC: "csc", BK_ATOMIC: "atomic", BK_FUSED: "fused", BK_REGION: "region"}
 
@@ -292,21 +295,26 @@ class Context:
         self.n_frames = n_frames
 
     # -- tuning -------------------------------------------------------------------
+    @staticmethod
+    def _tuning_dict(t) -> dict:
+        return dict(bk_mode=t.bk_mode, group=t.group, frame_tile=t.frame_tile,
+                    blocks_per_sm=t.blocks_per_sm, visit=t.visit, ms_per_iter=t.ms_per_iter)
+
     def tuning(self) -> dict:
         t = sig.MlemTuning()
         self._chk(core_lib().mlem_get_tuning(self._h, ctypes.byref(t)))
-        return dict(bk_mode=t.bk_mode, group=t.group, frame_tile=t.frame_tile,
-                    blocks_per_sm=t.blocks_per_sm, ms_per_iter=t.ms_per_iter)
+        return self._tuning_dict(t)
 
-    def set_tuning(self, bk_mode=BK_CSC, group=32, frame_tile=1, blocks_per_sm=8) -> None:
-        t = sig.MlemTuning(bk_mode, group, frame_tile, blocks_per_sm, 0.0)
+    def set_tuning(self, bk_mode=BK_CSC, group=32, frame_tile=1, blocks_per_sm=8,
+                   visit=0) -> None:
+        """visit: VISIT_FILE, VISIT_SORTED or VISIT_SORTED_BLOCKED."""
+        t = sig.MlemTuning(bk_mode, group, frame_tile, blocks_per_sm, visit, 0.0)
         self._chk(core_lib().mlem_set_tuning(self._h, ctypes.byref(t)))
 
     def autotune(self, deterministic_only: bool = False) -> dict:
         t = sig.MlemTuning()
         self._chk(core_lib().mlem_autotune(self._h, 1 if deterministic_only else 0, ctypes.byref(t)))
-        return dict(bk_mode=t.bk_mode, group=t.group, frame_tile=t.frame_tile,
-                    blocks_per_sm=t.blocks_per_sm, ms_per_iter=t.ms_per_iter)
+        return self._tuning_dict(t)
 
     # -- device pointers (ints) ----------------------------------------------------
     def fwproj_d(self, x_ptr: int, y_ptr: int, n_frames: int = 1, stream: int = 0) -> None:
@@ -374,18 +382,20 @@ class Batch:
             raise MlemError(st, core_lib().mlem_batch_last_error(self._h).decode(errors="replace"))
 
     def set_schedule(self, policy: int = BATCH_INTERLEAVED, items_per_block: int = 4,
-                     blocks_per_sm: int = 4, frame_tile: int = 0) -> None:
+                     blocks_per_sm: int = 4, frame_tile: int = 0, visit: int = VISIT_FILE) -> None:
         self._chk(core_lib().mlem_batch_set_schedule(self._h, policy, items_per_block,
-                                                     blocks_per_sm, frame_tile))
+                                                     blocks_per_sm, frame_tile, visit))
 
     def schedule(self) -> dict:
         pol, ipb, bps = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_int()
-        tile, n, ms = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_double()
+        tile, visit, n, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_uint32(), ctypes.c_double()
         self._chk(core_lib().mlem_batch_get_schedule(self._h, ctypes.byref(pol), ctypes.byref(ipb),
                                                      ctypes.byref(bps), ctypes.byref(tile),
-                                                     ctypes.byref(n), ctypes.byref(ms)))
+                                                     ctypes.byref(visit), ctypes.byref(n),
+                                                     ctypes.byref(ms)))
         return dict(policy=pol.value, items_per_block=ipb.value, blocks_per_sm=bps.value,
-                    frame_tile=tile.value, n_items=n.value, ms_per_iter=ms.value)
+                    frame_tile=tile.value, visit=visit.value, n_items=n.value,
+                    ms_per_iter=ms.value)
 
     def autotune(self) -> dict:
         ms = ctypes.c_double()

@@ -53,6 +53,10 @@ struct mlem_ctx {
     float* pscratch[2] = {nullptr, nullptr};
     size_t pscratch_floats = 0;
 
+    // Visiting order of the row kernels (row_order_build): rays with nearby
+    // entry and exit voxels next to each other.  Null with MLEM_FLAG_NO_ROW_ORDER.
+    uint32_t* row_order = nullptr;
+
     // frames
     uint32_t B = 0, Bp = 0;
     std::vector<double> sumin;
@@ -141,7 +145,8 @@ void dev_free(void* p) {
 }
 
 SparseView csr_view(const mlem_ctx* c) {
-    return SparseView{c->row_ptr, reinterpret_cast<const uint4*>(c->elems), c->R, c->Z};
+    return SparseView{c->row_ptr, reinterpret_cast<const uint4*>(c->elems), c->R, c->Z,
+                      c->row_order};
 }
 SparseView csc_view(const mlem_ctx* c) {
     return SparseView{c->col_ptr, reinterpret_cast<const uint4*>(c->celems), c->C, c->Z};
@@ -186,6 +191,7 @@ void default_tuning(mlem_ctx* c) {
     c->tuning.group = 32;
     c->tuning.frame_tile = c->Bp ? std::min(default_tile(c->Bp), 16) : 1;
     c->tuning.blocks_per_sm = 8;
+    c->tuning.visit = MLEM_VISIT_FILE;
     c->tuning.ms_per_iter = 0.0;
 }
 
@@ -255,9 +261,11 @@ int perm_scratch(mlem_ctx* c, size_t floats) {
 // Region-blocked copy for the tile size `frame_tile` (built once per tile
 // size; rebuilding frees the previous copy).  Never called during capture.
 int ensure_region(mlem_ctx* c, int frame_tile) {
-    const int rlog = region_rlog(frame_tile, c->C);
-    if (c->rb.el && c->rb.rlog == rlog) return MLEM_OK;
-    if (c->rb.el) {
+    int rlog = 0, sblog = 0;
+    uint32_t gpw = 0;
+    region_params(frame_tile, c->C, &rlog, &sblog, &gpw);
+    if (c->rb.el_fw && c->rb.rlog == rlog && c->rb.sblog == sblog && c->rb.gpw == gpw) return MLEM_OK;
+    if (c->rb.el_fw) {
         region_free(&c->rb);
         c->device_bytes -= c->rb_bytes;
         c->rb_bytes = 0;
@@ -266,17 +274,24 @@ int ensure_region(mlem_ctx* c, int frame_tile) {
     int line = 0;
     const cudaError_t e =
         region_build(SparseView{c->row_ptr, reinterpret_cast<const uint4*>(c->elems), c->R, c->Z},
-                     c->C, rlog, &c->rb, &bytes, &line, c->stream);
+                     c->C, rlog, sblog, gpw, &c->rb, &bytes, &line, c->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         return fail(c, e == cudaErrorMemoryAllocation ? MLEM_ERR_NOMEM : MLEM_ERR_CUDA,
-                    "region-blocked build (rlog %d) failed at k_region.cu:%d: %s", rlog, line,
-                    cudaGetErrorString(e));
+                    "region-blocked build (rlog %d, sblog %d) failed at k_region.cu:%d: %s", rlog,
+                    sblog, line, cudaGetErrorString(e));
     }
     c->rb_bytes = bytes;
     c->device_bytes += bytes;
     c->graph_dirty = true;
     return MLEM_OK;
+}
+
+bool region_ready(const mlem_ctx* c, int frame_tile) {
+    int rlog = 0, sblog = 0;
+    uint32_t gpw = 0;
+    region_params(frame_tile, c->C, &rlog, &sblog, &gpw);
+    return c->rb.el_fw && c->rb.rlog == rlog && c->rb.sblog == sblog && c->rb.gpw == gpw;
 }
 
 // ---------------------------------------------------------------------------
@@ -340,6 +355,18 @@ int finish_create(mlem_ctx* c) {
     double s = 0.0;
     for (uint32_t i = 0; i < c->C; ++i) s += c->norm_host[i];
     c->sumnorm = s;
+    // Row visiting order, from the device column indices (after the remap).
+    if (!(c->flags & MLEM_FLAG_NO_ROW_ORDER) && c->R > 1) {
+        uint32_t* order = nullptr;
+        TRY(dev_alloc(c, &order, c->R));
+        const cudaError_t e = row_order_build(csr_view(c), c->C, order, c->stream);
+        if (e != cudaSuccess) {
+            cudaFree(order);
+            c->device_bytes -= (size_t)c->R * 4;
+            CK(c, e);
+        }
+        c->row_order = order;
+    }
     default_tuning(c);
     return MLEM_OK;
 }
@@ -362,7 +389,8 @@ int new_ctx(mlem_ctx** out, uint32_t R, uint32_t C, uint64_t Z, uint32_t flags, 
                     e != cudaSuccess ? cudaGetErrorString(e) : "0 devices");
     if (device < 0 || device >= n_dev)
         return fail(nullptr, MLEM_ERR_INVALID, "device %d out of range (%d devices)", device, n_dev);
-    if (flags & ~(MLEM_FLAG_EXACT | MLEM_FLAG_NO_CSC | MLEM_FLAG_CHECKED | MLEM_FLAG_NATURAL_LAYOUT))
+    if (flags & ~(MLEM_FLAG_EXACT | MLEM_FLAG_NO_CSC | MLEM_FLAG_CHECKED | MLEM_FLAG_NATURAL_LAYOUT |
+                  MLEM_FLAG_NO_ROW_ORDER))
         return fail(nullptr, MLEM_ERR_INVALID, "unknown flags 0x%x", flags);
     if ((flags & MLEM_FLAG_EXACT) && (flags & MLEM_FLAG_NO_CSC))
         return fail(nullptr, MLEM_ERR_INVALID, "MLEM_FLAG_EXACT needs the CSC copy");
@@ -479,9 +507,17 @@ int mark(mlem_ctx* c, const PhaseEvents* pe, int i) {
     return MLEM_OK;
 }
 
+// The CSR as the row kernels of tuning t walk it.
+SparseView csr_visit(const mlem_ctx* c, const mlem_tuning& t) {
+    SparseView v = csr_view(c);
+    if (t.visit == MLEM_VISIT_FILE) v.order = nullptr;
+    v.blocked = v.order && t.visit == MLEM_VISIT_SORTED_BLOCKED;
+    return v;
+}
+
 int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                       const PhaseEvents* pe = nullptr) {
-    const SparseView csr = csr_view(c);
+    const SparseView csr = csr_visit(c, t);
     const uint32_t Bp = c->Bp;
     cudaStream_t st = c->stream;
     TRY(mark(c, pe, 0));
@@ -520,17 +556,17 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                 CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
                 break;
             case MLEM_BK_REGION:
-                if (!c->rb.el || c->rb.rlog != region_rlog(t.frame_tile, c->C))
+                if (!region_ready(c, t.frame_tile))
                     return fail(c, MLEM_ERR_STATE, "region-blocked copy not built for this frame tile");
                 CK(c, cudaMemsetAsync(c->correl, 0, (size_t)c->R * Bp * 4, st));
                 for (uint32_t f0 = 0; f0 < Bp; f0 += T)
                     CK(c, region_fwproj(c->rb, c->x, Bp, f0, c->C, c->correl, cfg, st));
                 CK(c, correl_inplace(c->correl, c->sino, (uint64_t)c->R * Bp, st));
                 TRY(mark(c, pe, 1));
+                // back projection with calcUpdate applied per region (no update vector)
                 for (uint32_t f0 = 0; f0 < Bp; f0 += T)
-                    CK(c, region_bkproj(c->rb, c->correl, Bp, f0, c->C, c->update, cfg, st));
+                    CK(c, region_bkproj_update(c->rb, c->correl, Bp, f0, c->C, c->norm, c->x, cfg, st));
                 TRY(mark(c, pe, 2));
-                CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
                 break;
             default:
                 return fail(c, MLEM_ERR_INVALID, "unknown back-projection mode %d", t.bk_mode);
@@ -558,15 +594,15 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
     for (int p = 0; p < MLEM_N_PHASES; ++p) { bytes[p] = 0.0; launches[p] = 0; }
     const int nt = (int)tiles;
     if (mode == MLEM_BK_REGION) {
-        // elements (padded to chunks), chunk segments, segment rows, per pass
-        const double NC = (double)c->rb.nchunks, S = (double)c->rb.nseg;
-        const double pass = 256.0 * NC + 4.0 * NC + 4.0 * S;
-        bytes[0] = tiles * pass + B * (4.0 * C + 4.0 * R) + B * 12.0 * R;  // x, f, correl pass
-        bytes[1] = tiles * pass + B * (4.0 * R + 4.0 * C);                  // c, update
-        bytes[2] = 4.0 * C + B * (4.0 * C + 8.0 * C + 4.0 * C);             // calcUpdate
+        // one region-major element copy and the segment rows per pass; per
+        // segment one partial (forward) or one correlation (backward) of B
+        // floats; x once, fw zeroing + correl pass over R x B
+        const double S = (double)c->rb.nseg, ZR = (double)c->rb.nel;
+        const double pass = 8.0 * ZR + 4.0 * S;
+        bytes[0] = tiles * pass + B * (4.0 * C + 4.0 * S) + B * 16.0 * R;
+        bytes[1] = tiles * pass + B * (4.0 * S + 8.0 * C) + 4.0 * C;  // c per segment, x r/w, norm
         launches[0] = nt + 1;
         launches[1] = nt;
-        launches[2] = 1;
         bytes[3] = 4.0 * C * B;
         launches[3] = 2;
         return;
@@ -796,7 +832,7 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->hist_zeros, (void*)c->hist_subn, (void*)c->tmp_r[0],
                     (void*)c->tmp_r[1], (void*)c->tmp_c[0], (void*)c->tmp_c[1], (void*)c->tmp_c[2],
                     (void*)c->tmp_sino, (void*)c->tmp_d, (void*)c->norm_nat, (void*)c->perm,
-                    (void*)c->pscratch[0], (void*)c->pscratch[1]})
+                    (void*)c->pscratch[0], (void*)c->pscratch[1], (void*)c->row_order})
         dev_free(p);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -835,7 +871,7 @@ int mlem_kernels_per_iteration(const mlem_ctx* c, int* n) {
     if (c->flags & MLEM_FLAG_EXACT) k += 2;
     else if (c->tuning.bk_mode == MLEM_BK_CSC) k += 2 * tiles;
     else if (c->tuning.bk_mode == MLEM_BK_ATOMIC) k += 2 * tiles + 1;
-    else if (c->tuning.bk_mode == MLEM_BK_REGION) k += 2 * tiles + 2;
+    else if (c->tuning.bk_mode == MLEM_BK_REGION) k += 2 * tiles + 1;  // + correl
     else k += tiles + 1;
     *n = k;
     return MLEM_OK;
@@ -911,7 +947,7 @@ int mlem_calc_fwproj(mlem_ctx* c, const float* image, float* out) {
     if (c->flags & MLEM_FLAG_EXACT)
         CK(c, fwproj_exact(csr_view(c), xd, 1, nullptr, nullptr, c->tmp_r[0], c->stream));
     else
-        CK(c, fwproj(csr_view(c), xd, 1, 0, nullptr, nullptr, c->tmp_r[0], cfg_for_frames(c, 1),
+        CK(c, fwproj(csr_visit(c, c->tuning), xd, 1, 0, nullptr, nullptr, c->tmp_r[0], cfg_for_frames(c, 1),
                      c->stream));
     CK(c, cudaMemcpyAsync(out, c->tmp_r[0], (size_t)c->R * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
@@ -946,7 +982,7 @@ int mlem_calc_bkproj(mlem_ctx* c, const float* correl, float* update) {
                          cfg_for_frames(c, 1), c->stream));
     } else {
         CK(c, cudaMemsetAsync(ud, 0, (size_t)c->C * 4, c->stream));
-        CK(c, bkproj_scatter(csr_view(c), c->tmp_r[0], 1, 0, ud, cfg_for_frames(c, 1), c->stream));
+        CK(c, bkproj_scatter(csr_visit(c, c->tuning), c->tmp_r[0], 1, 0, ud, cfg_for_frames(c, 1), c->stream));
     }
     if (c->bricked) CK(c, permute_to_natural(ud, c->tmp_c[0], c->perm, c->C, 1, c->stream));
     CK(c, cudaMemcpyAsync(update, c->tmp_c[0], (size_t)c->C * 4, cudaMemcpyDeviceToHost, c->stream));
@@ -1139,6 +1175,11 @@ int mlem_set_tuning(mlem_ctx* c, const mlem_tuning* t) {
     if (c->Bp && (c->Bp % (uint32_t)n.frame_tile))
         return fail(c, MLEM_ERR_INVALID, "frame tile %d does not divide the padded frame count %u",
                     n.frame_tile, c->Bp);
+    if (n.visit < MLEM_VISIT_FILE || n.visit > MLEM_VISIT_SORTED_BLOCKED)
+        return fail(c, MLEM_ERR_INVALID, "unknown row visiting order %d", n.visit);
+    if (n.visit != MLEM_VISIT_FILE && !c->row_order)
+        return fail(c, MLEM_ERR_INVALID,
+                    "sorted row visiting needs the row order (context made with MLEM_FLAG_NO_ROW_ORDER)");
     if (n.bk_mode == MLEM_BK_REGION) {
         TRY(set_device(c));
         TRY(ensure_region(c, n.frame_tile));
@@ -1179,12 +1220,18 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
             for (int tile : {1, 2, 4, 8, 16}) {
                 if (c->Bp % (uint32_t)tile) continue;
                 if (mode == MLEM_BK_REGION) {
-                    if (group != 32) continue;  // warp-wide kernels: the group is not used
-                    TRY(ensure_region(c, tile));
+                    if (group != 32) continue;  // lane groups follow the tile: no group
+                    if (ensure_region(c, tile) != MLEM_OK) continue;  // e.g. no memory: skip
                 }
-                for (int bps : {4, 8}) {
+                for (int bps : {4, 8})
+                for (int visit : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED, MLEM_VISIT_SORTED_BLOCKED}) {
                     if (mode == MLEM_BK_REGION && bps == 4) continue;  // grid is fixed by the tile
-                    mlem_tuning t{mode, group, tile, bps, 0.0};
+                    // the sorted orders need the row order; the region method has its
+                    // own layout; only the one-pass kernel walks blocked runs
+                    if (visit != MLEM_VISIT_FILE && (!c->row_order || mode == MLEM_BK_REGION))
+                        continue;
+                    if (visit == MLEM_VISIT_SORTED_BLOCKED && mode != MLEM_BK_FUSED) continue;
+                    mlem_tuning t{mode, group, tile, bps, visit, 0.0};
                     // warm-up once, then time two iterations
                     int s = enqueue_iteration(c, t, false);
                     if (s != MLEM_OK) { c->tuning = orig; return s; }
@@ -1228,7 +1275,7 @@ int mlem_fwproj_d(mlem_ctx* c, const float* x, float* y, uint32_t B, void* strea
     }
     const LaunchCfg cfg = cfg_for_frames(c, B);
     for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
-        CK(c, fwproj(csr_view(c), xd, B, f0, nullptr, nullptr, y, cfg, st));
+        CK(c, fwproj(csr_visit(c, c->tuning), xd, B, f0, nullptr, nullptr, y, cfg, st));
     return MLEM_OK;
 }
 
@@ -1247,7 +1294,7 @@ int mlem_bkproj_d(mlem_ctx* c, const float* y, float* x, uint32_t B, void* strea
             CK(c, bkproj_csc(csc_view(c), y, B, f0, nullptr, nullptr, xd, cfg, st));
         } else {
             if (f0 == 0) CK(c, cudaMemsetAsync(xd, 0, (size_t)c->C * B * 4, st));
-            CK(c, bkproj_scatter(csr_view(c), y, B, f0, xd, cfg, st));
+            CK(c, bkproj_scatter(csr_visit(c, c->tuning), y, B, f0, xd, cfg, st));
         }
     }
     if (c->bricked) CK(c, permute_to_natural(xd, x, c->perm, c->C, B, st));
@@ -1267,7 +1314,7 @@ int mlem_fwproj_correl_d(mlem_ctx* c, const float* x, const int32_t* sino, float
     }
     const LaunchCfg cfg = cfg_for_frames(c, B);
     for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
-        CK(c, fwproj(csr_view(c), xd, B, f0, sino, correl, nullptr, cfg, st));
+        CK(c, fwproj(csr_visit(c, c->tuning), xd, B, f0, sino, correl, nullptr, cfg, st));
     return MLEM_OK;
 }
 
@@ -1347,8 +1394,11 @@ struct mlem_batch {
     int device = 0;
     int n_sm = 148;
     cudaStream_t stream = nullptr;               // the first context's stream
-    std::vector<std::vector<uint64_t>> row_ptr;  // host copies, for cutting items
+    // Element prefix of each matrix in file order and in sorted order (empty
+    // without a row order), for cutting items of equal cost.
+    std::vector<std::vector<uint64_t>> pre_file, pre_sorted;
     int policy = MLEM_BATCH_INTERLEAVED;
+    int visit = MLEM_VISIT_FILE;
     int tile = 0;  // frames per pass, shared by the batch
     uint32_t items_per_block = 4;
     int blocks_per_sm = 4;  // k_batch_fused is bounded to 64 registers: 4 x 256 threads per SM
@@ -1418,7 +1468,9 @@ int batch_default_tile(const mlem_batch* b) {
 // row's offsets, sinogram entries and sums.
 double item_cost(const mlem_batch* b, size_t i, uint32_t r0, uint32_t r1) {
     const mlem_ctx* c = b->ctx[i];
-    const double nnz = (double)(b->row_ptr[i][r1] - b->row_ptr[i][r0]);
+    const std::vector<uint64_t>& pre =
+        (b->visit != MLEM_VISIT_FILE && !b->pre_sorted[i].empty()) ? b->pre_sorted[i] : b->pre_file[i];
+    const double nnz = (double)(pre[r1] - pre[r0]);
     const double passes = (double)(c->Bp / (uint32_t)b->tile);
     return nnz * (8.0 * passes + 8.0 * c->Bp) + (double)(r1 - r0) * (16.0 + 8.0 * c->Bp);
 }
@@ -1504,7 +1556,10 @@ int batch_refresh(mlem_batch* b, int chunk) {
         if (c->stream != b->stream) BCK(b, cudaStreamSynchronize(c->stream));
         TRY(bctx(b, c, ensure_history(c, chunk)));
         if (t.mats[i].Bp != c->Bp) reschedule = true;
-        t.mats[i] = BatchMat{csr_view(c), c->x, c->sino, c->update, c->Bp, 0u};
+        SparseView v = csr_view(c);
+        if (b->visit == MLEM_VISIT_FILE) v.order = nullptr;
+        v.blocked = v.order && b->visit == MLEM_VISIT_SORTED_BLOCKED && b->policy == MLEM_BATCH_ITEMS;
+        t.mats[i] = BatchMat{v, c->x, c->sino, c->update, c->Bp, 0u};
         t.row_base[i + 1] = t.row_base[i] + c->R;
         for (const void* p : {(const void*)c->x, (const void*)c->sino, (const void*)c->update,
                               (const void*)c->norm, (const void*)c->stats_scratch,
@@ -1642,17 +1697,27 @@ int mlem_batch_create(mlem_batch** out, mlem_ctx* const* ctxs, uint32_t n_ctx) {
     };
     if (cudaSetDevice(b->device) != cudaSuccess)
         return bail(bfail(b, MLEM_ERR_CUDA, "cudaSetDevice(%d) failed", b->device));
-    b->row_ptr.resize(n_ctx);
+    b->pre_file.resize(n_ctx);
+    b->pre_sorted.resize(n_ctx);
     for (uint32_t i = 0; i < n_ctx; ++i) {
         mlem_ctx* c = ctxs[i];
-        b->row_ptr[i].resize((size_t)c->R + 1);
+        std::vector<uint64_t>& pre = b->pre_file[i];
+        pre.resize((size_t)c->R + 1);
+        std::vector<uint32_t> order(c->row_order ? c->R : 0);
         cudaError_t e = cudaStreamSynchronize(c->stream);
         if (e == cudaSuccess)
-            e = cudaMemcpy(b->row_ptr[i].data(), c->row_ptr, ((size_t)c->R + 1) * 8,
-                           cudaMemcpyDeviceToHost);
+            e = cudaMemcpy(pre.data(), c->row_ptr, ((size_t)c->R + 1) * 8, cudaMemcpyDeviceToHost);
+        if (e == cudaSuccess && c->row_order)
+            e = cudaMemcpy(order.data(), c->row_order, (size_t)c->R * 4, cudaMemcpyDeviceToHost);
         if (e != cudaSuccess)
             return bail(bfail(b, MLEM_ERR_CUDA, "row offsets of context %u: %s", i,
                               cudaGetErrorString(e)));
+        if (c->row_order) {  // element prefix in sorted order (for the sorted visits)
+            std::vector<uint64_t>& ps = b->pre_sorted[i];
+            ps.resize((size_t)c->R + 1);
+            ps[0] = 0;
+            for (uint32_t k = 0; k < c->R; ++k) ps[k + 1] = ps[k] + (pre[order[k] + 1] - pre[order[k]]);
+        }
     }
     if (cudaMalloc(&b->counter, 256) != cudaSuccess) {
         cudaGetLastError();
@@ -1672,10 +1737,17 @@ void mlem_batch_destroy(mlem_batch* b) {
 }
 
 int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
-                            int blocks_per_sm, int frame_tile) {
+                            int blocks_per_sm, int frame_tile, int visit) {
     if (!b) return bfail(nullptr, MLEM_ERR_INVALID, "null batch");
     if (policy != MLEM_BATCH_INTERLEAVED && policy != MLEM_BATCH_ITEMS)
         return bfail(b, MLEM_ERR_INVALID, "unknown batch schedule %d", policy);
+    if (visit < MLEM_VISIT_FILE || visit > MLEM_VISIT_SORTED_BLOCKED)
+        return bfail(b, MLEM_ERR_INVALID, "unknown row visiting order %d", visit);
+    if (visit != MLEM_VISIT_FILE)
+        for (size_t i = 0; i < b->ctx.size(); ++i)
+            if (!b->ctx[i]->row_order)
+                return bfail(b, MLEM_ERR_INVALID,
+                             "sorted row visiting: context %zu has no row order (MLEM_FLAG_NO_ROW_ORDER)", i);
     if (items_per_block < 1 || items_per_block > 1024)
         return bfail(b, MLEM_ERR_INVALID, "items_per_block must be 1..1024 (got %u)", items_per_block);
     if (blocks_per_sm < 1 || blocks_per_sm > 32)
@@ -1686,6 +1758,7 @@ int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
                      "frame count", frame_tile);
     BCK(b, cudaSetDevice(b->device));
     b->policy = policy;
+    b->visit = visit;
     b->items_per_block = items_per_block;
     b->blocks_per_sm = blocks_per_sm;
     if (frame_tile != 0) b->tile = frame_tile;
@@ -1695,10 +1768,11 @@ int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
 }
 
 int mlem_batch_get_schedule(const mlem_batch* b, int* policy, uint32_t* items_per_block,
-                            int* blocks_per_sm, int* frame_tile, uint32_t* n_items,
+                            int* blocks_per_sm, int* frame_tile, int* visit, uint32_t* n_items,
                             double* ms_per_iter) {
     if (!b) return bfail(nullptr, MLEM_ERR_INVALID, "null batch");
     if (policy) *policy = b->policy;
+    if (visit) *visit = b->visit;
     if (items_per_block) *items_per_block = b->items_per_block;
     if (blocks_per_sm) *blocks_per_sm = b->blocks_per_sm;
     if (frame_tile) *frame_tile = b->tile;
@@ -1743,9 +1817,10 @@ int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter) {
         s = bfail(b, MLEM_ERR_CUDA, "event creation failed");
     uint32_t best_ipb = b->items_per_block;
     int best_bps = b->blocks_per_sm, best_tile = b->tile, best_policy = b->policy;
+    int best_visit = b->visit;
     double best = 1e30;
-    auto trial = [&](int policy, uint32_t ipb, int bps, int tile) -> int {
-        TRY(mlem_batch_set_schedule(b, policy, ipb, bps, tile));
+    auto trial = [&](int policy, uint32_t ipb, int bps, int tile, int visit) -> int {
+        TRY(mlem_batch_set_schedule(b, policy, ipb, bps, tile, visit));
         double ms = 0.0;
         TRY(batch_time(b, 2, e0, e1, &ms));
         TRY(restore());
@@ -1755,17 +1830,24 @@ int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter) {
             best_ipb = ipb;
             best_bps = bps;
             best_tile = tile;
+            best_visit = visit;
         }
         return MLEM_OK;
     };
-    // The frame tile with the interleaved schedule first, then the resident
-    // blocks, then the items schedule's granularity with that tile.
+    bool sorted_ok = true;
+    for (const mlem_ctx* c : b->ctx) sorted_ok = sorted_ok && c->row_order;
+    // The frame tile and the row order with the interleaved schedule first,
+    // then the resident blocks, then the items schedule with that tile.
     for (int t : {16, 8, 4, 2, 1})
-        if (s == MLEM_OK && tile_ok_all(b, t)) s = trial(MLEM_BATCH_INTERLEAVED, best_ipb, 4, t);
+        for (int v : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED})
+            if (s == MLEM_OK && tile_ok_all(b, t) && (v == MLEM_VISIT_FILE || sorted_ok))
+                s = trial(MLEM_BATCH_INTERLEAVED, best_ipb, 4, t, v);
     for (int bps : {3, 8})
-        if (s == MLEM_OK) s = trial(MLEM_BATCH_INTERLEAVED, best_ipb, bps, best_tile);
+        if (s == MLEM_OK) s = trial(MLEM_BATCH_INTERLEAVED, best_ipb, bps, best_tile, best_visit);
     for (uint32_t ipb : {1u, 4u, 16u, 64u})
-        if (s == MLEM_OK) s = trial(MLEM_BATCH_ITEMS, ipb, 4, best_tile);
+        for (int v : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED, MLEM_VISIT_SORTED_BLOCKED})
+            if (s == MLEM_OK && (v == MLEM_VISIT_FILE || sorted_ok))
+                s = trial(MLEM_BATCH_ITEMS, ipb, 4, best_tile, v);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (s == MLEM_OK) s = restore();
@@ -1773,7 +1855,7 @@ int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter) {
         s = bfail(b, MLEM_ERR_CUDA, "autotune: synchronize failed");
     release();
     if (s != MLEM_OK) return s;
-    TRY(mlem_batch_set_schedule(b, best_policy, best_ipb, best_bps, best_tile));
+    TRY(mlem_batch_set_schedule(b, best_policy, best_ipb, best_bps, best_tile, best_visit));
     b->ms_per_iter = best;
     if (ms_per_iter) *ms_per_iter = best;
     return MLEM_OK;

@@ -167,7 +167,8 @@ int run(int argc, char** argv) {
         check(mlem_autotune(ctx, std::strcmp(tune, "any") == 0 ? 0 : 1, &t), ctx);
         if (!csv)
             std::cout << "Autotuned: mode " << t.bk_mode << ", group " << t.group << ", frame tile "
-                      << t.frame_tile << ", " << t.ms_per_iter << " ms/iteration\n";
+                      << t.frame_tile << ", row visit " << t.visit << ", " << t.ms_per_iter
+                      << " ms/iteration\n";
     }
     if (!csv) std::cout << "Starting " << (o.iterations - first) << " MLEM iterations" << std::endl;
 

@@ -1,0 +1,87 @@
+// k_order.cu -- the row visiting order of the row kernels.
+//
+// A grid-stride row kernel runs neighbouring rows at the same time: the 8
+// warps of a block take 8 consecutive rows.  The rows of a Siddon matrix
+// (LORs) are random lines, so in file order those 8 rays share almost no
+// voxels and every image gather misses L1.  Sorting the rows by the Morton
+// interleave of (entry voxel, exit voxel) -- the first and last element of
+// the row, whose device indices are already a Morton code of the voxel --
+// puts rays with nearby endpoints next to each other: nearly coincident rays
+// whose gathers hit the same cache lines.  For a matrix without geometry the
+// key is still a valid (harmless) permutation.  Results change only by the
+// order of the scatter atomics, which is unordered anyway.
+#include <cub/device/device_radix_sort.cuh>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "kernels.h"
+
+namespace mlem {
+
+namespace {
+
+// Spread the 32 bits of v over the even bits of a 64-bit word.
+__device__ __forceinline__ uint64_t spread2(uint32_t v) {
+    uint64_t x = v;
+    x = (x | (x << 16)) & 0x0000FFFF0000FFFFull;
+    x = (x | (x << 8)) & 0x00FF00FF00FF00FFull;
+    x = (x | (x << 4)) & 0x0F0F0F0F0F0F0F0Full;
+    x = (x | (x << 2)) & 0x3333333333333333ull;
+    x = (x | (x << 1)) & 0x5555555555555555ull;
+    return x;
+}
+
+__global__ void k_row_keys(SparseView csr, uint64_t* __restrict__ key, uint32_t* __restrict__ idx) {
+    const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
+    for (uint64_t r = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; r < csr.n;
+         r += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t b = csr.ptr[r], e = csr.ptr[r + 1];
+        uint64_t k = ~0ull;  // empty rows last
+        if (e > b) {
+            const uint32_t a = el[b].x, z = el[e - 1].x;
+            const uint32_t lo = a < z ? a : z, hi = a < z ? z : a;  // direction-free
+            k = (spread2(hi) << 1) | spread2(lo);
+        }
+        key[r] = k;
+        idx[r] = (uint32_t)r;
+    }
+}
+
+}  // namespace
+
+cudaError_t row_order_build(const SparseView& csr, uint32_t C, uint32_t* order, cudaStream_t st) {
+    const uint64_t n = csr.n;
+    if (n == 0) return cudaSuccess;
+    int bits = 1;
+    while (bits < 32 && (1ull << bits) < (uint64_t)C) ++bits;
+    const int end_bit = std::min(64, 2 * bits);
+    uint64_t *key = nullptr, *key_sorted = nullptr;
+    uint32_t* idx = nullptr;
+    void* tmp = nullptr;
+    size_t tmp_bytes = 0;
+    cudaError_t e = cudaMalloc(&key, n * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&key_sorted, n * 8);
+    if (e == cudaSuccess) e = cudaMalloc(&idx, n * 4);
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key, key_sorted, idx, order,
+                                            (int64_t)n, 0, end_bit, st);
+    if (e == cudaSuccess) e = cudaMalloc(&tmp, std::max<size_t>(tmp_bytes, 256));
+    if (e == cudaSuccess) {
+        const int grid = (int)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
+        k_row_keys<<<grid, 256, 0, st>>>(csr, key, idx);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess)
+        e = cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, key, key_sorted, idx, order,
+                                            (int64_t)n, 0, end_bit, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) cudaGetLastError();
+    cudaFree(key);
+    cudaFree(key_sorted);
+    cudaFree(idx);
+    cudaFree(tmp);
+    return e;
+}
+
+}  // namespace mlem

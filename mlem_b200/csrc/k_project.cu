@@ -50,8 +50,9 @@ __global__ void __launch_bounds__(256) k_fwproj(SparseView csr, const float* __r
     MLEM_WARP_LOOP_SETUP
     const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
     for (uint64_t base = warp * RPW; base < csr.n; base += nwarps * RPW) {
-        const uint64_t r = base + lw / G;
-        const bool active = r < csr.n;
+        const uint64_t v = base + lw / G;
+        const bool active = v < csr.n;
+        const uint64_t r = active ? row_at(csr, v) : 0;
         uint64_t b = 0, e = 0;
         if (active) { b = csr.ptr[r]; e = csr.ptr[r + 1]; }
         float acc[VW];
@@ -119,8 +120,9 @@ __global__ void __launch_bounds__(256) k_bkproj_scatter(SparseView csr,
     constexpr int EPS = G / FL;
     const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
     for (uint64_t base = warp * RPW; base < csr.n; base += nwarps * RPW) {
-        const uint64_t r = base + lw / G;
-        if (r >= csr.n) continue;  // no shuffles in this kernel
+        const uint64_t v = base + lw / G;
+        if (v >= csr.n) continue;  // no shuffles in this kernel
+        const uint64_t r = row_at(csr, v);
         const uint64_t b = csr.ptr[r], e = csr.ptr[r + 1];
         float cv[VW];
         ld_vec<VW>(c + r * B + f0 + sub * VW, cv, ph);

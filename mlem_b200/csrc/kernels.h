@@ -20,7 +20,21 @@ struct SparseView {
     const uint4* pairs;   // elements as 16-byte pairs
     uint32_t n;           // rows (CSR) or columns (CSC)
     uint64_t nnz;
+    // Row kernels visit rows in this order when non-null: the k-th row a
+    // grid-stride walk reaches is order[k] (a permutation of [0, n)).  Only
+    // the visiting order changes; every vector stays indexed by row.
+    const uint32_t* order = nullptr;
+    // Row kernels that support it (the one-pass kernel): each warp walks one
+    // contiguous run of visiting positions instead of a grid stride, so that
+    // its consecutive rows (neighbours in `order`) re-use its L1 lines while
+    // the warps running beside it work on other rows.
+    bool blocked = false;
 };
+
+// Row index of visiting position v.
+__host__ __device__ inline uint64_t row_at(const SparseView& s, uint64_t v) {
+    return s.order ? (uint64_t)s.order[v] : v;
+}
 
 // Per-matrix launch configuration (chosen by the autotuner).
 struct LaunchCfg {
@@ -121,6 +135,14 @@ size_t transpose_scratch_bytes(uint32_t C);
 cudaError_t transpose(const SparseView& csr, uint32_t C, uint64_t* col_ptr, uint2* celems,
                       void* scratch, uint32_t* max_col_len, cudaStream_t st);
 
+// ---- row visiting order (k_order.cu) -------------------------------------------
+// order[k]: rows sorted by a key that interleaves the bits of the device
+// column indices of each row's first and last element (a ray's entry and
+// exit voxels for a geometric matrix, which the device voxel order makes
+// spatially coherent), so rows visited together share image lines in L1.
+// `order` holds csr.n entries; temporary memory is allocated and freed here.
+cudaError_t row_order_build(const SparseView& csr, uint32_t C, uint32_t* order, cudaStream_t st);
+
 // ---- matrix validation: every column < C and offsets non-decreasing ------
 cudaError_t validate_csr(const SparseView& csr, uint32_t C, unsigned int* bad_flag,
                          cudaStream_t st);
@@ -138,49 +160,65 @@ cudaError_t siddon_fill(const SiddonSpec& s, const uint64_t* row_ptr, uint2* ele
 cudaError_t project_f64(const SparseView& csr, const float* x, double* out, cudaStream_t st);
 
 // ---- region-blocked method (k_region.cu) -----------------------------------
-// Rows cut into segments, one per region (aligned block of 2^rlog device
-// voxels); elements stored region by region, each region padded to whole
-// 32-element chunks: {voxel index inside the region | head flag (bit 31) on
-// a segment's first element, value}.  seg_row[s]: row of segment s;
-// chunk_seg[c]: segment of chunk c's first element.
+// Rows cut into segments, one per region (aligned block of RS = 2^rlog device
+// voxels), segments ordered by region.  Two region-major copies of the
+// elements, {word, value} with word = (segment index inside the region <<
+// rlog) | voxel index inside the region:
+//   el_fw: segment-major (the rows' element order inside each segment);
+//   el_bk: per block of SB = 2^sblog consecutive segments of a region,
+//          voxel-major.
+// Both are stored per block in span tiles: gpw spans of 16 consecutive
+// elements, element k of every span of a tile side by side (one coalesced
+// warp load per step); blocks are padded to whole tiles with value-0 copies.
+// seg_row[s]: row of segment s (region order).
 struct RegionView {
-    const uint64_t* reg_chunk_ptr;  // nreg+1 chunk ranges
-    const uint2* el;
+    const uint32_t* reg_order;    // nreg regions, most elements first
+    const uint64_t* reg_seg_ptr;  // nreg+1 segment ranges
+    const uint64_t* reg_el_ptr;   // nreg+1 element ranges
+    const uint32_t* reg_blk_ptr;  // nreg+1 block ranges
+    const uint64_t* blk_el_ptr;   // nblk+1 element ranges
     const uint32_t* seg_row;
-    const uint32_t* chunk_seg;
-    uint64_t nchunks;
+    const uint2* el_fw;
+    const uint2* el_bk;
     uint32_t nreg;
-    int rlog;
+    int rlog, sblog;
 };
 
 struct RegionBlocks {
-    uint64_t* reg_chunk_ptr = nullptr;
-    uint2* el = nullptr;
+    uint32_t* reg_order = nullptr;
+    uint64_t* reg_seg_ptr = nullptr;
+    uint64_t* reg_el_ptr = nullptr;
+    uint32_t* reg_blk_ptr = nullptr;
+    uint64_t* blk_el_ptr = nullptr;
     uint32_t* seg_row = nullptr;
-    uint32_t* chunk_seg = nullptr;
-    uint64_t nchunks = 0;
-    uint32_t nreg = 0;
-    int rlog = 0;
-    uint64_t nseg = 0;
+    uint2* el_fw = nullptr;
+    uint2* el_bk = nullptr;
+    uint32_t nreg = 0, nblk = 0;
+    uint64_t nseg = 0, nel = 0;  // nel: elements of one copy, padding included
+    int rlog = 0, sblog = 0;
+    uint32_t gpw = 0;            // lane groups per warp the copies are interleaved for
     RegionView view() const {
-        return RegionView{reg_chunk_ptr, el, seg_row, chunk_seg, nchunks, nreg, rlog};
+        return RegionView{reg_order, reg_seg_ptr, reg_el_ptr, reg_blk_ptr, blk_el_ptr,
+                          seg_row,   el_fw,       el_bk,      nreg,        rlog,       sblog};
     }
 };
 
-// Shared memory of one region tile: 2^rlog voxels x frame_tile floats.
+// Shared memory of one image / update tile (RS x BT floats) at most.
 constexpr size_t kRegionTileBytes = 65536;
-// Region size (log2 voxels) for a frame tile and C voxels.
-int region_rlog(int frame_tile, uint32_t C);
+// Region size (log2 voxels), segment block size (log2) and lane groups per
+// warp for a frame tile and C voxels.
+void region_params(int frame_tile, uint32_t C, int* rlog, int* sblog, uint32_t* gpw);
 // failed_line (nullable) receives the k_region.cu line of a failing step.
-cudaError_t region_build(const SparseView& csr, uint32_t C, int rlog, RegionBlocks* out,
-                         size_t* bytes, int* failed_line, cudaStream_t st);
+cudaError_t region_build(const SparseView& csr, uint32_t C, int rlog, int sblog, uint32_t gpw,
+                         RegionBlocks* out, size_t* bytes, int* failed_line, cudaStream_t st);
 void region_free(RegionBlocks* rb);
 // fw[row][f] += segment partial projections (fw zeroed by the caller).
 cudaError_t region_fwproj(const RegionBlocks& rb, const float* x, uint32_t B, uint32_t f0,
                           uint32_t C, float* fw, const LaunchCfg& cfg, cudaStream_t st);
-// u[col][f] += (A^T c)[col][f] (u zeroed by the caller).
-cudaError_t region_bkproj(const RegionBlocks& rb, const float* c, uint32_t B, uint32_t f0,
-                          uint32_t C, float* u, const LaunchCfg& cfg, cudaStream_t st);
+// x[col][f] *= calcUpdate factor((A^T c)[col][f], norm[col]) for the frames of the tile.
+cudaError_t region_bkproj_update(const RegionBlocks& rb, const float* c, uint32_t B, uint32_t f0,
+                                 uint32_t C, const float* norm, float* x, const LaunchCfg& cfg,
+                                 cudaStream_t st);
 // f[i] = calcCorrel(s[i], f[i]).
 cudaError_t correl_inplace(float* f, const int32_t* s, uint64_t n, cudaStream_t st);
 

@@ -54,17 +54,21 @@ def _check(ctxs, members):
             assert ob.rel_l2(got[b], want[b]) <= TOL_MLEM, (m.n_rows, b)
 
 
-@pytest.mark.parametrize("policy,items_per_block,blocks_per_sm,tile", [
-    (api.BATCH_INTERLEAVED, 4, 4, 0), (api.BATCH_INTERLEAVED, 1, 3, 1),
-    (api.BATCH_INTERLEAVED, 1, 8, 4), (api.BATCH_ITEMS, 4, 4, 0), (api.BATCH_ITEMS, 1, 3, 4),
-    (api.BATCH_ITEMS, 32, 4, 2), (api.BATCH_ITEMS, 2, 1, 1), (api.BATCH_ITEMS, 1024, 8, 4)])
-def test_batch_matches_oracle(members, policy, items_per_block, blocks_per_sm, tile):
+IL, IT = api.BATCH_INTERLEAVED, api.BATCH_ITEMS
+FILE, SORTED, BLOCKED = api.VISIT_FILE, api.VISIT_SORTED, api.VISIT_SORTED_BLOCKED
+
+
+@pytest.mark.parametrize("policy,items_per_block,blocks_per_sm,tile,visit", [
+    (IL, 4, 4, 0, FILE), (IL, 1, 3, 1, SORTED), (IL, 1, 8, 4, FILE), (IL, 1, 4, 2, BLOCKED),
+    (IT, 4, 4, 0, FILE), (IT, 1, 3, 4, SORTED), (IT, 32, 4, 2, BLOCKED), (IT, 2, 1, 1, FILE),
+    (IT, 1024, 8, 4, SORTED), (IT, 16, 4, 4, BLOCKED)])
+def test_batch_matches_oracle(members, policy, items_per_block, blocks_per_sm, tile, visit):
     ctxs = _contexts(members)
     try:
         with api.Batch(ctxs) as b:
-            b.set_schedule(policy, items_per_block, blocks_per_sm, tile)
+            b.set_schedule(policy, items_per_block, blocks_per_sm, tile, visit)
             sched = b.schedule()
-            assert sched["policy"] == policy
+            assert sched["policy"] == policy and sched["visit"] == visit
             if policy == api.BATCH_ITEMS:
                 assert sched["n_items"] >= len(ctxs)
             if tile:
@@ -137,6 +141,7 @@ def test_batch_follows_new_sinograms(members):
 
 def test_batch_rejects_bad_input(members):
     ctxs = _contexts(members)
+    unsorted = _contexts(members[:1], flags=api.FLAG_NO_ROW_ORDER)[0]
     m = members[0][0]
     exact = api.Context.from_matrix(m, flags=api.FLAG_EXACT)
     exact.set_sinograms(members[0][1])
@@ -162,8 +167,13 @@ def test_batch_rejects_bad_input(members):
                 b.set_schedule(api.BATCH_INTERLEAVED, 4, 4, 3)
             with pytest.raises(api.MlemError):
                 b.set_schedule(7, 4, 4, 0)
+            with pytest.raises(api.MlemError):
+                b.set_schedule(IL, 4, 4, 0, 9)
             b.iterate(ITERS)  # still usable after the rejected calls
         _check(ctxs, members)
+        with api.Batch([unsorted] + ctxs[1:]) as b:
+            with pytest.raises(api.MlemError):  # a context without a row order
+                b.set_schedule(IL, 4, 4, 0, SORTED)
     finally:
-        for c in ctxs + [exact, bare]:
+        for c in ctxs + [exact, bare, unsorted]:
             c.close()

@@ -75,11 +75,13 @@ MODES = [api.BK_CSC, api.BK_ATOMIC, api.BK_FUSED, api.BK_REGION]
 
 
 @pytest.mark.parametrize("name", CASES)
-@pytest.mark.parametrize("mode", MODES)
-def test_mlem_matches_reference_image(ctxs, name, mode):
+@pytest.mark.parametrize("mode,visit", [(m, api.VISIT_FILE) for m in MODES] + [
+    (api.BK_CSC, api.VISIT_SORTED), (api.BK_ATOMIC, api.VISIT_SORTED),
+    (api.BK_FUSED, api.VISIT_SORTED), (api.BK_FUSED, api.VISIT_SORTED_BLOCKED)])
+def test_mlem_matches_reference_image(ctxs, name, mode, visit):
     ctx, m, sino, iters, gold = ctxs[name]
     ctx.set_sinograms(sino)
-    ctx.set_tuning(bk_mode=mode, group=32, frame_tile=1, blocks_per_sm=8)
+    ctx.set_tuning(bk_mode=mode, group=32, frame_tile=1, blocks_per_sm=8, visit=visit)
     ctx.init_images()
     sums, zeros, _ = ctx.iterate(iters)
     img = ctx.get_images()[0]
@@ -219,6 +221,11 @@ def test_invalid_inputs_raise():
             ctx.set_tuning(bk_mode=api.BK_CSC, group=6, frame_tile=1)
         with pytest.raises(api.MlemError):
             ctx.set_tuning(bk_mode=api.BK_CSC, group=32, frame_tile=3)
+        with pytest.raises(api.MlemError):
+            ctx.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=1, visit=3)
+    with api.Context(re_, el, 2, 2, flags=api.FLAG_NO_ROW_ORDER) as ctx:
+        with pytest.raises(api.MlemError):  # no row order to visit in
+            ctx.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=1, visit=api.VISIT_SORTED)
 
 
 def test_autotune_restores_images(ctxs):
@@ -235,11 +242,14 @@ def test_autotune_restores_images(ctxs):
 
 @pytest.mark.parametrize("name", CASES)
 def test_brick_layout_changes_no_result(golden, name):
-    """The device brick layout only relabels voxels: CSC-mode images, the
-    CSR/CSC copies and the column sums are bit-identical to natural order."""
+    """The device voxel layout only relabels voxels and the row order only
+    changes the order rows are visited in: CSC-mode images (per-row and
+    per-column sums in a fixed order), the CSR/CSC copies and the column sums
+    are bit-identical to natural voxel order and file row order."""
     m, sino, iters, gold, _ = golden.case(name)
     out = []
-    for flags in (0, api.FLAG_NATURAL_LAYOUT):
+    for flags in (0, api.FLAG_NATURAL_LAYOUT, api.FLAG_NO_ROW_ORDER,
+                  api.FLAG_NATURAL_LAYOUT | api.FLAG_NO_ROW_ORDER):
         with api.Context.from_matrix(m, flags=flags) as ctx:
             ctx.set_sinograms(sino)
             ctx.set_tuning(bk_mode=api.BK_CSC, group=32, frame_tile=1, blocks_per_sm=8)
@@ -247,7 +257,33 @@ def test_brick_layout_changes_no_result(golden, name):
             ctx.iterate(iters)
             out.append((ctx.get_images().tobytes(), ctx.column_sums().tobytes(),
                         ctx.csc()[1].tobytes(), ctx.csr()[1].tobytes()))
-    assert out[0] == out[1]
+    assert all(o == out[0] for o in out)
+
+
+@pytest.mark.parametrize("frames", [1, 16])
+def test_row_order_changes_only_rounding(golden, frames):
+    """The sorted row visits move only the order of the scatter atomics: the
+    images agree with file order within float rounding, and with the oracle
+    within the MLEM tolerance."""
+    m, sino, iters, gold, _ = golden.case("plain_small_it10")
+    sinos = np.stack([np.roll(sino, 7 * b) for b in range(frames)]).astype(np.int32)
+    want = [ob.mlem(m, sinos[b], iters)[0] for b in range(frames)]
+    runs = [(api.BK_ATOMIC, api.VISIT_FILE), (api.BK_ATOMIC, api.VISIT_SORTED),
+            (api.BK_FUSED, api.VISIT_FILE), (api.BK_FUSED, api.VISIT_SORTED),
+            (api.BK_FUSED, api.VISIT_SORTED_BLOCKED)]
+    imgs = []
+    with api.Context.from_matrix(m) as ctx:
+        ctx.set_sinograms(sinos)
+        for mode, visit in runs:
+            ctx.set_tuning(bk_mode=mode, group=32, frame_tile=min(frames, 8), blocks_per_sm=8,
+                           visit=visit)
+            ctx.init_images()
+            ctx.iterate(iters)
+            imgs.append(ctx.get_images())
+    for img in imgs:
+        for b in range(frames):
+            assert ob.rel_l2(img[b], imgs[0][b]) <= 1e-5
+            assert ob.rel_l2(img[b], want[b]) <= TOL_MLEM
 
 
 def test_device_pointer_api_in_natural_order(small_ctx=None):
