@@ -9,7 +9,9 @@ MLEM iteration (forward projection + correlation + back projection + update,
 plus the per-iteration image-sum census the reference prints).  The matrix
 (6.2 GB) is larger than the 126 MB L2, so no L2 flush is needed between
 steps.  The batched line ("batched-b16") runs 16 sinograms over the same
-matrix in one pass per iteration.
+matrix in one pass per iteration; the "uneven" line batches three matrices
+of different geometry (12, 8 and 4 sinograms) in one kernel per iteration
+(mlem_b200.uneven).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -49,6 +51,8 @@ def parse_args():
     ap.add_argument("--mode", choices=["auto", "csc", "atomic", "fused", "region"], default="auto",
                     help="back-projection method; auto = autotuned")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true",
+                    help="skip the uneven three-geometry batch (one GPU only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=3)
     return ap.parse_args()
@@ -271,7 +275,7 @@ def run_ours(a, rank, world, local_rank):
         api.BK_CSC: ("k_fwproj", "k_bkproj_csc", "-", "k_stats"),
         api.BK_ATOMIC: ("k_fwproj", "k_bkproj_scatter", "k_apply_update", "k_stats"),
         api.BK_FUSED: ("k_fused_row", "-", "k_apply_update", "k_stats"),
-        api.BK_REGION: ("k_rb_fwproj", "k_rb_bkproj", "-", "k_stats"),
+        api.BK_REGION: ("k_rb_fwproj", "k_rb_bkproj", "-", "k_stats"),  # bkproj applies the update
     }[tuning["bk_mode"]]
     traffic = committed_traffic().get(kernel_names[dom])
     achieved = ph_bytes[dom] / (ph_ms[dom] / 1e3) / 1e9
@@ -294,6 +298,7 @@ def run_ours(a, rank, world, local_rank):
                    "n_cols": ctx.n_cols, "nnz": int(ctx.nnz), "frames": 1,
                    "bk_mode": api.BK_NAMES[tuning["bk_mode"]], "group": tuning["group"],
                    "frame_tile": tuning["frame_tile"], "blocks_per_sm": tuning["blocks_per_sm"],
+                   "row_visit": api.VISIT_NAMES[tuning["visit"]],
                    "l2": "inputs larger than L2 (6.2 GB matrix), no flush",
                    "parallelism": "replicas" if world > 1 else "single"},
         "hbm_gbs": round(total_bytes / (ms_per_step / 1e3) / 1e9, 1),
@@ -327,7 +332,7 @@ def run_ours(a, rank, world, local_rank):
             "per_frame_speedup_vs_plain": round((16 / bms) / (1 / ms_per_step), 3),
             "hbm_gbs": round(float(bph_bytes.sum()) / (bms / 1e3) / 1e9, 1),
             "bk_mode": api.BK_NAMES[tb["bk_mode"]], "group": tb["group"],
-            "frame_tile": tb["frame_tile"],
+            "frame_tile": tb["frame_tile"], "row_visit": api.VISIT_NAMES[tb["visit"]],
             "phases_ms": [round(float(x), 4) for x in bph_ms],
         }
 
@@ -336,6 +341,13 @@ def run_ours(a, rank, world, local_rank):
         line["cpu_baseline"] = cpu_baseline_from_ctx(ctx, frames.sinograms[0], g, a.cpu_iters)
 
     ctx.close()
+
+    # --- uneven batch over three geometries (12 + 8 + 4 frames), one GPU ---
+    if world == 1 and not a.no_uneven:
+        from mlem_b200 import uneven
+        torch.cuda.synchronize()
+        line["uneven"] = uneven.run(iters=max(10, min(a.steps, 20)), warmup=3, device=local_rank)
+
     if dist is not None:
         dist.destroy_process_group()
     return line

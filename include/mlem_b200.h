@@ -89,7 +89,7 @@ typedef struct {
     int group;          /* lanes per row/column: 4, 8, 16 or 32 */
     int frame_tile;     /* frames per pass over the matrix: 1, 2, 4, 8 or 16 */
     int blocks_per_sm;  /* 1..8 blocks of 256 threads per SM */
-    int visit;          /* row visiting order: MLEM_VISIT_FILE, _SORTED or _SORTED_BLOCKED */
+    int visit;          /* row visiting order: MLEM_VISIT_FILE, _SORTED or _SORTED_CHUNKED */
     double ms_per_iter; /* measured by mlem_autotune; 0 when set by hand */
 } mlem_tuning;
 
@@ -98,7 +98,8 @@ typedef struct {
  * by the order of the scatter atomics. */
 #define MLEM_VISIT_FILE 0           /* file order, grid stride */
 #define MLEM_VISIT_SORTED 1         /* rows sorted by entry/exit voxel, grid stride */
-#define MLEM_VISIT_SORTED_BLOCKED 2 /* sorted; each warp walks one contiguous run (one-pass kernel) */
+#define MLEM_VISIT_SORTED_CHUNKED 2 /* sorted; CTAs take chunks of neighbouring rows from a counter
+                                       (one-pass method, group 32) */
 
 /* ---- errors ------------------------------------------------------------- */
 const char* mlem_last_error(const mlem_ctx* ctx);
@@ -294,9 +295,9 @@ const char* mlem_batch_last_error(const mlem_batch* b);
 /* policy: MLEM_BATCH_INTERLEAVED or MLEM_BATCH_ITEMS; items_per_block (1..1024,
  * items schedule): about that many items for every resident block
  * (blocks_per_sm x SMs); frame_tile in {1,2,4,8,16} dividing every context's
- * padded frame count (0 keeps the current tile); visit: MLEM_VISIT_* row
- * order of every matrix (the sorted ones need every context's row order;
- * MLEM_VISIT_SORTED_BLOCKED walks runs only in the items schedule). */
+ * padded frame count (0 keeps the current tile); visit: MLEM_VISIT_FILE or
+ * MLEM_VISIT_SORTED for every matrix (sorted needs every context's row
+ * order; with the items schedule a sorted item is a run of neighbouring rows). */
 int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
                             int blocks_per_sm, int frame_tile, int visit);
 /* Current schedule; any pointer may be NULL.  n_items: 0 for the interleaved

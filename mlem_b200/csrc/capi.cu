@@ -56,6 +56,7 @@ struct mlem_ctx {
     // Visiting order of the row kernels (row_order_build): rays with nearby
     // entry and exit voxels next to each other.  Null with MLEM_FLAG_NO_ROW_ORDER.
     uint32_t* row_order = nullptr;
+    unsigned int* counter = nullptr;  // work counter of the dynamically scheduled kernels
 
     // frames
     uint32_t B = 0, Bp = 0;
@@ -355,6 +356,7 @@ int finish_create(mlem_ctx* c) {
     double s = 0.0;
     for (uint32_t i = 0; i < c->C; ++i) s += c->norm_host[i];
     c->sumnorm = s;
+    TRY(dev_alloc(c, &c->counter, 64));
     // Row visiting order, from the device column indices (after the remap).
     if (!(c->flags & MLEM_FLAG_NO_ROW_ORDER) && c->R > 1) {
         uint32_t* order = nullptr;
@@ -511,8 +513,15 @@ int mark(mlem_ctx* c, const PhaseEvents* pe, int i) {
 SparseView csr_visit(const mlem_ctx* c, const mlem_tuning& t) {
     SparseView v = csr_view(c);
     if (t.visit == MLEM_VISIT_FILE) v.order = nullptr;
-    v.blocked = v.order && t.visit == MLEM_VISIT_SORTED_BLOCKED;
     return v;
+}
+
+// Rows per chunk of MLEM_VISIT_SORTED_CHUNKED: about 16 chunks for every
+// resident CTA (4 per SM; measured best on the plain-full matrix with 16
+// frames), at least 32 rows.
+uint32_t chunk_rows_of(const mlem_ctx* c) {
+    const uint64_t ctas = (uint64_t)c->n_sm * 4;
+    return (uint32_t)std::max<uint64_t>(32, (c->R + ctas * 16 - 1) / (ctas * 16));
 }
 
 int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
@@ -549,8 +558,12 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                 CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
                 break;
             case MLEM_BK_FUSED:
-                for (uint32_t f0 = 0; f0 < Bp; f0 += T)
-                    CK(c, fused_row(csr, c->x, Bp, f0, c->sino, c->update, cfg, st));
+                if (t.visit == MLEM_VISIT_SORTED_CHUNKED)
+                    CK(c, fused_chunked(csr, c->x, Bp, t.frame_tile, c->sino, c->update,
+                                        chunk_rows_of(c), c->counter, c->n_sm, st));
+                else
+                    for (uint32_t f0 = 0; f0 < Bp; f0 += T)
+                        CK(c, fused_row(csr, c->x, Bp, f0, c->sino, c->update, cfg, st));
                 TRY(mark(c, pe, 1));
                 TRY(mark(c, pe, 2));
                 CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
@@ -609,7 +622,7 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
     }
     if (mode == MLEM_BK_FUSED) {
         bytes[0] = tiles * csr_pass + B * (4.0 * C + 4.0 * R + 4.0 * C);  // x, sino, update
-        launches[0] = nt;
+        launches[0] = (!exact && c->tuning.visit == MLEM_VISIT_SORTED_CHUNKED) ? 1 : nt;
     } else {
         bytes[0] = tiles * csr_pass + B * (4.0 * C + 4.0 * R + 4.0 * R);  // x, sino, correl
         launches[0] = exact ? 1 : nt;
@@ -832,7 +845,8 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->hist_zeros, (void*)c->hist_subn, (void*)c->tmp_r[0],
                     (void*)c->tmp_r[1], (void*)c->tmp_c[0], (void*)c->tmp_c[1], (void*)c->tmp_c[2],
                     (void*)c->tmp_sino, (void*)c->tmp_d, (void*)c->norm_nat, (void*)c->perm,
-                    (void*)c->pscratch[0], (void*)c->pscratch[1], (void*)c->row_order})
+                    (void*)c->pscratch[0], (void*)c->pscratch[1], (void*)c->row_order,
+                    (void*)c->counter})
         dev_free(p);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -872,6 +886,7 @@ int mlem_kernels_per_iteration(const mlem_ctx* c, int* n) {
     else if (c->tuning.bk_mode == MLEM_BK_CSC) k += 2 * tiles;
     else if (c->tuning.bk_mode == MLEM_BK_ATOMIC) k += 2 * tiles + 1;
     else if (c->tuning.bk_mode == MLEM_BK_REGION) k += 2 * tiles + 1;  // + correl
+    else if (c->tuning.visit == MLEM_VISIT_SORTED_CHUNKED) k += 2;  // all tiles in one launch
     else k += tiles + 1;
     *n = k;
     return MLEM_OK;
@@ -1175,11 +1190,13 @@ int mlem_set_tuning(mlem_ctx* c, const mlem_tuning* t) {
     if (c->Bp && (c->Bp % (uint32_t)n.frame_tile))
         return fail(c, MLEM_ERR_INVALID, "frame tile %d does not divide the padded frame count %u",
                     n.frame_tile, c->Bp);
-    if (n.visit < MLEM_VISIT_FILE || n.visit > MLEM_VISIT_SORTED_BLOCKED)
+    if (n.visit < MLEM_VISIT_FILE || n.visit > MLEM_VISIT_SORTED_CHUNKED)
         return fail(c, MLEM_ERR_INVALID, "unknown row visiting order %d", n.visit);
     if (n.visit != MLEM_VISIT_FILE && !c->row_order)
         return fail(c, MLEM_ERR_INVALID,
                     "sorted row visiting needs the row order (context made with MLEM_FLAG_NO_ROW_ORDER)");
+    if (n.visit == MLEM_VISIT_SORTED_CHUNKED && n.group != 32)
+        return fail(c, MLEM_ERR_INVALID, "the chunked row visit runs 32 lanes per row (group 32)");
     if (n.bk_mode == MLEM_BK_REGION) {
         TRY(set_device(c));
         TRY(ensure_region(c, n.frame_tile));
@@ -1224,13 +1241,15 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
                     if (ensure_region(c, tile) != MLEM_OK) continue;  // e.g. no memory: skip
                 }
                 for (int bps : {4, 8})
-                for (int visit : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED, MLEM_VISIT_SORTED_BLOCKED}) {
+                for (int visit : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED, MLEM_VISIT_SORTED_CHUNKED}) {
                     if (mode == MLEM_BK_REGION && bps == 4) continue;  // grid is fixed by the tile
                     // the sorted orders need the row order; the region method has its
-                    // own layout; only the one-pass kernel walks blocked runs
+                    // own layout; only the one-pass method walks chunks
                     if (visit != MLEM_VISIT_FILE && (!c->row_order || mode == MLEM_BK_REGION))
                         continue;
-                    if (visit == MLEM_VISIT_SORTED_BLOCKED && mode != MLEM_BK_FUSED) continue;
+                    if (visit == MLEM_VISIT_SORTED_CHUNKED && mode != MLEM_BK_FUSED) continue;
+                    // chunked: warp-wide rows, resident grid (group and blocks fixed)
+                    if (visit == MLEM_VISIT_SORTED_CHUNKED && (group != 32 || bps != 8)) continue;
                     mlem_tuning t{mode, group, tile, bps, visit, 0.0};
                     // warm-up once, then time two iterations
                     int s = enqueue_iteration(c, t, false);
@@ -1558,7 +1577,6 @@ int batch_refresh(mlem_batch* b, int chunk) {
         if (t.mats[i].Bp != c->Bp) reschedule = true;
         SparseView v = csr_view(c);
         if (b->visit == MLEM_VISIT_FILE) v.order = nullptr;
-        v.blocked = v.order && b->visit == MLEM_VISIT_SORTED_BLOCKED && b->policy == MLEM_BATCH_ITEMS;
         t.mats[i] = BatchMat{v, c->x, c->sino, c->update, c->Bp, 0u};
         t.row_base[i + 1] = t.row_base[i] + c->R;
         for (const void* p : {(const void*)c->x, (const void*)c->sino, (const void*)c->update,
@@ -1741,8 +1759,8 @@ int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
     if (!b) return bfail(nullptr, MLEM_ERR_INVALID, "null batch");
     if (policy != MLEM_BATCH_INTERLEAVED && policy != MLEM_BATCH_ITEMS)
         return bfail(b, MLEM_ERR_INVALID, "unknown batch schedule %d", policy);
-    if (visit < MLEM_VISIT_FILE || visit > MLEM_VISIT_SORTED_BLOCKED)
-        return bfail(b, MLEM_ERR_INVALID, "unknown row visiting order %d", visit);
+    if (visit != MLEM_VISIT_FILE && visit != MLEM_VISIT_SORTED)
+        return bfail(b, MLEM_ERR_INVALID, "row visiting order %d is not a batch order", visit);
     if (visit != MLEM_VISIT_FILE)
         for (size_t i = 0; i < b->ctx.size(); ++i)
             if (!b->ctx[i]->row_order)
@@ -1845,7 +1863,7 @@ int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter) {
     for (int bps : {3, 8})
         if (s == MLEM_OK) s = trial(MLEM_BATCH_INTERLEAVED, best_ipb, bps, best_tile, best_visit);
     for (uint32_t ipb : {1u, 4u, 16u, 64u})
-        for (int v : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED, MLEM_VISIT_SORTED_BLOCKED})
+        for (int v : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED})
             if (s == MLEM_OK && (v == MLEM_VISIT_FILE || sorted_ok))
                 s = trial(MLEM_BATCH_ITEMS, ipb, 4, best_tile, v);
     if (e0) cudaEventDestroy(e0);

@@ -77,7 +77,53 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_interleaved(const Ba
     }
 }
 
+// One matrix in dynamically scheduled chunks of consecutive visiting
+// positions (the items schedule with uniform items and no item list).
+template <int BT>
+__global__ void __launch_bounds__(kBatchThreads, 4) k_fused_chunked(SparseView csr,
+                                                                     const float* __restrict__ x,
+                                                                     uint32_t B,
+                                                                     const int32_t* __restrict__ sino,
+                                                                     float* __restrict__ u,
+                                                                     uint32_t chunk,
+                                                                     unsigned int* __restrict__ counter) {
+    __shared__ uint32_t s_chunk;
+    const uint64_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint64_t nchunks = (csr.n + chunk - 1) / chunk;
+    for (;;) {
+        if (threadIdx.x == 0) s_chunk = atomicAdd(counter, 1u);
+        __syncthreads();
+        const uint64_t ci = s_chunk;
+        __syncthreads();  // s_chunk is rewritten by the next grab
+        if (ci >= nchunks) return;  // block-uniform
+        const uint64_t r0 = ci * chunk, r1 = r0 + chunk < csr.n ? r0 + chunk : csr.n;
+#pragma unroll 1
+        for (uint32_t f0 = 0; f0 < B; f0 += BT)
+            fused_row_range<32, BT>(csr, x, B, f0, sino, u, r0, r1, warp, nwarps);
+    }
+}
+
 }  // namespace
+
+cudaError_t fused_chunked(const SparseView& csr, const float* x, uint32_t B, int frame_tile,
+                          const int32_t* sino, float* u, uint32_t chunk_rows,
+                          unsigned int* counter, int sm_count, cudaStream_t st) {
+    if (csr.n == 0) return cudaSuccess;
+    if (chunk_rows == 0 || (uint64_t)(csr.n + chunk_rows - 1) / chunk_rows > 0xffffffffull)
+        return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
+    if (e != cudaSuccess) return e;
+    const int grid = std::max(1, sm_count * 4);  // the resident CTAs (64 registers, 256 threads)
+    switch (frame_tile) {
+        case 1: k_fused_chunked<1><<<grid, kBatchThreads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
+        case 2: k_fused_chunked<2><<<grid, kBatchThreads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
+        case 4: k_fused_chunked<4><<<grid, kBatchThreads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
+        case 8: k_fused_chunked<8><<<grid, kBatchThreads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
+        case 16: k_fused_chunked<16><<<grid, kBatchThreads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
+        default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
 
 cudaError_t batch_interleaved(const BatchTable& t, int frame_tile, int sm_count,
                               int blocks_per_sm, cudaStream_t st) {

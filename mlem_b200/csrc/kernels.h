@@ -24,11 +24,6 @@ struct SparseView {
     // grid-stride walk reaches is order[k] (a permutation of [0, n)).  Only
     // the visiting order changes; every vector stays indexed by row.
     const uint32_t* order = nullptr;
-    // Row kernels that support it (the one-pass kernel): each warp walks one
-    // contiguous run of visiting positions instead of a grid stride, so that
-    // its consecutive rows (neighbours in `order`) re-use its L1 lines while
-    // the warps running beside it work on other rows.
-    bool blocked = false;
 };
 
 // Row index of visiting position v.
@@ -256,6 +251,14 @@ static_assert(sizeof(BatchTable) <= 32764, "kernel parameter space (CUDA >= 12.1
 cudaError_t batch_fused(const BatchTable& t, const BatchItem* items, uint32_t n_items,
                         unsigned int* counter, int frame_tile, int sm_count, int blocks_per_sm,
                         cudaStream_t st);
+// One matrix in chunks (MLEM_VISIT_SORTED_CHUNKED): CTAs take chunks of
+// chunk_rows consecutive visiting positions from `counter` (reset here on the
+// stream), and do every frame tile of a chunk's rows back to back -- each CTA
+// stays on neighbouring rows for many steps (L1 reuse of their voxels) while
+// the grid as a whole moves through one window of the order.
+cudaError_t fused_chunked(const SparseView& csr, const float* x, uint32_t B, int frame_tile,
+                          const int32_t* sino, float* u, uint32_t chunk_rows,
+                          unsigned int* counter, int sm_count, cudaStream_t st);
 // Interleaved schedule: the same work in grid-stride order over the virtual
 // row space.
 cudaError_t batch_interleaved(const BatchTable& t, int frame_tile, int sm_count,

@@ -171,17 +171,9 @@ __device__ __forceinline__ void fused_row_range(const SparseView& csr, const flo
     const int sub = lane % FL;
     const uint64_t ps = l2_evict_first(), ph = l2_evict_last();
     const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
-    uint64_t start = r_begin + warp * RPW, stop = r_end, step = nwarps * RPW;
-    if (csr.blocked) {  // one contiguous run of whole RPW-row steps per warp
-        const uint64_t steps = (r_end - r_begin + RPW - 1) / RPW;
-        const uint64_t per = (steps + nwarps - 1) / nwarps * RPW;
-        start = r_begin + warp * per;
-        stop = start + per < r_end ? start + per : r_end;
-        step = RPW;
-    }
-    for (uint64_t base = start; base < stop; base += step) {
+    for (uint64_t base = r_begin + warp * RPW; base < r_end; base += nwarps * RPW) {
         const uint64_t v = base + lw / G;  // visiting position
-        const bool active = v < stop;
+        const bool active = v < r_end;
         const uint64_t r = active ? row_at(csr, v) : 0;
         uint64_t b = 0, e = 0;
         if (active) { b = csr.ptr[r]; e = csr.ptr[r + 1]; }

@@ -48,7 +48,9 @@ def _time_ms(stream, fn, reps):
 
 
 def _best_solo(ctx, stream, api):
-    """Fastest one-pass (MLEM_BK_FUSED) tuning of one context on its own."""
+    """Fastest one-pass (MLEM_BK_FUSED) tuning of one context on its own, over
+    the same choices the batch has (frame tile, row visiting order) plus the
+    lanes per row and resident blocks of the single-matrix kernel."""
     saved = ctx.get_images()
     padded = next(p for p in (1, 2, 4, 8, 16, 32, 48, 64) if ctx.n_frames <= p)
     best = None
@@ -57,12 +59,16 @@ def _best_solo(ctx, stream, api):
             continue
         for group in (16, 32):
             for bps in (4, 8):
-                ctx.set_tuning(bk_mode=api.BK_FUSED, group=group, frame_tile=tile,
-                               blocks_per_sm=bps)
-                ctx.iterate(1, stats=False)
-                ms = _time_ms(stream, lambda k: ctx.iterate(k, stats=False), 2)
-                if best is None or ms < best[0]:
-                    best = (ms, dict(group=group, frame_tile=tile, blocks_per_sm=bps))
+                for visit in (api.VISIT_FILE, api.VISIT_SORTED, api.VISIT_SORTED_CHUNKED):
+                    if visit == api.VISIT_SORTED_CHUNKED and group != 32:
+                        continue
+                    ctx.set_tuning(bk_mode=api.BK_FUSED, group=group, frame_tile=tile,
+                                   blocks_per_sm=bps, visit=visit)
+                    ctx.iterate(1, stats=False)
+                    ms = _time_ms(stream, lambda k: ctx.iterate(k, stats=False), 2)
+                    if best is None or ms < best[0]:
+                        best = (ms, dict(group=group, frame_tile=tile, blocks_per_sm=bps,
+                                         visit=visit))
     ctx.set_tuning(bk_mode=api.BK_FUSED, **best[1])
     ctx.set_images(saved)
     return best[1]

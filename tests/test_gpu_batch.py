@@ -55,13 +55,13 @@ def _check(ctxs, members):
 
 
 IL, IT = api.BATCH_INTERLEAVED, api.BATCH_ITEMS
-FILE, SORTED, BLOCKED = api.VISIT_FILE, api.VISIT_SORTED, api.VISIT_SORTED_BLOCKED
+FILE, SORTED = api.VISIT_FILE, api.VISIT_SORTED
 
 
 @pytest.mark.parametrize("policy,items_per_block,blocks_per_sm,tile,visit", [
-    (IL, 4, 4, 0, FILE), (IL, 1, 3, 1, SORTED), (IL, 1, 8, 4, FILE), (IL, 1, 4, 2, BLOCKED),
-    (IT, 4, 4, 0, FILE), (IT, 1, 3, 4, SORTED), (IT, 32, 4, 2, BLOCKED), (IT, 2, 1, 1, FILE),
-    (IT, 1024, 8, 4, SORTED), (IT, 16, 4, 4, BLOCKED)])
+    (IL, 4, 4, 0, FILE), (IL, 1, 3, 1, SORTED), (IL, 1, 8, 4, FILE), (IL, 1, 4, 2, SORTED),
+    (IT, 4, 4, 0, FILE), (IT, 1, 3, 4, SORTED), (IT, 32, 4, 2, SORTED), (IT, 2, 1, 1, FILE),
+    (IT, 1024, 8, 4, SORTED), (IT, 16, 4, 4, SORTED)])
 def test_batch_matches_oracle(members, policy, items_per_block, blocks_per_sm, tile, visit):
     ctxs = _contexts(members)
     try:
@@ -169,6 +169,8 @@ def test_batch_rejects_bad_input(members):
                 b.set_schedule(7, 4, 4, 0)
             with pytest.raises(api.MlemError):
                 b.set_schedule(IL, 4, 4, 0, 9)
+            with pytest.raises(api.MlemError):  # a single-matrix order only
+                b.set_schedule(IT, 4, 4, 0, api.VISIT_SORTED_CHUNKED)
             b.iterate(ITERS)  # still usable after the rejected calls
         _check(ctxs, members)
         with api.Batch([unsorted] + ctxs[1:]) as b:

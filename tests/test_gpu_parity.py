@@ -77,7 +77,7 @@ MODES = [api.BK_CSC, api.BK_ATOMIC, api.BK_FUSED, api.BK_REGION]
 @pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("mode,visit", [(m, api.VISIT_FILE) for m in MODES] + [
     (api.BK_CSC, api.VISIT_SORTED), (api.BK_ATOMIC, api.VISIT_SORTED),
-    (api.BK_FUSED, api.VISIT_SORTED), (api.BK_FUSED, api.VISIT_SORTED_BLOCKED)])
+    (api.BK_FUSED, api.VISIT_SORTED), (api.BK_FUSED, api.VISIT_SORTED_CHUNKED)])
 def test_mlem_matches_reference_image(ctxs, name, mode, visit):
     ctx, m, sino, iters, gold = ctxs[name]
     ctx.set_sinograms(sino)
@@ -270,7 +270,7 @@ def test_row_order_changes_only_rounding(golden, frames):
     want = [ob.mlem(m, sinos[b], iters)[0] for b in range(frames)]
     runs = [(api.BK_ATOMIC, api.VISIT_FILE), (api.BK_ATOMIC, api.VISIT_SORTED),
             (api.BK_FUSED, api.VISIT_FILE), (api.BK_FUSED, api.VISIT_SORTED),
-            (api.BK_FUSED, api.VISIT_SORTED_BLOCKED)]
+            (api.BK_FUSED, api.VISIT_SORTED_CHUNKED)]
     imgs = []
     with api.Context.from_matrix(m) as ctx:
         ctx.set_sinograms(sinos)
