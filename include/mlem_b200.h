@@ -88,7 +88,8 @@ typedef struct {
     int bk_mode;        /* MLEM_BK_CSC, MLEM_BK_ATOMIC, MLEM_BK_FUSED or MLEM_BK_REGION */
     int group;          /* lanes per row/column: 4, 8, 16 or 32 */
     int frame_tile;     /* frames per pass over the matrix: 1, 2, 4, 8 or 16 */
-    int blocks_per_sm;  /* 1..8 blocks of 256 threads per SM */
+    int blocks_per_sm;  /* 1..8 blocks of 256 threads per SM (chunked visit: 1, 2 or 4 CTAs
+                           of 1024, 512 or 256 threads) */
     int visit;          /* row visiting order: MLEM_VISIT_FILE, _SORTED or _SORTED_CHUNKED */
     double ms_per_iter; /* measured by mlem_autotune; 0 when set by hand */
 } mlem_tuning;

@@ -56,6 +56,7 @@ struct mlem_ctx {
     // Visiting order of the row kernels (row_order_build): rays with nearby
     // entry and exit voxels next to each other.  Null with MLEM_FLAG_NO_ROW_ORDER.
     uint32_t* row_order = nullptr;
+    ulonglong2* row_ranges = nullptr;  // element range of each visited row (row_ranges_build)
     unsigned int* counter = nullptr;  // work counter of the dynamically scheduled kernels
 
     // frames
@@ -147,7 +148,7 @@ void dev_free(void* p) {
 
 SparseView csr_view(const mlem_ctx* c) {
     return SparseView{c->row_ptr, reinterpret_cast<const uint4*>(c->elems), c->R, c->Z,
-                      c->row_order};
+                      c->row_order, c->row_order ? c->row_ranges : nullptr};
 }
 SparseView csc_view(const mlem_ctx* c) {
     return SparseView{c->col_ptr, reinterpret_cast<const uint4*>(c->celems), c->C, c->Z};
@@ -368,6 +369,8 @@ int finish_create(mlem_ctx* c) {
             CK(c, e);
         }
         c->row_order = order;
+        TRY(dev_alloc(c, &c->row_ranges, c->R));
+        CK(c, row_ranges_build(csr_view(c), c->row_order, c->row_ranges, c->stream));
     }
     default_tuning(c);
     return MLEM_OK;
@@ -512,15 +515,22 @@ int mark(mlem_ctx* c, const PhaseEvents* pe, int i) {
 // The CSR as the row kernels of tuning t walk it.
 SparseView csr_visit(const mlem_ctx* c, const mlem_tuning& t) {
     SparseView v = csr_view(c);
-    if (t.visit == MLEM_VISIT_FILE) v.order = nullptr;
+    if (t.visit == MLEM_VISIT_FILE) {
+        v.order = nullptr;
+        v.vrange = nullptr;
+    }
     return v;
 }
 
-// Rows per chunk of MLEM_VISIT_SORTED_CHUNKED: about 16 chunks for every
-// resident CTA (4 per SM; measured best on the plain-full matrix with 16
-// frames), at least 32 rows.
-uint32_t chunk_rows_of(const mlem_ctx* c) {
-    const uint64_t ctas = (uint64_t)c->n_sm * 4;
+// MLEM_VISIT_SORTED_CHUNKED: resident CTAs per SM (blocks_per_sm 1, 2 or 4
+// picks CTAs of 1024, 512 or 256 threads; larger values mean 4) and rows per
+// chunk: about 16 chunks for every resident CTA (measured best on the
+// plain-full matrix with 16 frames), at least 32 rows.
+int chunk_ctas_per_sm(const mlem_tuning& t) {
+    return t.blocks_per_sm <= 1 ? 1 : t.blocks_per_sm == 2 ? 2 : 4;
+}
+uint32_t chunk_rows_of(const mlem_ctx* c, const mlem_tuning& t) {
+    const uint64_t ctas = (uint64_t)c->n_sm * chunk_ctas_per_sm(t);
     return (uint32_t)std::max<uint64_t>(32, (c->R + ctas * 16 - 1) / (ctas * 16));
 }
 
@@ -560,7 +570,8 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
             case MLEM_BK_FUSED:
                 if (t.visit == MLEM_VISIT_SORTED_CHUNKED)
                     CK(c, fused_chunked(csr, c->x, Bp, t.frame_tile, c->sino, c->update,
-                                        chunk_rows_of(c), c->counter, c->n_sm, st));
+                                        chunk_rows_of(c, t), chunk_ctas_per_sm(t), c->counter,
+                                        c->n_sm, st));
                 else
                     for (uint32_t f0 = 0; f0 < Bp; f0 += T)
                         CK(c, fused_row(csr, c->x, Bp, f0, c->sino, c->update, cfg, st));
@@ -846,7 +857,7 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->tmp_r[1], (void*)c->tmp_c[0], (void*)c->tmp_c[1], (void*)c->tmp_c[2],
                     (void*)c->tmp_sino, (void*)c->tmp_d, (void*)c->norm_nat, (void*)c->perm,
                     (void*)c->pscratch[0], (void*)c->pscratch[1], (void*)c->row_order,
-                    (void*)c->counter})
+                    (void*)c->row_ranges, (void*)c->counter})
         dev_free(p);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -1248,9 +1259,10 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
                     if (visit != MLEM_VISIT_FILE && (!c->row_order || mode == MLEM_BK_REGION))
                         continue;
                     if (visit == MLEM_VISIT_SORTED_CHUNKED && mode != MLEM_BK_FUSED) continue;
-                    // chunked: warp-wide rows, resident grid (group and blocks fixed)
-                    if (visit == MLEM_VISIT_SORTED_CHUNKED && (group != 32 || bps != 8)) continue;
-                    mlem_tuning t{mode, group, tile, bps, visit, 0.0};
+                    // chunked: warp-wide rows; CTAs per SM 4 (bps 4) or 1 (bps 8 -> 1 below)
+                    if (visit == MLEM_VISIT_SORTED_CHUNKED && group != 32) continue;
+                    mlem_tuning t{mode, group, tile,
+                                  visit == MLEM_VISIT_SORTED_CHUNKED && bps == 8 ? 1 : bps, visit, 0.0};
                     // warm-up once, then time two iterations
                     int s = enqueue_iteration(c, t, false);
                     if (s != MLEM_OK) { c->tuning = orig; return s; }
@@ -1576,7 +1588,10 @@ int batch_refresh(mlem_batch* b, int chunk) {
         TRY(bctx(b, c, ensure_history(c, chunk)));
         if (t.mats[i].Bp != c->Bp) reschedule = true;
         SparseView v = csr_view(c);
-        if (b->visit == MLEM_VISIT_FILE) v.order = nullptr;
+        if (b->visit == MLEM_VISIT_FILE) {
+            v.order = nullptr;
+            v.vrange = nullptr;
+        }
         t.mats[i] = BatchMat{v, c->x, c->sino, c->update, c->Bp, 0u};
         t.row_base[i + 1] = t.row_base[i] + c->R;
         for (const void* p : {(const void*)c->x, (const void*)c->sino, (const void*)c->update,

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_interleaved(const Ba
 // One matrix in dynamically scheduled chunks of consecutive visiting
 // positions (the items schedule with uniform items and no item list).
 template <int BT>
-__global__ void __launch_bounds__(kBatchThreads, 4) k_fused_chunked(SparseView csr,
+__global__ void __launch_bounds__(1024, 1) k_fused_chunked(SparseView csr,
                                                                      const float* __restrict__ x,
                                                                      uint32_t B,
                                                                      const int32_t* __restrict__ sino,
@@ -106,20 +106,22 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_fused_chunked(SparseView c
 }  // namespace
 
 cudaError_t fused_chunked(const SparseView& csr, const float* x, uint32_t B, int frame_tile,
-                          const int32_t* sino, float* u, uint32_t chunk_rows,
+                          const int32_t* sino, float* u, uint32_t chunk_rows, int ctas_per_sm,
                           unsigned int* counter, int sm_count, cudaStream_t st) {
     if (csr.n == 0) return cudaSuccess;
     if (chunk_rows == 0 || (uint64_t)(csr.n + chunk_rows - 1) / chunk_rows > 0xffffffffull)
         return cudaErrorInvalidValue;
+    if (ctas_per_sm != 1 && ctas_per_sm != 2 && ctas_per_sm != 4) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;
-    const int grid = std::max(1, sm_count * 4);  // the resident CTAs (64 registers, 256 threads)
+    // the resident CTAs: 64 registers x 1024 threads per SM, in 1, 2 or 4 CTAs
+    const int grid = std::max(1, sm_count * ctas_per_sm), threads = 1024 / ctas_per_sm;
     switch (frame_tile) {
-        case 1: k_fused_chunked<1><<<grid, kBatchThreads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
-        case 2: k_fused_chunked<2><<<grid, kBatchThreads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
-        case 4: k_fused_chunked<4><<<grid, kBatchThreads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
-        case 8: k_fused_chunked<8><<<grid, kBatchThreads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
-        case 16: k_fused_chunked<16><<<grid, kBatchThreads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
+        case 1: k_fused_chunked<1><<<grid, threads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
+        case 2: k_fused_chunked<2><<<grid, threads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
+        case 4: k_fused_chunked<4><<<grid, threads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
+        case 8: k_fused_chunked<8><<<grid, threads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
+        case 16: k_fused_chunked<16><<<grid, threads, 0, st>>>(csr, x, B, sino, u, chunk_rows, counter); break;
         default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

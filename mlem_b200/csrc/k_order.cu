@@ -48,7 +48,24 @@ __global__ void k_row_keys(SparseView csr, uint64_t* __restrict__ key, uint32_t*
     }
 }
 
+__global__ void k_row_ranges(SparseView csr, const uint32_t* __restrict__ order,
+                             ulonglong2* __restrict__ vrange) {
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < csr.n;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t r = order[k];
+        vrange[k] = make_ulonglong2(csr.ptr[r], csr.ptr[r + 1]);
+    }
+}
+
 }  // namespace
+
+cudaError_t row_ranges_build(const SparseView& csr, const uint32_t* order, ulonglong2* vrange,
+                             cudaStream_t st) {
+    if (csr.n == 0) return cudaSuccess;
+    const int grid = (int)std::min<uint64_t>((csr.n + 255) / 256, 148ull * 16);
+    k_row_ranges<<<grid, 256, 0, st>>>(csr, order, vrange);
+    return cudaGetLastError();
+}
 
 cudaError_t row_order_build(const SparseView& csr, uint32_t C, uint32_t* order, cudaStream_t st) {
     const uint64_t n = csr.n;

@@ -24,6 +24,9 @@ struct SparseView {
     // grid-stride walk reaches is order[k] (a permutation of [0, n)).  Only
     // the visiting order changes; every vector stays indexed by row.
     const uint32_t* order = nullptr;
+    // With `order`: vrange[k] = {ptr[order[k]], ptr[order[k] + 1]}, the
+    // element range of the k-th visited row in one load (no order -> ptr chain).
+    const ulonglong2* vrange = nullptr;
 };
 
 // Row index of visiting position v.
@@ -137,6 +140,9 @@ cudaError_t transpose(const SparseView& csr, uint32_t C, uint64_t* col_ptr, uint
 // spatially coherent), so rows visited together share image lines in L1.
 // `order` holds csr.n entries; temporary memory is allocated and freed here.
 cudaError_t row_order_build(const SparseView& csr, uint32_t C, uint32_t* order, cudaStream_t st);
+// vrange[k] = {ptr[order[k]], ptr[order[k] + 1]} for k < csr.n.
+cudaError_t row_ranges_build(const SparseView& csr, const uint32_t* order, ulonglong2* vrange,
+                             cudaStream_t st);
 
 // ---- matrix validation: every column < C and offsets non-decreasing ------
 cudaError_t validate_csr(const SparseView& csr, uint32_t C, unsigned int* bad_flag,
@@ -256,8 +262,10 @@ cudaError_t batch_fused(const BatchTable& t, const BatchItem* items, uint32_t n_
 // stream), and do every frame tile of a chunk's rows back to back -- each CTA
 // stays on neighbouring rows for many steps (L1 reuse of their voxels) while
 // the grid as a whole moves through one window of the order.
+// ctas_per_sm: 1, 2 or 4 resident CTAs of 1024, 512 or 256 threads (the
+// CTAs of one SM share its L1, a bigger CTA puts more neighbouring rows on it).
 cudaError_t fused_chunked(const SparseView& csr, const float* x, uint32_t B, int frame_tile,
-                          const int32_t* sino, float* u, uint32_t chunk_rows,
+                          const int32_t* sino, float* u, uint32_t chunk_rows, int ctas_per_sm,
                           unsigned int* counter, int sm_count, cudaStream_t st);
 // Interleaved schedule: the same work in grid-stride order over the virtual
 // row space.

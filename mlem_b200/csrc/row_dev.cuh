@@ -74,6 +74,46 @@ __device__ __forceinline__ void ld_counts(const int32_t* __restrict__ p, int32_t
     }
 }
 
+// L2 prefetch of the bytes [p, p + bytes) rounded out to 16-byte bounds (at
+// most 64 KiB): a hint -- nothing completes or waits on it.  The caller keeps
+// the rounded range inside the allocation (the element arrays carry a spare
+// 16 bytes).
+__device__ __forceinline__ void prefetch_l2(const void* p, uint64_t bytes) {
+    const uint64_t a0 = reinterpret_cast<uint64_t>(p) & ~15ull;
+    const uint64_t a1 = (reinterpret_cast<uint64_t>(p) + bytes + 15) & ~15ull;
+    const uint32_t n = (uint32_t)(a1 - a0 < 65536 ? a1 - a0 : 65536);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"(n) : "memory");
+}
+
+// Element range [b, e) and row index r of visiting position v.
+__device__ __forceinline__ void visit_range(const SparseView& csr, uint64_t v, uint64_t& r,
+                                            uint64_t& b, uint64_t& e) {
+    if (csr.vrange) {
+        const ulonglong2 q = csr.vrange[v];
+        r = csr.order[v];
+        b = q.x;
+        e = q.y;
+    } else {
+        r = row_at(csr, v);
+        b = csr.ptr[r];
+        e = csr.ptr[r + 1];
+    }
+}
+
+// Element range [b, e) of visiting position v (no row index).
+__device__ __forceinline__ void visit_bounds(const SparseView& csr, uint64_t v, uint64_t& b,
+                                             uint64_t& e) {
+    if (csr.vrange) {
+        const ulonglong2 q = csr.vrange[v];
+        b = q.x;
+        e = q.y;
+    } else {
+        const uint64_t r = row_at(csr, v);
+        b = csr.ptr[r];
+        e = csr.ptr[r + 1];
+    }
+}
+
 // u[...] += w * c[...] for VW floats (one vector reduction, 4..16 bytes).
 template <int VW>
 __device__ __forceinline__ void red_vec(float* __restrict__ p, float w, const float (&c)[VW]) {
@@ -174,9 +214,19 @@ __device__ __forceinline__ void fused_row_range(const SparseView& csr, const flo
     for (uint64_t base = r_begin + warp * RPW; base < r_end; base += nwarps * RPW) {
         const uint64_t v = base + lw / G;  // visiting position
         const bool active = v < r_end;
-        const uint64_t r = active ? row_at(csr, v) : 0;
-        uint64_t b = 0, e = 0;
-        if (active) { b = csr.ptr[r]; e = csr.ptr[r + 1]; }
+        uint64_t r = 0, b = 0, e = 0;
+        if (active) visit_range(csr, v, r, b, e);
+        // Sorted visits: the row this lane group takes next -- its range load
+        // goes out beside this row's, and its elements are prefetched into L2
+        // while this row is worked on.  (In file order the next row of a
+        // grid-stride walk is thousands of rows away and the prefetch only
+        // adds L2 requests: measured 2.49 -> 2.80 ms on the plain-full matrix.)
+        const uint64_t nv = v + nwarps * RPW;
+        if (csr.vrange && lane == 0 && nv < r_end) {
+            uint64_t nb, ne;
+            visit_bounds(csr, nv, nb, ne);
+            if (ne > nb) prefetch_l2(el + nb, (ne - nb) * 8);
+        }
         float acc[VW];
         uint2 kept[kBatch];
         const bool in_regs =
