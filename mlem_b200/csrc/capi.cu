@@ -1626,9 +1626,10 @@ int batch_enqueue(mlem_batch* b, bool stats, const PhaseEvents* pe = nullptr) {
     TRY(bmark(b, pe, 0));
     if (b->policy == MLEM_BATCH_ITEMS)
         BCK(b, batch_fused(b->table, b->items_d, (uint32_t)b->items.size(), b->counter, b->tile,
-                           b->n_sm, b->blocks_per_sm, st));
+                           b->visit == MLEM_VISIT_SORTED, b->n_sm, b->blocks_per_sm, st));
     else
-        BCK(b, batch_interleaved(b->table, b->tile, b->n_sm, b->blocks_per_sm, st));
+        BCK(b, batch_interleaved(b->table, b->tile, b->visit == MLEM_VISIT_SORTED, b->n_sm,
+                                 b->blocks_per_sm, st));
     TRY(bmark(b, pe, 1));
     TRY(bmark(b, pe, 2));
     for (mlem_ctx* c : b->ctx) BCK(b, apply_update(c->x, c->update, c->norm, c->C, c->Bp, true, st));

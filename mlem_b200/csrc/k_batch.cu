@@ -27,7 +27,7 @@ namespace {
 
 constexpr int kBatchThreads = 256;
 
-template <int BT>
+template <int BT, bool SORTED>
 __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_fused(const BatchTable t,
                                                                    const BatchItem* __restrict__ items,
                                                                    uint32_t n_items,
@@ -47,8 +47,8 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_fused(const BatchTab
         const uint32_t Bp = m.Bp;
 #pragma unroll 1
         for (uint32_t f0 = 0; f0 < Bp; f0 += BT)
-            fused_row_range<32, BT>(m.csr, m.x, Bp, f0, m.sino, m.u, item.row0, item.row1, warp,
-                                    nwarps);
+            fused_row_range<32, BT, SORTED>(m.csr, m.x, Bp, f0, m.sino, m.u, item.row0, item.row1,
+                                            warp, nwarps);
     }
 }
 
@@ -60,7 +60,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_fused(const BatchTab
 // matrix's.  Each row does all its frame tiles back to back.  The table is a
 // kernel parameter: it lives in the constant bank like k_fused_row's
 // arguments instead of taking registers.
-template <int BT>
+template <int BT, bool SORTED>
 __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_interleaved(const BatchTable t) {
     const uint64_t nw = ((uint64_t)gridDim.x * blockDim.x) >> 5;
     uint64_t v = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -72,7 +72,7 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_interleaved(const Ba
         const uint32_t Bp = t.mats[mi].Bp;
 #pragma unroll 1
         for (uint32_t f0 = 0; f0 < Bp; f0 += BT)
-            fused_row_range<32, BT>(t.mats[mi].csr, t.mats[mi].x, Bp, f0, t.mats[mi].sino,
+            fused_row_range<32, BT, SORTED>(t.mats[mi].csr, t.mats[mi].x, Bp, f0, t.mats[mi].sino,
                                     t.mats[mi].u, r, r + 1, 0, 1);
     }
 }
@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(1024, 1) k_fused_chunked(SparseView csr,
         const uint64_t r0 = ci * chunk, r1 = r0 + chunk < csr.n ? r0 + chunk : csr.n;
 #pragma unroll 1
         for (uint32_t f0 = 0; f0 < B; f0 += BT)
-            fused_row_range<32, BT>(csr, x, B, f0, sino, u, r0, r1, warp, nwarps);
+            fused_row_range<32, BT, true>(csr, x, B, f0, sino, u, r0, r1, warp, nwarps);
     }
 }
 
@@ -112,6 +112,7 @@ cudaError_t fused_chunked(const SparseView& csr, const float* x, uint32_t B, int
     if (chunk_rows == 0 || (uint64_t)(csr.n + chunk_rows - 1) / chunk_rows > 0xffffffffull)
         return cudaErrorInvalidValue;
     if (ctas_per_sm != 1 && ctas_per_sm != 2 && ctas_per_sm != 4) return cudaErrorInvalidValue;
+    if (!csr.order || !csr.vrange) return cudaErrorInvalidValue;  // a sorted visit
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;
     // the resident CTAs: 64 registers x 1024 threads per SM, in 1, 2 or 4 CTAs
@@ -127,39 +128,36 @@ cudaError_t fused_chunked(const SparseView& csr, const float* x, uint32_t B, int
     return cudaGetLastError();
 }
 
-cudaError_t batch_interleaved(const BatchTable& t, int frame_tile, int sm_count,
+#define MLEM_BATCH_TILES(KERNEL, ...)                                                \
+    switch (frame_tile) {                                                            \
+        case 1: (sorted ? KERNEL<1, true> : KERNEL<1, false>)<<<__VA_ARGS__; break;  \
+        case 2: (sorted ? KERNEL<2, true> : KERNEL<2, false>)<<<__VA_ARGS__; break;  \
+        case 4: (sorted ? KERNEL<4, true> : KERNEL<4, false>)<<<__VA_ARGS__; break;  \
+        case 8: (sorted ? KERNEL<8, true> : KERNEL<8, false>)<<<__VA_ARGS__; break;  \
+        case 16: (sorted ? KERNEL<16, true> : KERNEL<16, false>)<<<__VA_ARGS__; break; \
+        default: return cudaErrorInvalidValue;                                       \
+    }
+
+cudaError_t batch_interleaved(const BatchTable& t, int frame_tile, bool sorted, int sm_count,
                               int blocks_per_sm, cudaStream_t st) {
     if (t.n == 0 || t.n > kBatchTableMax) return cudaErrorInvalidValue;
     const int grid = std::max(1, sm_count * blocks_per_sm);
-    switch (frame_tile) {
-        case 1: k_batch_interleaved<1><<<grid, kBatchThreads, 0, st>>>(t); break;
-        case 2: k_batch_interleaved<2><<<grid, kBatchThreads, 0, st>>>(t); break;
-        case 4: k_batch_interleaved<4><<<grid, kBatchThreads, 0, st>>>(t); break;
-        case 8: k_batch_interleaved<8><<<grid, kBatchThreads, 0, st>>>(t); break;
-        case 16: k_batch_interleaved<16><<<grid, kBatchThreads, 0, st>>>(t); break;
-        default: return cudaErrorInvalidValue;
-    }
+    MLEM_BATCH_TILES(k_batch_interleaved, grid, kBatchThreads, 0, st>>>(t))
     return cudaGetLastError();
 }
 
 cudaError_t batch_fused(const BatchTable& t, const BatchItem* items, uint32_t n_items,
-                        unsigned int* counter, int frame_tile, int sm_count, int blocks_per_sm,
-                        cudaStream_t st) {
+                        unsigned int* counter, int frame_tile, bool sorted, int sm_count,
+                        int blocks_per_sm, cudaStream_t st) {
     if (n_items == 0) return cudaSuccess;
     if (t.n == 0 || t.n > kBatchTableMax) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
     if (e != cudaSuccess) return e;
     const int grid = std::max(1, std::min<int>((int)std::min<uint32_t>(n_items, 1u << 30),
                                                sm_count * blocks_per_sm));
-    switch (frame_tile) {
-        case 1: k_batch_fused<1><<<grid, kBatchThreads, 0, st>>>(t, items, n_items, counter); break;
-        case 2: k_batch_fused<2><<<grid, kBatchThreads, 0, st>>>(t, items, n_items, counter); break;
-        case 4: k_batch_fused<4><<<grid, kBatchThreads, 0, st>>>(t, items, n_items, counter); break;
-        case 8: k_batch_fused<8><<<grid, kBatchThreads, 0, st>>>(t, items, n_items, counter); break;
-        case 16: k_batch_fused<16><<<grid, kBatchThreads, 0, st>>>(t, items, n_items, counter); break;
-        default: return cudaErrorInvalidValue;
-    }
+    MLEM_BATCH_TILES(k_batch_fused, grid, kBatchThreads, 0, st>>>(t, items, n_items, counter))
     return cudaGetLastError();
 }
+#undef MLEM_BATCH_TILES
 
 }  // namespace mlem

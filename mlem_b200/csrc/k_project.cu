@@ -145,15 +145,16 @@ __global__ void __launch_bounds__(256) k_bkproj_scatter(SparseView csr,
 // matrix streams from HBM once per iteration.  The per-row work is in
 // fused_row_range (row_dev.cuh), shared with the multi-matrix kernel.
 // ---------------------------------------------------------------------------
-template <int G, int BT>
+template <int G, int BT, bool SORTED>
 __global__ void __launch_bounds__(256) k_fused_row(SparseView csr, const float* __restrict__ x,
                                                    uint32_t B, uint32_t f0,
                                                    const int32_t* __restrict__ sino,
                                                    float* __restrict__ u) {
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    fused_row_range<G, BT>(csr, x, B, f0, sino, u, 0, csr.n, warp, nwarps);
+    fused_row_range<G, BT, SORTED>(csr, x, B, f0, sino, u, 0, csr.n, warp, nwarps);
 }
+
 
 #undef MLEM_WARP_LOOP_SETUP
 
@@ -278,7 +279,20 @@ cudaError_t dispatch(const LaunchCfg& cfg, cudaStream_t st, Args... args);
 MLEM_KERNEL_FUNCTOR(FwprojK, k_fwproj)
 MLEM_KERNEL_FUNCTOR(BkprojCscK, k_bkproj_csc)
 MLEM_KERNEL_FUNCTOR(ScatterK, k_bkproj_scatter)
-MLEM_KERNEL_FUNCTOR(FusedK, k_fused_row)
+template <int G, int BT>
+struct FusedK {  // file order
+    template <typename... A>
+    static void run(int grid, cudaStream_t st, A... a) {
+        k_fused_row<G, BT, false><<<grid, 256, 0, st>>>(a...);
+    }
+};
+template <int G, int BT>
+struct FusedSortedK {  // sorted visiting order (csr.order + csr.vrange)
+    template <typename... A>
+    static void run(int grid, cudaStream_t st, A... a) {
+        k_fused_row<G, BT, true><<<grid, 256, 0, st>>>(a...);
+    }
+};
 #undef MLEM_KERNEL_FUNCTOR
 
 template <template <int, int> class K, int G, typename... Args>
@@ -343,6 +357,8 @@ cudaError_t fused_row(const SparseView& csr, const float* x, uint32_t B, uint32_
                       const int32_t* sino, float* u, const LaunchCfg& cfg, cudaStream_t st) {
     if (!cfg_valid(cfg) || (B % cfg.frame_tile) || (f0 % cfg.frame_tile)) return cudaErrorInvalidValue;
     if (csr.n == 0) return cudaSuccess;
+    if (csr.order && !csr.vrange) return cudaErrorInvalidValue;  // sorted visits carry vrange
+    if (csr.vrange) return dispatch<FusedSortedK>(cfg, st, csr, x, B, f0, sino, u);
     return dispatch<FusedK>(cfg, st, csr, x, B, f0, sino, u);
 }
 

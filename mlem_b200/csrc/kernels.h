@@ -254,9 +254,11 @@ static_assert(sizeof(BatchTable) <= 32764, "kernel parameter space (CUDA >= 12.1
 // Items schedule: every item does u[mat] += A^T correl(A x) over its rows,
 // all frames of its matrix in passes of frame_tile (1, 2, 4, 8 or 16;
 // divides every Bp).  `counter` (one uint) is reset on the stream first.
+// sorted: every matrix of the table is visited in its sorted order (their
+// views carry order and vrange); else every one in file order.
 cudaError_t batch_fused(const BatchTable& t, const BatchItem* items, uint32_t n_items,
-                        unsigned int* counter, int frame_tile, int sm_count, int blocks_per_sm,
-                        cudaStream_t st);
+                        unsigned int* counter, int frame_tile, bool sorted, int sm_count,
+                        int blocks_per_sm, cudaStream_t st);
 // One matrix in chunks (MLEM_VISIT_SORTED_CHUNKED): CTAs take chunks of
 // chunk_rows consecutive visiting positions from `counter` (reset here on the
 // stream), and do every frame tile of a chunk's rows back to back -- each CTA
@@ -269,7 +271,7 @@ cudaError_t fused_chunked(const SparseView& csr, const float* x, uint32_t B, int
                           unsigned int* counter, int sm_count, cudaStream_t st);
 // Interleaved schedule: the same work in grid-stride order over the virtual
 // row space.
-cudaError_t batch_interleaved(const BatchTable& t, int frame_tile, int sm_count,
+cudaError_t batch_interleaved(const BatchTable& t, int frame_tile, bool sorted, int sm_count,
                               int blocks_per_sm, cudaStream_t st);
 
 }  // namespace mlem

@@ -85,35 +85,6 @@ __device__ __forceinline__ void prefetch_l2(const void* p, uint64_t bytes) {
     asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(a0), "r"(n) : "memory");
 }
 
-// Element range [b, e) and row index r of visiting position v.
-__device__ __forceinline__ void visit_range(const SparseView& csr, uint64_t v, uint64_t& r,
-                                            uint64_t& b, uint64_t& e) {
-    if (csr.vrange) {
-        const ulonglong2 q = csr.vrange[v];
-        r = csr.order[v];
-        b = q.x;
-        e = q.y;
-    } else {
-        r = row_at(csr, v);
-        b = csr.ptr[r];
-        e = csr.ptr[r + 1];
-    }
-}
-
-// Element range [b, e) of visiting position v (no row index).
-__device__ __forceinline__ void visit_bounds(const SparseView& csr, uint64_t v, uint64_t& b,
-                                             uint64_t& e) {
-    if (csr.vrange) {
-        const ulonglong2 q = csr.vrange[v];
-        b = q.x;
-        e = q.y;
-    } else {
-        const uint64_t r = row_at(csr, v);
-        b = csr.ptr[r];
-        e = csr.ptr[r + 1];
-    }
-}
-
 // u[...] += w * c[...] for VW floats (one vector reduction, 4..16 bytes).
 template <int VW>
 __device__ __forceinline__ void red_vec(float* __restrict__ p, float w, const float (&c)[VW]) {
@@ -196,7 +167,11 @@ __device__ __forceinline__ void slot_allreduce(float (&acc)[Lanes<BT>::VW]) {
 // One pass per row over rows [r_begin, r_end): forward projection, calcCorrel
 // and the scatter of the row into the update vector.  `warp` / `nwarps`
 // number the warps that share the range (grid-wide or block-wide).
-template <int G, int BT>
+// SORTED: the view carries the sorted visiting order with its row ranges
+// (csr.vrange); otherwise rows are visited in file order (csr.order null).
+// A compile-time choice: the file-order loop measured 2.49 vs 3.15 ms on the
+// plain-full matrix when the sorted path was a runtime branch inside it.
+template <int G, int BT, bool SORTED>
 __device__ __forceinline__ void fused_row_range(const SparseView& csr, const float* __restrict__ x,
                                                 uint32_t B, uint32_t f0,
                                                 const int32_t* __restrict__ sino,
@@ -215,17 +190,28 @@ __device__ __forceinline__ void fused_row_range(const SparseView& csr, const flo
         const uint64_t v = base + lw / G;  // visiting position
         const bool active = v < r_end;
         uint64_t r = 0, b = 0, e = 0;
-        if (active) visit_range(csr, v, r, b, e);
-        // Sorted visits: the row this lane group takes next -- its range load
-        // goes out beside this row's, and its elements are prefetched into L2
-        // while this row is worked on.  (In file order the next row of a
-        // grid-stride walk is thousands of rows away and the prefetch only
-        // adds L2 requests: measured 2.49 -> 2.80 ms on the plain-full matrix.)
-        const uint64_t nv = v + nwarps * RPW;
-        if (csr.vrange && lane == 0 && nv < r_end) {
-            uint64_t nb, ne;
-            visit_bounds(csr, nv, nb, ne);
-            if (ne > nb) prefetch_l2(el + nb, (ne - nb) * 8);
+        if constexpr (SORTED) {
+            if (active) {
+                const ulonglong2 q = csr.vrange[v];
+                r = csr.order[v];
+                b = q.x;
+                e = q.y;
+            }
+            // the row this lane group takes next: its range load goes out beside
+            // this row's, and its elements are prefetched into L2 while this row
+            // is worked on (in file order the next row of a grid-stride walk is
+            // thousands of rows away and a prefetch only adds L2 requests)
+            const uint64_t nv = v + nwarps * RPW;
+            if (lane == 0 && nv < r_end) {
+                const ulonglong2 nq = csr.vrange[nv];
+                if (nq.y > nq.x) prefetch_l2(el + nq.x, (nq.y - nq.x) * 8);
+            }
+        } else {
+            r = v;
+            if (active) {
+                b = csr.ptr[r];
+                e = csr.ptr[r + 1];
+            }
         }
         float acc[VW];
         uint2 kept[kBatch];
