@@ -275,6 +275,13 @@ struct RLanes2 {
 };
 
 template <int VW>
+__device__ __forceinline__ void sts_vec(float* p, const float (&v)[VW]) {
+    if constexpr (VW == 4) *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
+    else if constexpr (VW == 2) *reinterpret_cast<float2*>(p) = make_float2(v[0], v[1]);
+    else *p = v[0];
+}
+
+template <int VW>
 __device__ __forceinline__ void lds_vec(const float* p, float (&v)[VW]) {
     if constexpr (VW == 4) {
         const float4 t = *reinterpret_cast<const float4*>(p);
@@ -384,6 +391,7 @@ __global__ void __launch_bounds__(kRbThreads, 2) k_rb_bkproj(RegionView rv, cons
         for (uint64_t t0 = E0 + (uint64_t)warp * TILE; t0 < E1; t0 += (uint64_t)nwarps * TILE) {
             const uint2* __restrict__ sp = rv.el_bk + t0 + grp;
             uint32_t cur = 0xffffffffu;
+            bool first = true;  // the current run is the span's first
             float acc[VW];
 #pragma unroll
             for (int i = 0; i < VW; ++i) acc[i] = 0.0f;
@@ -397,8 +405,23 @@ __global__ void __launch_bounds__(kRbThreads, 2) k_rb_bkproj(RegionView rv, cons
                     const uint32_t vox = q[j].x & mask;
                     if (vox != cur) {
                         if (cur != 0xffffffffu) {
+                            // A run that started after the span's first element and
+                            // ended before its last is in no other span: this lane
+                            // group owns the voxel, a plain read-modify-write does.
+                            // The first (and last) run may be shared with the
+                            // neighbouring span: atomics.
+                            float* dst = ut + cur * BT + sub * VW;
+                            if (first) {
 #pragma unroll
-                            for (int i = 0; i < VW; ++i) atomicAdd(ut + cur * BT + sub * VW + i, acc[i]);
+                                for (int i = 0; i < VW; ++i) atomicAdd(dst + i, acc[i]);
+                            } else {
+                                float t[VW];
+                                lds_vec<VW>(dst, t);
+#pragma unroll
+                                for (int i = 0; i < VW; ++i) t[i] += acc[i];
+                                sts_vec<VW>(dst, t);
+                            }
+                            first = false;
                         }
                         cur = vox;
 #pragma unroll
