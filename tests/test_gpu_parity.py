@@ -174,7 +174,7 @@ def test_device_generator_matches_host_generator():
         assert np.array_equal(ctx.project_f64(x), synth.project_f64(hm, x))
 
 
-def test_skewed_matrix_long_rows_and_columns():
+def test_skewed_matrix_long_rows_and_columns(golden):
     """A 12k-element row and columns longer than the shared-memory sort."""
     rng = np.random.default_rng(7)
     R, C = 3000, 512
@@ -194,13 +194,37 @@ def test_skewed_matrix_long_rows_and_columns():
         cp_o, ce_o = ob.transpose(m)
         assert np.array_equal(cp, cp_o) and ce.tobytes() == ce_o.tobytes()
         assert ctx.column_sums().tobytes() == ob.column_sums(m).tobytes()
+        want, _ = ob.mlem(m, sino, 5)
         for mode in MODES:
             ctx.set_sinograms(sino)
             ctx.set_tuning(bk_mode=mode, group=32, frame_tile=1, blocks_per_sm=8)
             ctx.init_images()
             ctx.iterate(5)
-            want, _ = ob.mlem(m, sino, 5)
             assert ob.rel_l2(ctx.get_images()[0], want) <= TOL_MLEM
+        # sorted visits: the long rows exceed the 64 KiB next-row prefetch and a chunk
+        for visit, bps in ((api.VISIT_SORTED, 8), (api.VISIT_SORTED_CHUNKED, 4),
+                           (api.VISIT_SORTED_CHUNKED, 1)):
+            ctx.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=1, blocks_per_sm=bps,
+                           visit=visit)
+            ctx.init_images()
+            ctx.iterate(5)
+            assert ob.rel_l2(ctx.get_images()[0], want) <= TOL_MLEM
+        # a batch with a regular matrix: items cut around the long rows
+        small_m, small_sino, _, _, _ = golden.case("tiny_it10")
+        with api.Context.from_matrix(small_m) as other:
+            other.set_sinograms(small_sino)
+            other.init_images()
+            ctx.init_images()
+            for policy, visit in ((api.BATCH_ITEMS, api.VISIT_SORTED),
+                                  (api.BATCH_INTERLEAVED, api.VISIT_FILE)):
+                with api.Batch([ctx, other]) as b:
+                    b.set_schedule(policy, 64, 4, 1, visit)
+                    ctx.init_images()
+                    other.init_images()
+                    b.iterate(5)
+                assert ob.rel_l2(ctx.get_images()[0], want) <= TOL_MLEM
+                want_o, _ = ob.mlem(small_m, small_sino, 5)
+                assert ob.rel_l2(other.get_images()[0], want_o) <= TOL_MLEM
 
 
 def test_invalid_inputs_raise():
