@@ -274,8 +274,9 @@ def run_ours(a, rank, world, local_rank):
     kernel_names = {
         api.BK_CSC: ("k_fwproj", "k_bkproj_csc", "-", "k_stats"),
         api.BK_ATOMIC: ("k_fwproj", "k_bkproj_scatter", "k_apply_update", "k_stats"),
-        api.BK_FUSED: ("k_fused_chunked" if tuning["visit"] == api.VISIT_SORTED_CHUNKED
-                       else "k_fused_row", "-", "k_apply_update", "k_stats"),
+        api.BK_FUSED: ({api.VISIT_SORTED_CHUNKED: "k_fused_chunked",
+                        api.VISIT_SORTED_STAGED: "k_fused_staged"}.get(tuning["visit"], "k_fused_row"),
+                       "-", "k_apply_update", "k_stats"),
         api.BK_REGION: ("k_rb_fwproj", "k_rb_bkproj", "-", "k_stats"),  # bkproj applies the update
     }[tuning["bk_mode"]]
     traffic = committed_traffic().get(kernel_names[dom])

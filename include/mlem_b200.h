@@ -89,8 +89,9 @@ typedef struct {
     int group;          /* lanes per row/column: 4, 8, 16 or 32 */
     int frame_tile;     /* frames per pass over the matrix: 1, 2, 4, 8 or 16 */
     int blocks_per_sm;  /* 1..8 blocks of 256 threads per SM (chunked visit: 1, 2 or 4 CTAs
-                           of 1024, 512 or 256 threads) */
-    int visit;          /* row visiting order: MLEM_VISIT_FILE, _SORTED or _SORTED_CHUNKED */
+                           of 1024, 512 or 256 threads; staged visit: 1..4 CTAs of 256) */
+    int visit;          /* row visiting order: MLEM_VISIT_FILE, _SORTED, _SORTED_CHUNKED or
+                           _SORTED_STAGED */
     double ms_per_iter; /* measured by mlem_autotune; 0 when set by hand */
 } mlem_tuning;
 
@@ -101,6 +102,9 @@ typedef struct {
 #define MLEM_VISIT_SORTED 1         /* rows sorted by entry/exit voxel, grid stride */
 #define MLEM_VISIT_SORTED_CHUNKED 2 /* sorted; CTAs take chunks of neighbouring rows from a counter
                                        (one-pass method, group 32) */
+#define MLEM_VISIT_SORTED_STAGED 3  /* as chunked, each warp's rows pipelined: elements staged in
+                                       shared memory by asynchronous copies rows ahead (one-pass
+                                       method, group 32) */
 
 /* ---- errors ------------------------------------------------------------- */
 const char* mlem_last_error(const mlem_ctx* ctx);

@@ -42,8 +42,9 @@ FLAG_NO_ROW_ORDER = 0x10
 
 BK_AUTO, BK_CSC, BK_ATOMIC, BK_FUSED, BK_REGION = 0, 1, 2, 3, 4
 BATCH_INTERLEAVED, BATCH_ITEMS = 0, 1
-VISIT_FILE, VISIT_SORTED, VISIT_SORTED_CHUNKED = 0, 1, 2
-VISIT_NAMES = {VISIT_FILE: "file", VISIT_SORTED: "sorted", VISIT_SORTED_CHUNKED: "sorted-chunked"}
+VISIT_FILE, VISIT_SORTED, VISIT_SORTED_CHUNKED, VISIT_SORTED_STAGED = 0, 1, 2, 3
+VISIT_NAMES = {VISIT_FILE: "file", VISIT_SORTED: "sorted", VISIT_SORTED_CHUNKED: "sorted-chunked",
+               VISIT_SORTED_STAGED: "sorted-staged"}
 BATCH_NAMES = {BATCH_INTERLEAVED: "interleaved", BATCH_ITEMS: "items"}
 BK_NAMES = {BK_CSC: "csc", BK_ATOMIC: "atomic", BK_FUSED: "fused", BK_REGION: "region"}
 
@@ -307,7 +308,8 @@ class Context:
 
     def set_tuning(self, bk_mode=BK_CSC, group=32, frame_tile=1, blocks_per_sm=8,
                    visit=0) -> None:
-        """visit: VISIT_FILE, VISIT_SORTED or VISIT_SORTED_CHUNKED (one-pass method)."""
+        """visit: VISIT_FILE, VISIT_SORTED, or VISIT_SORTED_CHUNKED / VISIT_SORTED_STAGED
+        (one-pass method, group 32)."""
         t = sig.MlemTuning(bk_mode, group, frame_tile, blocks_per_sm, visit, 0.0)
         self._chk(core_lib().mlem_set_tuning(self._h, ctypes.byref(t)))
 

@@ -529,8 +529,15 @@ SparseView csr_visit(const mlem_ctx* c, const mlem_tuning& t) {
 int chunk_ctas_per_sm(const mlem_tuning& t) {
     return t.blocks_per_sm <= 1 ? 1 : t.blocks_per_sm == 2 ? 2 : 4;
 }
+// MLEM_VISIT_SORTED_STAGED: 1..4 resident CTAs of 256 threads per SM.
+int staged_ctas_per_sm(const mlem_tuning& t) { return std::min(4, std::max(1, t.blocks_per_sm)); }
+bool chunk_visit(int visit) {
+    return visit == MLEM_VISIT_SORTED_CHUNKED || visit == MLEM_VISIT_SORTED_STAGED;
+}
 uint32_t chunk_rows_of(const mlem_ctx* c, const mlem_tuning& t) {
-    const uint64_t ctas = (uint64_t)c->n_sm * chunk_ctas_per_sm(t);
+    const uint64_t ctas = (uint64_t)c->n_sm * (t.visit == MLEM_VISIT_SORTED_STAGED
+                                                   ? staged_ctas_per_sm(t)
+                                                   : chunk_ctas_per_sm(t));
     return (uint32_t)std::max<uint64_t>(32, (c->R + ctas * 16 - 1) / (ctas * 16));
 }
 
@@ -568,7 +575,11 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                 CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
                 break;
             case MLEM_BK_FUSED:
-                if (t.visit == MLEM_VISIT_SORTED_CHUNKED)
+                if (t.visit == MLEM_VISIT_SORTED_STAGED)
+                    CK(c, fused_staged(csr, c->x, Bp, t.frame_tile, c->sino, c->update,
+                                       chunk_rows_of(c, t), staged_ctas_per_sm(t), c->counter,
+                                       c->n_sm, st));
+                else if (t.visit == MLEM_VISIT_SORTED_CHUNKED)
                     CK(c, fused_chunked(csr, c->x, Bp, t.frame_tile, c->sino, c->update,
                                         chunk_rows_of(c, t), chunk_ctas_per_sm(t), c->counter,
                                         c->n_sm, st));
@@ -633,7 +644,7 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
     }
     if (mode == MLEM_BK_FUSED) {
         bytes[0] = tiles * csr_pass + B * (4.0 * C + 4.0 * R + 4.0 * C);  // x, sino, update
-        launches[0] = (!exact && c->tuning.visit == MLEM_VISIT_SORTED_CHUNKED) ? 1 : nt;
+        launches[0] = (!exact && chunk_visit(c->tuning.visit)) ? 1 : nt;
     } else {
         bytes[0] = tiles * csr_pass + B * (4.0 * C + 4.0 * R + 4.0 * R);  // x, sino, correl
         launches[0] = exact ? 1 : nt;
@@ -897,7 +908,7 @@ int mlem_kernels_per_iteration(const mlem_ctx* c, int* n) {
     else if (c->tuning.bk_mode == MLEM_BK_CSC) k += 2 * tiles;
     else if (c->tuning.bk_mode == MLEM_BK_ATOMIC) k += 2 * tiles + 1;
     else if (c->tuning.bk_mode == MLEM_BK_REGION) k += 2 * tiles + 1;  // + correl
-    else if (c->tuning.visit == MLEM_VISIT_SORTED_CHUNKED) k += 2;  // all tiles in one launch
+    else if (chunk_visit(c->tuning.visit)) k += 2;  // all tiles in one launch
     else k += tiles + 1;
     *n = k;
     return MLEM_OK;
@@ -1201,13 +1212,13 @@ int mlem_set_tuning(mlem_ctx* c, const mlem_tuning* t) {
     if (c->Bp && (c->Bp % (uint32_t)n.frame_tile))
         return fail(c, MLEM_ERR_INVALID, "frame tile %d does not divide the padded frame count %u",
                     n.frame_tile, c->Bp);
-    if (n.visit < MLEM_VISIT_FILE || n.visit > MLEM_VISIT_SORTED_CHUNKED)
+    if (n.visit < MLEM_VISIT_FILE || n.visit > MLEM_VISIT_SORTED_STAGED)
         return fail(c, MLEM_ERR_INVALID, "unknown row visiting order %d", n.visit);
     if (n.visit != MLEM_VISIT_FILE && !c->row_order)
         return fail(c, MLEM_ERR_INVALID,
                     "sorted row visiting needs the row order (context made with MLEM_FLAG_NO_ROW_ORDER)");
-    if (n.visit == MLEM_VISIT_SORTED_CHUNKED && n.group != 32)
-        return fail(c, MLEM_ERR_INVALID, "the chunked row visit runs 32 lanes per row (group 32)");
+    if (chunk_visit(n.visit) && n.group != 32)
+        return fail(c, MLEM_ERR_INVALID, "the chunked row visits run 32 lanes per row (group 32)");
     if (n.bk_mode == MLEM_BK_REGION) {
         TRY(set_device(c));
         TRY(ensure_region(c, n.frame_tile));
@@ -1252,17 +1263,21 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
                     if (ensure_region(c, tile) != MLEM_OK) continue;  // e.g. no memory: skip
                 }
                 for (int bps : {4, 8})
-                for (int visit : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED, MLEM_VISIT_SORTED_CHUNKED}) {
+                for (int visit : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED, MLEM_VISIT_SORTED_CHUNKED,
+                                  MLEM_VISIT_SORTED_STAGED}) {
                     if (mode == MLEM_BK_REGION && bps == 4) continue;  // grid is fixed by the tile
                     // the sorted orders need the row order; the region method has its
                     // own layout; only the one-pass method walks chunks
                     if (visit != MLEM_VISIT_FILE && (!c->row_order || mode == MLEM_BK_REGION))
                         continue;
-                    if (visit == MLEM_VISIT_SORTED_CHUNKED && mode != MLEM_BK_FUSED) continue;
-                    // chunked: warp-wide rows; CTAs per SM 4 (bps 4) or 1 (bps 8 -> 1 below)
-                    if (visit == MLEM_VISIT_SORTED_CHUNKED && group != 32) continue;
-                    mlem_tuning t{mode, group, tile,
-                                  visit == MLEM_VISIT_SORTED_CHUNKED && bps == 8 ? 1 : bps, visit, 0.0};
+                    if (chunk_visit(visit) && mode != MLEM_BK_FUSED) continue;
+                    // chunked: warp-wide rows; CTAs per SM 4 (bps 4) or 1 (bps 8 -> 1 below);
+                    // staged: 4 or 3 CTAs of 256 threads
+                    if (chunk_visit(visit) && group != 32) continue;
+                    const int ctas = visit == MLEM_VISIT_SORTED_CHUNKED ? (bps == 8 ? 1 : bps)
+                                     : visit == MLEM_VISIT_SORTED_STAGED ? (bps == 8 ? 3 : bps)
+                                                                         : bps;
+                    mlem_tuning t{mode, group, tile, ctas, visit, 0.0};
                     // warm-up once, then time two iterations
                     int s = enqueue_iteration(c, t, false);
                     if (s != MLEM_OK) { c->tuning = orig; return s; }

@@ -269,6 +269,12 @@ cudaError_t batch_fused(const BatchTable& t, const BatchItem* items, uint32_t n_
 cudaError_t fused_chunked(const SparseView& csr, const float* x, uint32_t B, int frame_tile,
                           const int32_t* sino, float* u, uint32_t chunk_rows, int ctas_per_sm,
                           unsigned int* counter, int sm_count, cudaStream_t st);
+// The same chunked walk with each warp's rows pipelined: the next row's
+// elements staged in shared memory by cp.async, ranges and counts loaded
+// ahead (k_staged.cu).  ctas_per_sm: 1..4 CTAs of 256 threads.
+cudaError_t fused_staged(const SparseView& csr, const float* x, uint32_t B, int frame_tile,
+                         const int32_t* sino, float* u, uint32_t chunk_rows, int ctas_per_sm,
+                         unsigned int* counter, int sm_count, cudaStream_t st);
 // Interleaved schedule: the same work in grid-stride order over the virtual
 // row space.
 cudaError_t batch_interleaved(const BatchTable& t, int frame_tile, bool sorted, int sm_count,

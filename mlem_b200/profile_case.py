@@ -27,8 +27,9 @@ def main(argv=None):
     ap.add_argument("--frames", type=int, default=1)
     ap.add_argument("--iters", type=int, default=3)
     ap.add_argument("--natural", action="store_true", help="keep the natural voxel order")
-    ap.add_argument("--visit", choices=["file", "sorted", "chunked"], default="file",
-                    help="row visiting order (chunked: sorted, CTAs take chunks of rows)")
+    ap.add_argument("--visit", choices=["file", "sorted", "chunked", "staged"], default="file",
+                    help="row visiting order (chunked: sorted, CTAs take chunks of rows; "
+                         "staged: chunked with each warp's rows pipelined through shared memory)")
     a = ap.parse_args(argv)
     nx, ny, nz = a.grid
     g = synth.Geometry(nx, ny, nz, a.rows, a.count[0], a.count[1], seed=a.seed)
@@ -43,7 +44,7 @@ def main(argv=None):
             mode = {"csc": api.BK_CSC, "atomic": api.BK_ATOMIC, "fused": api.BK_FUSED,
                     "region": api.BK_REGION}[a.mode]
             visit = {"file": api.VISIT_FILE, "sorted": api.VISIT_SORTED,
-                     "chunked": api.VISIT_SORTED_CHUNKED}[a.visit]
+                     "chunked": api.VISIT_SORTED_CHUNKED, "staged": api.VISIT_SORTED_STAGED}[a.visit]
             ctx.set_tuning(bk_mode=mode, group=a.group, frame_tile=a.frame_tile,
                            blocks_per_sm=a.blocks_per_sm, visit=visit)
         ctx.init_images()

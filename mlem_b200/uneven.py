@@ -59,8 +59,9 @@ def _best_solo(ctx, stream, api):
             continue
         for group in (16, 32):
             for bps in (4, 8):
-                for visit in (api.VISIT_FILE, api.VISIT_SORTED, api.VISIT_SORTED_CHUNKED):
-                    if visit == api.VISIT_SORTED_CHUNKED and group != 32:
+                for visit in (api.VISIT_FILE, api.VISIT_SORTED, api.VISIT_SORTED_CHUNKED,
+                              api.VISIT_SORTED_STAGED):
+                    if visit in (api.VISIT_SORTED_CHUNKED, api.VISIT_SORTED_STAGED) and group != 32:
                         continue
                     ctx.set_tuning(bk_mode=api.BK_FUSED, group=group, frame_tile=tile,
                                    blocks_per_sm=bps, visit=visit)

@@ -77,7 +77,8 @@ MODES = [api.BK_CSC, api.BK_ATOMIC, api.BK_FUSED, api.BK_REGION]
 @pytest.mark.parametrize("name", CASES)
 @pytest.mark.parametrize("mode,visit", [(m, api.VISIT_FILE) for m in MODES] + [
     (api.BK_CSC, api.VISIT_SORTED), (api.BK_ATOMIC, api.VISIT_SORTED),
-    (api.BK_FUSED, api.VISIT_SORTED), (api.BK_FUSED, api.VISIT_SORTED_CHUNKED)])
+    (api.BK_FUSED, api.VISIT_SORTED), (api.BK_FUSED, api.VISIT_SORTED_CHUNKED),
+    (api.BK_FUSED, api.VISIT_SORTED_STAGED)])
 def test_mlem_matches_reference_image(ctxs, name, mode, visit):
     ctx, m, sino, iters, gold = ctxs[name]
     ctx.set_sinograms(sino)
@@ -201,9 +202,11 @@ def test_skewed_matrix_long_rows_and_columns(golden):
             ctx.init_images()
             ctx.iterate(5)
             assert ob.rel_l2(ctx.get_images()[0], want) <= TOL_MLEM
-        # sorted visits: the long rows exceed the 64 KiB next-row prefetch and a chunk
+        # sorted visits: the long rows exceed the 64 KiB next-row prefetch, a chunk and a
+        # shared-memory stage
         for visit, bps in ((api.VISIT_SORTED, 8), (api.VISIT_SORTED_CHUNKED, 4),
-                           (api.VISIT_SORTED_CHUNKED, 1)):
+                           (api.VISIT_SORTED_CHUNKED, 1), (api.VISIT_SORTED_STAGED, 4),
+                           (api.VISIT_SORTED_STAGED, 1)):
             ctx.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=1, blocks_per_sm=bps,
                            visit=visit)
             ctx.init_images()
@@ -246,7 +249,7 @@ def test_invalid_inputs_raise():
         with pytest.raises(api.MlemError):
             ctx.set_tuning(bk_mode=api.BK_CSC, group=32, frame_tile=3)
         with pytest.raises(api.MlemError):
-            ctx.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=1, visit=3)
+            ctx.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=1, visit=4)
     with api.Context(re_, el, 2, 2, flags=api.FLAG_NO_ROW_ORDER) as ctx:
         with pytest.raises(api.MlemError):  # no row order to visit in
             ctx.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=1, visit=api.VISIT_SORTED)
@@ -292,14 +295,17 @@ def test_row_order_changes_only_rounding(golden, frames):
     m, sino, iters, gold, _ = golden.case("plain_small_it10")
     sinos = np.stack([np.roll(sino, 7 * b) for b in range(frames)]).astype(np.int32)
     want = [ob.mlem(m, sinos[b], iters)[0] for b in range(frames)]
-    runs = [(api.BK_ATOMIC, api.VISIT_FILE), (api.BK_ATOMIC, api.VISIT_SORTED),
-            (api.BK_FUSED, api.VISIT_FILE), (api.BK_FUSED, api.VISIT_SORTED),
-            (api.BK_FUSED, api.VISIT_SORTED_CHUNKED)]
+    tile = min(frames, 8)
+    runs = [(api.BK_ATOMIC, api.VISIT_FILE, tile), (api.BK_ATOMIC, api.VISIT_SORTED, tile),
+            (api.BK_FUSED, api.VISIT_FILE, tile), (api.BK_FUSED, api.VISIT_SORTED, tile),
+            (api.BK_FUSED, api.VISIT_SORTED_CHUNKED, tile),
+            (api.BK_FUSED, api.VISIT_SORTED_STAGED, tile),
+            (api.BK_FUSED, api.VISIT_SORTED_STAGED, frames)]
     imgs = []
     with api.Context.from_matrix(m) as ctx:
         ctx.set_sinograms(sinos)
-        for mode, visit in runs:
-            ctx.set_tuning(bk_mode=mode, group=32, frame_tile=min(frames, 8), blocks_per_sm=8,
+        for mode, visit, ft in runs:
+            ctx.set_tuning(bk_mode=mode, group=32, frame_tile=ft, blocks_per_sm=8,
                            visit=visit)
             ctx.init_images()
             ctx.iterate(iters)
