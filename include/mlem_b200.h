@@ -301,10 +301,20 @@ const char* mlem_batch_last_error(const mlem_batch* b);
  * items schedule): about that many items for every resident block
  * (blocks_per_sm x SMs); frame_tile in {1,2,4,8,16} dividing every context's
  * padded frame count (0 keeps the current tile); visit: MLEM_VISIT_FILE or
- * MLEM_VISIT_SORTED for every matrix (sorted needs every context's row
- * order; with the items schedule a sorted item is a run of neighbouring rows). */
+ * MLEM_VISIT_SORTED for every matrix, or MLEM_VISIT_SORTED_STAGED with the
+ * items schedule (sorted needs every context's row order; with the items
+ * schedule a sorted item is a run of neighbouring rows; staged pipelines each
+ * warp's rows of an item through shared memory, at most 4 blocks per SM). */
 int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
                             int blocks_per_sm, int frame_tile, int visit);
+/* A frame tile for each context (n_ctx entries): 0 follows the batch's tile,
+ * else 1, 2, 4, 8 or 16 dividing that context's padded frame count.  The
+ * contexts that share a tile share one kernel per iteration (heaviest group
+ * first).  mlem_batch_set_schedule with a non-zero frame_tile sets every
+ * context back to the batch's tile. */
+int mlem_batch_set_tiles(mlem_batch* b, const int* tiles);
+/* The frame tile each context runs with (n_ctx entries). */
+int mlem_batch_get_tiles(const mlem_batch* b, int* tiles);
 /* Current schedule; any pointer may be NULL.  n_items: 0 for the interleaved
  * schedule.  ms_per_iter: from the last autotune, else 0. */
 int mlem_batch_get_schedule(const mlem_batch* b, int* policy, uint32_t* items_per_block,

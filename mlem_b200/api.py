@@ -388,6 +388,21 @@ class Batch:
         self._chk(core_lib().mlem_batch_set_schedule(self._h, policy, items_per_block,
                                                      blocks_per_sm, frame_tile, visit))
 
+    def set_tiles(self, tiles) -> None:
+        """A frame tile per context (0: the batch's tile); contexts sharing a
+        tile share one kernel per iteration."""
+        tiles = [int(t) for t in tiles]
+        if len(tiles) != len(self.contexts):
+            raise MlemError(MLEM_ERR_INVALID, "one frame tile per context")
+        arr = (ctypes.c_int * len(tiles))(*tiles)
+        self._chk(core_lib().mlem_batch_set_tiles(self._h, arr))
+
+    def tiles(self) -> list:
+        """The frame tile each context runs with."""
+        arr = (ctypes.c_int * len(self.contexts))()
+        self._chk(core_lib().mlem_batch_get_tiles(self._h, arr))
+        return list(arr)
+
     def schedule(self) -> dict:
         pol, ipb, bps = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_int()
         tile, visit, n, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_uint32(), ctypes.c_double()
@@ -397,7 +412,7 @@ class Batch:
                                                      ctypes.byref(ms)))
         return dict(policy=pol.value, items_per_block=ipb.value, blocks_per_sm=bps.value,
                     frame_tile=tile.value, visit=visit.value, n_items=n.value,
-                    ms_per_iter=ms.value)
+                    ms_per_iter=ms.value, tiles=self.tiles())
 
     def autotune(self) -> dict:
         ms = ctypes.c_double()

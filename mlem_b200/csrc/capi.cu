@@ -1445,16 +1445,29 @@ struct mlem_batch {
     std::vector<std::vector<uint64_t>> pre_file, pre_sorted;
     int policy = MLEM_BATCH_INTERLEAVED;
     int visit = MLEM_VISIT_FILE;
-    int tile = 0;  // frames per pass, shared by the batch
+    int tile = 0;  // frames per pass of every context without a tile of its own
+    std::vector<int> tiles;  // per context: 0 = the batch tile, else its own frame tile
     uint32_t items_per_block = 4;
     int blocks_per_sm = 4;  // k_batch_fused is bounded to 64 registers: 4 x 256 threads per SM
     double ms_per_iter = 0.0;
 
+    // The contexts that share a frame tile form a group: one kernel per group
+    // and iteration, heaviest group first.  A group's table is the kernels'
+    // parameter; its items are b->items[item0, item0 + n_items), with `mat`
+    // indexing the group's table; ctx_of maps the table back to contexts.
+    struct Group {
+        int tile = 1;
+        double cost = 0.0;
+        BatchTable table{};
+        std::vector<size_t> ctx_of;
+        uint32_t item0 = 0, n_items = 0;
+    };
+    std::vector<Group> groups;
+    BatchTable table{};  // every context in order; the groups' tables are cut from it
     std::vector<BatchItem> items;
-    BatchTable table{};  // the kernels' parameter
     BatchItem* items_d = nullptr;
     size_t items_cap = 0;
-    unsigned int* counter = nullptr;
+    unsigned int* counter = nullptr;  // one counter per group, kCounterStride apart
     bool scheduled = false;
 
     cudaGraphExec_t graph = nullptr;
@@ -1502,12 +1515,25 @@ bool tile_ok_all(const mlem_batch* b, int t) {
     return true;
 }
 
+// The batch tile must divide the padded frame count of every context that
+// has no tile of its own.
+bool batch_tile_ok(const mlem_batch* b, int t) {
+    for (size_t i = 0; i < b->ctx.size(); ++i)
+        if (!b->tiles[i] && !tile_ok(t, b->ctx[i]->Bp)) return false;
+    return true;
+}
+
 // Widest tile (<= 16) dividing every padded frame count.
 int batch_default_tile(const mlem_batch* b) {
     for (int t : {16, 8, 4, 2})
         if (tile_ok_all(b, t)) return t;
     return 1;
 }
+
+int eff_tile(const mlem_batch* b, size_t i) { return b->tiles[i] ? b->tiles[i] : b->tile; }
+
+// Per-group counters sit a cache sector apart (the counter buffer holds 64 uints).
+constexpr uint32_t kCounterStride = 8;
 
 // Cost of rows [r0, r1) of context i: element bytes once per frame-tile
 // pass, one gather and one scatter of 4 bytes per element and frame, and the
@@ -1517,60 +1543,100 @@ double item_cost(const mlem_batch* b, size_t i, uint32_t r0, uint32_t r1) {
     const std::vector<uint64_t>& pre =
         (b->visit != MLEM_VISIT_FILE && !b->pre_sorted[i].empty()) ? b->pre_sorted[i] : b->pre_file[i];
     const double nnz = (double)(pre[r1] - pre[r0]);
-    const double passes = (double)(c->Bp / (uint32_t)b->tile);
+    const double passes = (double)(c->Bp / (uint32_t)eff_tile(b, i));
     return nnz * (8.0 * passes + 8.0 * c->Bp) + (double)(r1 - r0) * (16.0 + 8.0 * c->Bp);
 }
 
-// Cut the rows of every matrix into items of about total / (resident blocks x
-// items_per_block) cost; full items of the costliest matrix first in row
-// order (neighbouring rows share image voxels in L2), then the ragged
-// remainders, heaviest first.
+// Group the contexts by frame tile (heaviest group first) with each group's
+// table taken from b->table.  Returns true when the grouping differs from
+// the current one (the items must then be cut again); the item ranges of an
+// unchanged grouping are kept.
+bool build_groups(mlem_batch* b) {
+    std::vector<mlem_batch::Group> gs;
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+        const int t = eff_tile(b, i);
+        auto it = std::find_if(gs.begin(), gs.end(), [&](const mlem_batch::Group& g) { return g.tile == t; });
+        if (it == gs.end()) {
+            gs.emplace_back();
+            gs.back().tile = t;
+            gs.back().table.n = 0;
+            gs.back().table.row_base[0] = 0;
+            it = gs.end() - 1;
+        }
+        BatchTable& t_ = it->table;
+        t_.mats[t_.n] = b->table.mats[i];
+        t_.row_base[t_.n + 1] = t_.row_base[t_.n] + b->ctx[i]->R;
+        ++t_.n;
+        it->ctx_of.push_back(i);
+        it->cost += item_cost(b, i, 0, b->ctx[i]->R);
+    }
+    std::stable_sort(gs.begin(), gs.end(), [](const mlem_batch::Group& a, const mlem_batch::Group& c) {
+        return a.cost > c.cost;
+    });
+    bool same = gs.size() == b->groups.size();
+    for (size_t g = 0; same && g < gs.size(); ++g)
+        same = gs[g].tile == b->groups[g].tile && gs[g].ctx_of == b->groups[g].ctx_of;
+    if (same)
+        for (size_t g = 0; g < gs.size(); ++g) {
+            gs[g].item0 = b->groups[g].item0;
+            gs[g].n_items = b->groups[g].n_items;
+        }
+    b->groups = std::move(gs);
+    return !same;
+}
+
+// Cut the rows of every group's matrices into items of about group total /
+// (resident blocks x items_per_block) cost; within a group, full items of
+// the costliest matrix first in row order (neighbouring rows share image
+// voxels in L2), then the ragged remainders, heaviest first.
 int batch_schedule(mlem_batch* b) {
-    const size_t n = b->ctx.size();
+    b->items.clear();
     if (b->policy != MLEM_BATCH_ITEMS) {  // the interleaved schedule needs no items
-        b->items.clear();
+        for (auto& g : b->groups) g.item0 = g.n_items = 0;
         b->scheduled = true;
         b->graph_dirty = true;
         return MLEM_OK;
     }
-    std::vector<double> total(n, 0.0);
-    double all = 0.0;
-    for (size_t i = 0; i < n; ++i) {
-        total[i] = item_cost(b, i, 0, b->ctx[i]->R);
-        all += total[i];
-    }
     const double resident = (double)b->n_sm * (double)b->blocks_per_sm;
-    const double target = std::max(all / (resident * (double)b->items_per_block), 1.0);
-    std::vector<size_t> order(n);
-    for (size_t i = 0; i < n; ++i) order[i] = i;
-    std::stable_sort(order.begin(), order.end(),
-                     [&](size_t a, size_t c) { return total[a] > total[c]; });
-    std::vector<BatchItem> full;
-    std::vector<std::pair<double, BatchItem>> tail;
-    for (size_t i : order) {
-        const uint32_t R = b->ctx[i]->R;
-        uint32_t r0 = 0;
-        while (r0 < R) {
-            uint32_t lo = r0 + 1, hi = R;  // smallest r1 whose cost reaches the target
-            while (lo < hi) {
-                const uint32_t mid = lo + (hi - lo) / 2;
-                if (item_cost(b, i, r0, mid) >= target) hi = mid;
-                else lo = mid + 1;
+    for (auto& g : b->groups) {
+        const size_t n = g.ctx_of.size();
+        std::vector<double> total(n, 0.0);
+        for (size_t j = 0; j < n; ++j) total[j] = item_cost(b, g.ctx_of[j], 0, b->ctx[g.ctx_of[j]]->R);
+        const double target = std::max(g.cost / (resident * (double)b->items_per_block), 1.0);
+        std::vector<size_t> order(n);
+        for (size_t j = 0; j < n; ++j) order[j] = j;
+        std::stable_sort(order.begin(), order.end(),
+                         [&](size_t a, size_t c) { return total[a] > total[c]; });
+        std::vector<BatchItem> full;
+        std::vector<std::pair<double, BatchItem>> tail;
+        for (size_t j : order) {
+            const size_t i = g.ctx_of[j];
+            const uint32_t R = b->ctx[i]->R;
+            uint32_t r0 = 0;
+            while (r0 < R) {
+                uint32_t lo = r0 + 1, hi = R;  // smallest r1 whose cost reaches the target
+                while (lo < hi) {
+                    const uint32_t mid = lo + (hi - lo) / 2;
+                    if (item_cost(b, i, r0, mid) >= target) hi = mid;
+                    else lo = mid + 1;
+                }
+                const BatchItem it{(uint32_t)j, r0, lo, 0u};
+                const double cost = item_cost(b, i, r0, lo);
+                if (cost >= 0.5 * target) full.push_back(it);
+                else tail.emplace_back(cost, it);
+                r0 = lo;
             }
-            const BatchItem it{(uint32_t)i, r0, lo, 0u};
-            const double cost = item_cost(b, i, r0, lo);
-            if (cost >= 0.5 * target) full.push_back(it);
-            else tail.emplace_back(cost, it);
-            r0 = lo;
         }
+        std::stable_sort(tail.begin(), tail.end(),
+                         [](const std::pair<double, BatchItem>& a,
+                            const std::pair<double, BatchItem>& c) { return a.first > c.first; });
+        if (b->items.size() + full.size() + tail.size() > 0xffffffffull)
+            return bfail(b, MLEM_ERR_INVALID, "too many work items");
+        g.item0 = (uint32_t)b->items.size();
+        b->items.insert(b->items.end(), full.begin(), full.end());
+        for (auto& t : tail) b->items.push_back(t.second);
+        g.n_items = (uint32_t)b->items.size() - g.item0;
     }
-    std::stable_sort(tail.begin(), tail.end(),
-                     [](const std::pair<double, BatchItem>& a,
-                        const std::pair<double, BatchItem>& c) { return a.first > c.first; });
-    b->items = std::move(full);
-    for (auto& t : tail) b->items.push_back(t.second);
-    if (b->items.size() > 0xffffffffull)
-        return bfail(b, MLEM_ERR_INVALID, "too many work items (%zu)", b->items.size());
     if (b->items.size() > b->items_cap) {
         dev_free(b->items_d);
         b->items_d = nullptr;
@@ -1617,7 +1683,12 @@ int batch_refresh(mlem_batch* b, int chunk) {
         sig.push_back(reinterpret_cast<const void*>((uintptr_t)c->Bp));
         sig.push_back(reinterpret_cast<const void*>((uintptr_t)c->B));
     }
-    if (!tile_ok_all(b, b->tile)) {
+    for (size_t i = 0; i < b->ctx.size(); ++i)
+        if (b->tiles[i] && !tile_ok(b->tiles[i], b->ctx[i]->Bp)) {  // new frame count
+            b->tiles[i] = 0;
+            reschedule = true;
+        }
+    if (!batch_tile_ok(b, b->tile)) {
         b->tile = batch_default_tile(b);
         reschedule = true;
     }
@@ -1625,6 +1696,7 @@ int batch_refresh(mlem_batch* b, int chunk) {
         b->graph_dirty = true;
         b->graph_sig = sig;
     }
+    if (build_groups(b)) reschedule = true;
     if (reschedule) TRY(batch_schedule(b));
     return MLEM_OK;
 }
@@ -1639,12 +1711,20 @@ int bmark(mlem_batch* b, const PhaseEvents* pe, int i) {
 int batch_enqueue(mlem_batch* b, bool stats, const PhaseEvents* pe = nullptr) {
     cudaStream_t st = b->stream;
     TRY(bmark(b, pe, 0));
-    if (b->policy == MLEM_BATCH_ITEMS)
-        BCK(b, batch_fused(b->table, b->items_d, (uint32_t)b->items.size(), b->counter, b->tile,
-                           b->visit == MLEM_VISIT_SORTED, b->n_sm, b->blocks_per_sm, st));
-    else
-        BCK(b, batch_interleaved(b->table, b->tile, b->visit == MLEM_VISIT_SORTED, b->n_sm,
-                                 b->blocks_per_sm, st));
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        const mlem_batch::Group& g = b->groups[gi];
+        unsigned int* counter = b->counter + gi * kCounterStride;
+        const BatchItem* items = b->items_d + g.item0;
+        if (b->policy == MLEM_BATCH_ITEMS && b->visit == MLEM_VISIT_SORTED_STAGED)
+            BCK(b, batch_staged(g.table, items, g.n_items, counter, g.tile, b->n_sm,
+                                b->blocks_per_sm, st));
+        else if (b->policy == MLEM_BATCH_ITEMS)
+            BCK(b, batch_fused(g.table, items, g.n_items, counter, g.tile,
+                               b->visit == MLEM_VISIT_SORTED, b->n_sm, b->blocks_per_sm, st));
+        else
+            BCK(b, batch_interleaved(g.table, g.tile, b->visit == MLEM_VISIT_SORTED, b->n_sm,
+                                     b->blocks_per_sm, st));
+    }
     TRY(bmark(b, pe, 1));
     TRY(bmark(b, pe, 2));
     for (mlem_ctx* c : b->ctx) BCK(b, apply_update(c->x, c->update, c->norm, c->C, c->Bp, true, st));
@@ -1734,6 +1814,7 @@ int mlem_batch_create(mlem_batch** out, mlem_ctx* const* ctxs, uint32_t n_ctx) {
     }
     mlem_batch* b = new mlem_batch();
     b->ctx.assign(ctxs, ctxs + n_ctx);
+    b->tiles.assign(n_ctx, 0);
     b->device = ctxs[0]->device;
     b->n_sm = ctxs[0]->n_sm;
     b->stream = ctxs[0]->stream;
@@ -1790,8 +1871,10 @@ int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
     if (!b) return bfail(nullptr, MLEM_ERR_INVALID, "null batch");
     if (policy != MLEM_BATCH_INTERLEAVED && policy != MLEM_BATCH_ITEMS)
         return bfail(b, MLEM_ERR_INVALID, "unknown batch schedule %d", policy);
-    if (visit != MLEM_VISIT_FILE && visit != MLEM_VISIT_SORTED)
-        return bfail(b, MLEM_ERR_INVALID, "row visiting order %d is not a batch order", visit);
+    if (visit != MLEM_VISIT_FILE && visit != MLEM_VISIT_SORTED &&
+        !(visit == MLEM_VISIT_SORTED_STAGED && policy == MLEM_BATCH_ITEMS))
+        return bfail(b, MLEM_ERR_INVALID, "row visiting order %d is not a batch order for schedule %d",
+                     visit, policy);
     if (visit != MLEM_VISIT_FILE)
         for (size_t i = 0; i < b->ctx.size(); ++i)
             if (!b->ctx[i]->row_order)
@@ -1810,7 +1893,10 @@ int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
     b->visit = visit;
     b->items_per_block = items_per_block;
     b->blocks_per_sm = blocks_per_sm;
-    if (frame_tile != 0) b->tile = frame_tile;
+    if (frame_tile != 0) {  // one tile for every context again
+        b->tile = frame_tile;
+        std::fill(b->tiles.begin(), b->tiles.end(), 0);
+    }
     b->scheduled = false;
     b->graph_dirty = true;
     return batch_refresh(b, 1);
@@ -1827,6 +1913,32 @@ int mlem_batch_get_schedule(const mlem_batch* b, int* policy, uint32_t* items_pe
     if (frame_tile) *frame_tile = b->tile;
     if (n_items) *n_items = (uint32_t)b->items.size();
     if (ms_per_iter) *ms_per_iter = b->ms_per_iter;
+    return MLEM_OK;
+}
+
+int mlem_batch_set_tiles(mlem_batch* b, const int* tiles) {
+    if (!b || !tiles) return bfail(b, MLEM_ERR_INVALID, "null argument");
+    for (size_t i = 0; i < b->ctx.size(); ++i)
+        if (tiles[i] != 0 && !tile_ok(tiles[i], b->ctx[i]->Bp))
+            return bfail(b, MLEM_ERR_INVALID,
+                         "context %zu: frame tile %d must be 1, 2, 4, 8 or 16 and divide its padded "
+                         "frame count %u", i, tiles[i], b->ctx[i]->Bp);
+    std::vector<int> keep = b->tiles;
+    b->tiles.assign(tiles, tiles + b->ctx.size());
+    if (!batch_tile_ok(b, b->tile)) {
+        b->tiles = keep;
+        return bfail(b, MLEM_ERR_INVALID, "the batch frame tile %d does not divide the padded frame "
+                     "count of a context without a tile of its own", b->tile);
+    }
+    BCK(b, cudaSetDevice(b->device));
+    b->scheduled = false;
+    b->graph_dirty = true;
+    return batch_refresh(b, 1);
+}
+
+int mlem_batch_get_tiles(const mlem_batch* b, int* tiles) {
+    if (!b || !tiles) return bfail(const_cast<mlem_batch*>(b), MLEM_ERR_INVALID, "null argument");
+    for (size_t i = 0; i < b->ctx.size(); ++i) tiles[i] = eff_tile(b, i);
     return MLEM_OK;
 }
 
@@ -1894,9 +2006,35 @@ int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter) {
     for (int bps : {3, 8})
         if (s == MLEM_OK) s = trial(MLEM_BATCH_INTERLEAVED, best_ipb, bps, best_tile, best_visit);
     for (uint32_t ipb : {1u, 4u, 16u, 64u})
-        for (int v : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED})
+        for (int v : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED, MLEM_VISIT_SORTED_STAGED})
             if (s == MLEM_OK && (v == MLEM_VISIT_FILE || sorted_ok))
                 s = trial(MLEM_BATCH_ITEMS, ipb, 4, best_tile, v);
+    // Then, with that schedule, a frame tile of its own for each context,
+    // heaviest first (contexts sharing a tile share a kernel).
+    std::vector<int> best_tiles(b->ctx.size(), 0);
+    if (s == MLEM_OK && b->ctx.size() > 1) {
+        s = mlem_batch_set_schedule(b, best_policy, best_ipb, best_bps, best_tile, best_visit);
+        std::vector<size_t> order(b->ctx.size());
+        for (size_t i = 0; i < order.size(); ++i) order[i] = i;
+        std::vector<double> cost(b->ctx.size());
+        for (size_t i = 0; i < cost.size(); ++i) cost[i] = item_cost(b, i, 0, b->ctx[i]->R);
+        std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t c) { return cost[a] > cost[c]; });
+        for (size_t i : order)
+            for (int t : {16, 8, 4, 2, 1}) {
+                if (s != MLEM_OK || !tile_ok(t, b->ctx[i]->Bp)) continue;
+                if (t == (best_tiles[i] ? best_tiles[i] : best_tile)) continue;
+                std::vector<int> cand = best_tiles;
+                cand[i] = t;
+                s = mlem_batch_set_tiles(b, cand.data());
+                double ms = 0.0;
+                if (s == MLEM_OK) s = batch_time(b, 2, e0, e1, &ms);
+                if (s == MLEM_OK) s = restore();
+                if (s == MLEM_OK && ms < best) {
+                    best = ms;
+                    best_tiles = cand;
+                }
+            }
+    }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     if (s == MLEM_OK) s = restore();
@@ -1905,6 +2043,7 @@ int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter) {
     release();
     if (s != MLEM_OK) return s;
     TRY(mlem_batch_set_schedule(b, best_policy, best_ipb, best_bps, best_tile, best_visit));
+    TRY(mlem_batch_set_tiles(b, best_tiles.data()));
     b->ms_per_iter = best;
     if (ms_per_iter) *ms_per_iter = best;
     return MLEM_OK;
@@ -1972,13 +2111,13 @@ int mlem_batch_profile(mlem_batch* b, int n, double* ms, double* bytes, int* lau
     for (size_t i = 0; i < b->ctx.size(); ++i) {
         double pb[MLEM_N_PHASES];
         int pl[MLEM_N_PHASES];
-        phase_bytes_for(b->ctx[i], MLEM_BK_FUSED, b->tile, pb, pl);
+        phase_bytes_for(b->ctx[i], MLEM_BK_FUSED, eff_tile(b, i), pb, pl);
         for (int p = 0; p < MLEM_N_PHASES; ++p) {
             tb[p] += pb[p];
             tl[p] += pl[p];
         }
     }
-    tl[MLEM_PHASE_PROJECT] = 1;  // one kernel for all matrices and frame tiles
+    tl[MLEM_PHASE_PROJECT] = (int)b->groups.size();  // one kernel per frame-tile group
     for (int p = 0; p < MLEM_N_PHASES; ++p) {
         if (ms) ms[p] = acc[p] / n;
         if (bytes) bytes[p] = tb[p];

@@ -20,6 +20,7 @@
 #include "common.cuh"
 #include "kernels.h"
 #include "row_dev.cuh"
+#include "staged_dev.cuh"
 
 namespace mlem {
 
@@ -50,6 +51,48 @@ __global__ void __launch_bounds__(kBatchThreads, 4) k_batch_fused(const BatchTab
             fused_row_range<32, BT, SORTED>(m.csr, m.x, Bp, f0, m.sino, m.u, item.row0, item.row1,
                                             warp, nwarps);
     }
+}
+
+// Items schedule with the staged row walk (staged_dev.cuh): the warps of a
+// CTA pipeline their rows of the item through shared-memory stages.  Sorted
+// visiting order only (the walk reads csr.vrange / csr.order).
+template <int BT>
+__global__ void __launch_bounds__(kBatchThreads, 4) k_batch_staged(const BatchTable t,
+                                                                    const BatchItem* __restrict__ items,
+                                                                    uint32_t n_items,
+                                                                    unsigned int* __restrict__ counter) {
+    extern __shared__ uint4 s_stage[];
+    __shared__ BatchItem s_item;
+    const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    const uint2* stages = reinterpret_cast<const uint2*>(s_stage) + (size_t)warp * kStages * kStageCap;
+    const uint32_t sa = (uint32_t)__cvta_generic_to_shared(stages);
+    for (;;) {
+        if (threadIdx.x == 0) {
+            const uint32_t it = atomicAdd(counter, 1u);
+            s_item = it < n_items ? items[it] : BatchItem{0u, 0u, 0u, 1u};
+        }
+        __syncthreads();
+        const BatchItem item = s_item;
+        __syncthreads();                 // s_item is rewritten by the next grab
+        if (item.pad) return;            // block-uniform: no items left
+        const BatchMat& m = t.mats[item.mat];
+        const uint32_t Bp = m.Bp;
+#pragma unroll 1
+        for (uint32_t f0 = 0; f0 < Bp; f0 += BT)
+            staged_walk<BT, kStages>(m.csr, m.x, Bp, f0, m.sino, m.u, item.row0 + warp, item.row1,
+                                     nwarps, stages, sa);
+    }
+}
+
+template <int BT>
+cudaError_t launch_batch_staged(const BatchTable& t, const BatchItem* items, uint32_t n_items,
+                                unsigned int* counter, int grid, cudaStream_t st) {
+    const size_t smem = staged_smem_bytes(kBatchThreads);
+    cudaError_t e = cudaFuncSetAttribute(k_batch_staged<BT>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    k_batch_staged<BT><<<grid, kBatchThreads, smem, st>>>(t, items, n_items, counter);
+    return cudaGetLastError();
 }
 
 // Interleaved schedule: the rows of all matrices form one virtual row space
@@ -157,6 +200,28 @@ cudaError_t batch_fused(const BatchTable& t, const BatchItem* items, uint32_t n_
                                                sm_count * blocks_per_sm));
     MLEM_BATCH_TILES(k_batch_fused, grid, kBatchThreads, 0, st>>>(t, items, n_items, counter))
     return cudaGetLastError();
+}
+
+cudaError_t batch_staged(const BatchTable& t, const BatchItem* items, uint32_t n_items,
+                         unsigned int* counter, int frame_tile, int sm_count, int blocks_per_sm,
+                         cudaStream_t st) {
+    if (n_items == 0) return cudaSuccess;
+    if (t.n == 0 || t.n > kBatchTableMax) return cudaErrorInvalidValue;
+    for (uint32_t i = 0; i < t.n; ++i)
+        if (!t.mats[i].csr.order || !t.mats[i].csr.vrange) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(counter, 0, sizeof(unsigned int), st);
+    if (e != cudaSuccess) return e;
+    // at most 4 resident CTAs: each holds 32 KiB of stages
+    const int grid = std::max(1, std::min<int>((int)std::min<uint32_t>(n_items, 1u << 30),
+                                               sm_count * std::min(blocks_per_sm, 4)));
+    switch (frame_tile) {
+        case 1: return launch_batch_staged<1>(t, items, n_items, counter, grid, st);
+        case 2: return launch_batch_staged<2>(t, items, n_items, counter, grid, st);
+        case 4: return launch_batch_staged<4>(t, items, n_items, counter, grid, st);
+        case 8: return launch_batch_staged<8>(t, items, n_items, counter, grid, st);
+        case 16: return launch_batch_staged<16>(t, items, n_items, counter, grid, st);
+        default: return cudaErrorInvalidValue;
+    }
 }
 #undef MLEM_BATCH_TILES
 

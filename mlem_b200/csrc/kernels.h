@@ -259,6 +259,11 @@ static_assert(sizeof(BatchTable) <= 32764, "kernel parameter space (CUDA >= 12.1
 cudaError_t batch_fused(const BatchTable& t, const BatchItem* items, uint32_t n_items,
                         unsigned int* counter, int frame_tile, bool sorted, int sm_count,
                         int blocks_per_sm, cudaStream_t st);
+// The items schedule with the staged row walk (staged_dev.cuh): every matrix
+// in its sorted order; at most 4 resident CTAs per SM.
+cudaError_t batch_staged(const BatchTable& t, const BatchItem* items, uint32_t n_items,
+                         unsigned int* counter, int frame_tile, int sm_count, int blocks_per_sm,
+                         cudaStream_t st);
 // One matrix in chunks (MLEM_VISIT_SORTED_CHUNKED): CTAs take chunks of
 // chunk_rows consecutive visiting positions from `counter` (reset here on the
 // stream), and do every frame tile of a chunk's rows back to back -- each CTA

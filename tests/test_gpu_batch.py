@@ -55,13 +55,14 @@ def _check(ctxs, members):
 
 
 IL, IT = api.BATCH_INTERLEAVED, api.BATCH_ITEMS
-FILE, SORTED = api.VISIT_FILE, api.VISIT_SORTED
+FILE, SORTED, STAGED = api.VISIT_FILE, api.VISIT_SORTED, api.VISIT_SORTED_STAGED
 
 
 @pytest.mark.parametrize("policy,items_per_block,blocks_per_sm,tile,visit", [
     (IL, 4, 4, 0, FILE), (IL, 1, 3, 1, SORTED), (IL, 1, 8, 4, FILE), (IL, 1, 4, 2, SORTED),
     (IT, 4, 4, 0, FILE), (IT, 1, 3, 4, SORTED), (IT, 32, 4, 2, SORTED), (IT, 2, 1, 1, FILE),
-    (IT, 1024, 8, 4, SORTED), (IT, 16, 4, 4, SORTED)])
+    (IT, 1024, 8, 4, SORTED), (IT, 16, 4, 4, SORTED),
+    (IT, 4, 4, 0, STAGED), (IT, 1, 3, 1, STAGED), (IT, 64, 8, 4, STAGED), (IT, 1024, 4, 2, STAGED)])
 def test_batch_matches_oracle(members, policy, items_per_block, blocks_per_sm, tile, visit):
     ctxs = _contexts(members)
     try:
@@ -74,6 +75,34 @@ def test_batch_matches_oracle(members, policy, items_per_block, blocks_per_sm, t
             if tile:
                 assert sched["frame_tile"] == tile
             b.iterate(ITERS)
+        _check(ctxs, members)
+    finally:
+        for c in ctxs:
+            c.close()
+
+
+@pytest.mark.parametrize("policy,visit", [(IT, SORTED), (IT, STAGED), (IL, FILE)])
+@pytest.mark.parametrize("tiles", [[4, 16, 8], [1, 4, 2], [2, 0, 1], [0, 2, 0]])
+def test_batch_tiles_per_context(members, policy, visit, tiles):
+    """Contexts with frame tiles of their own (padded frame counts 4, 16, 8):
+    one kernel per tile group, every image equal to the oracle's."""
+    ctxs = _contexts(members)
+    try:
+        with api.Batch(ctxs) as b:
+            b.set_schedule(policy, 4, 4, 4, visit)
+            b.set_tiles(tiles)
+            assert b.tiles() == [t if t else 4 for t in tiles]
+            b.iterate(ITERS)
+            assert b.schedule()["tiles"] == [t if t else 4 for t in tiles]
+            _, _, launches = b.profile(1)
+            assert launches[0] == len(set(t if t else 4 for t in tiles))
+            ctxs_again = _contexts(members)  # fresh images: the profile ran one iteration
+            for c, c2 in zip(ctxs, ctxs_again):
+                c.set_images(c2.get_images())
+                c2.close()
+            b.iterate(ITERS)
+            b.set_schedule(policy, 4, 4, 2, visit)  # a batch tile again: every context follows it
+            assert b.tiles() == [2, 2, 2]
         _check(ctxs, members)
     finally:
         for c in ctxs:
@@ -111,6 +140,8 @@ def test_batch_autotune_restores_images(members):
             sched = b.autotune()
             assert sched["ms_per_iter"] > 0
             assert sched["frame_tile"] in (1, 2, 4)  # must divide 4, 8 and 16
+            for t, padded in zip(sched["tiles"], (4, 16, 8)):
+                assert t in (1, 2, 4, 8, 16) and padded % t == 0
             for c, x in zip(ctxs, before):
                 assert c.get_images().tobytes() == x.tobytes()
             b.iterate(ITERS)
@@ -171,11 +202,21 @@ def test_batch_rejects_bad_input(members):
                 b.set_schedule(IL, 4, 4, 0, 9)
             with pytest.raises(api.MlemError):  # a single-matrix order only
                 b.set_schedule(IT, 4, 4, 0, api.VISIT_SORTED_CHUNKED)
+            with pytest.raises(api.MlemError):  # staged: the items schedule only
+                b.set_schedule(IL, 4, 4, 0, STAGED)
+            with pytest.raises(api.MlemError):  # 8 does not divide the padded count 4
+                b.set_tiles([8, 0, 0])
+            with pytest.raises(api.MlemError):
+                b.set_tiles([4, 3, 0])
+            with pytest.raises(api.MlemError):
+                b.set_tiles([4, 4])
             b.iterate(ITERS)  # still usable after the rejected calls
         _check(ctxs, members)
         with api.Batch([unsorted] + ctxs[1:]) as b:
             with pytest.raises(api.MlemError):  # a context without a row order
                 b.set_schedule(IL, 4, 4, 0, SORTED)
+            with pytest.raises(api.MlemError):
+                b.set_schedule(IT, 4, 4, 0, STAGED)
     finally:
         for c in ctxs + [exact, bare, unsorted]:
             c.close()

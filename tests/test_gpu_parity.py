@@ -219,6 +219,7 @@ def test_skewed_matrix_long_rows_and_columns(golden):
             other.init_images()
             ctx.init_images()
             for policy, visit in ((api.BATCH_ITEMS, api.VISIT_SORTED),
+                                  (api.BATCH_ITEMS, api.VISIT_SORTED_STAGED),
                                   (api.BATCH_INTERLEAVED, api.VISIT_FILE)):
                 with api.Batch([ctx, other]) as b:
                     b.set_schedule(policy, 64, 4, 1, visit)
