@@ -116,6 +116,13 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def two_pass_bytes(nnz, rows, cols):
+    """Algorithmic bytes of one plain iteration as two passes over the matrix:
+    CSR (8R offsets + 8Z + 4C image + 4R sinogram + 4R correlation) and CSC
+    (8C offsets + 8Z + 4R correlation + 4C norm + 8C image read and write)."""
+    return float(16 * int(nnz) + 20 * int(rows) + 24 * int(cols))
+
+
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -304,6 +311,15 @@ def run_ours(a, rank, world, local_rank):
                    "l2": "inputs larger than L2 (6.2 GB matrix), no flush",
                    "parallelism": "replicas" if world > 1 else "single"},
         "hbm_gbs": round(total_bytes / (ms_per_step / 1e3) / 1e9, 1),
+        # the same iteration against the two-pass byte count of the reference's
+        # algorithm (CSR pass for calcFwProj + CSC pass for calcBkProj):
+        # 16 Z + 20 R + 24 C bytes, which the one-pass kernel does not move
+        "two_pass_formula": {
+            "bytes_per_iteration": two_pass_bytes(ctx.nnz, ctx.n_rows, ctx.n_cols),
+            "achieved_gbs": round(two_pass_bytes(ctx.nnz, ctx.n_rows, ctx.n_cols)
+                                  / (ms_per_step / 1e3) / 1e9, 1),
+            "frac": round(two_pass_bytes(ctx.nnz, ctx.n_rows, ctx.n_cols)
+                          / (ms_per_step / 1e3) / 1e9 / peak, 4)},
         "iteration_roofline_frac": round(total_bytes / (ms_per_step / 1e3) / 1e9 / peak, 4),
         "bytes_per_iteration": total_bytes,
         "roofline": roofline, "phases": phases, "e2e": e2e,

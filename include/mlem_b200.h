@@ -213,6 +213,25 @@ int mlem_set_tuning(mlem_ctx* ctx, const mlem_tuning* t);
  * image state is restored afterwards. */
 int mlem_autotune(mlem_ctx* ctx, int deterministic_only, mlem_tuning* best);
 
+/* ---- ordered subsets (OSEM) ---------------------------------------------
+ * No counterpart in the reference (its thesis names OSEM as future work).
+ * Rows are split into n_subsets interleaved subsets (row r in subset
+ * r % n_subsets) and every iteration of mlem_iterate / mlem_step_host runs
+ * them in order 0, 1, ...: the one-pass forward projection, correlation and
+ * back projection over the subset's rows, then
+ *   x *= norm_s != 0 ? u / norm_s : (norm != 0 ? 1 : u)
+ * with norm_s the subset's column sums (bit-exact sums over the CSC, in row
+ * order; atomic without a CSC), so a voxel the subset does not see keeps its
+ * value and one subset is the reference's calcUpdate.  The image statistics
+ * are taken after each full iteration.  Needs the one-pass method
+ * (MLEM_BK_FUSED, any row visit; mlem_autotune then tries only it); not in
+ * the bit-exact mode.  n_subsets 1 turns subsets off.  mlem_set_norm_d does
+ * not change the subset column sums. */
+int mlem_set_subsets(mlem_ctx* ctx, uint32_t n_subsets);
+int mlem_get_subsets(const mlem_ctx* ctx, uint32_t* n_subsets);
+/* Column sums of subset s (natural voxel order, C floats); n_subsets >= 2. */
+int mlem_subset_column_sums(mlem_ctx* ctx, uint32_t s, float* out);
+
 /* ---- device-pointer entry points (torch extension, custom drivers) ------ */
 /* y[R][B] = A x[C][B]. */
 int mlem_fwproj_d(mlem_ctx* ctx, const float* x, float* y, uint32_t n_frames, void* stream);

@@ -313,6 +313,21 @@ class Context:
         t = sig.MlemTuning(bk_mode, group, frame_tile, blocks_per_sm, visit, 0.0)
         self._chk(core_lib().mlem_set_tuning(self._h, ctypes.byref(t)))
 
+    def set_subsets(self, n: int) -> None:
+        """Ordered subsets (OSEM): rows r % n form subset r's sub-iteration;
+        1 turns them off.  Runs on the one-pass method (BK_FUSED)."""
+        self._chk(core_lib().mlem_set_subsets(self._h, int(n)))
+
+    def subsets(self) -> int:
+        n = ctypes.c_uint32()
+        self._chk(core_lib().mlem_get_subsets(self._h, ctypes.byref(n)))
+        return n.value
+
+    def subset_column_sums(self, s: int) -> np.ndarray:
+        out = np.zeros(self.n_cols, np.float32)
+        self._chk(core_lib().mlem_subset_column_sums(self._h, int(s), _p(out)))
+        return out
+
     def autotune(self, deterministic_only: bool = False) -> dict:
         t = sig.MlemTuning()
         self._chk(core_lib().mlem_autotune(self._h, 1 if deterministic_only else 0, ctypes.byref(t)))

@@ -59,6 +59,19 @@ struct mlem_ctx {
     ulonglong2* row_ranges = nullptr;  // element range of each visited row (row_ranges_build)
     unsigned int* counter = nullptr;  // work counter of the dynamically scheduled kernels
 
+    // Ordered subsets (mlem_set_subsets): row r in subset r % n_subsets.
+    // sub_norm[s * C ...]: subset column sums (device voxel order); the visiting
+    // lists hold every subset's rows back to back (subset s at sub_off[s]), in
+    // file order and, with a row order, in the sorted order, with their ranges.
+    uint32_t n_subsets = 1;
+    float* sub_norm = nullptr;
+    uint32_t* sub_file = nullptr;
+    ulonglong2* sub_file_ranges = nullptr;
+    uint32_t* sub_sorted = nullptr;
+    ulonglong2* sub_sorted_ranges = nullptr;
+    std::vector<uint64_t> sub_off;
+    size_t sub_bytes = 0;  // device bytes of the subset buffers
+
     // frames
     uint32_t B = 0, Bp = 0;
     std::vector<double> sumin;
@@ -534,11 +547,43 @@ int staged_ctas_per_sm(const mlem_tuning& t) { return std::min(4, std::max(1, t.
 bool chunk_visit(int visit) {
     return visit == MLEM_VISIT_SORTED_CHUNKED || visit == MLEM_VISIT_SORTED_STAGED;
 }
-uint32_t chunk_rows_of(const mlem_ctx* c, const mlem_tuning& t) {
+uint32_t chunk_rows_of(const mlem_ctx* c, const mlem_tuning& t, uint64_t rows) {
     const uint64_t ctas = (uint64_t)c->n_sm * (t.visit == MLEM_VISIT_SORTED_STAGED
                                                    ? staged_ctas_per_sm(t)
                                                    : chunk_ctas_per_sm(t));
-    return (uint32_t)std::max<uint64_t>(32, (c->R + ctas * 16 - 1) / (ctas * 16));
+    (void)c;
+    return (uint32_t)std::max<uint64_t>(32, (rows + ctas * 16 - 1) / (ctas * 16));
+}
+
+// The rows of subset s as the row kernels of tuning t walk them: the subset's
+// visiting list (sorted for the sorted visits when the row order exists, else
+// file order) as the view's order.
+SparseView subset_view(const mlem_ctx* c, const mlem_tuning& t, uint32_t s) {
+    SparseView v = csr_view(c);
+    const bool sorted = t.visit != MLEM_VISIT_FILE && c->sub_sorted;
+    const uint64_t o = c->sub_off[s];
+    v.order = (sorted ? c->sub_sorted : c->sub_file) + o;
+    v.vrange = (sorted ? c->sub_sorted_ranges : c->sub_file_ranges) + o;
+    v.n = (uint32_t)(c->sub_off[s + 1] - o);
+    return v;
+}
+
+// One-pass method over the rows of `csr` (all rows, or one subset's).
+int fused_pass(mlem_ctx* c, const mlem_tuning& t, const SparseView& csr, cudaStream_t st) {
+    const uint32_t Bp = c->Bp;
+    const uint32_t T = (uint32_t)t.frame_tile;
+    if (t.visit == MLEM_VISIT_SORTED_STAGED)
+        CK(c, fused_staged(csr, c->x, Bp, t.frame_tile, c->sino, c->update,
+                           chunk_rows_of(c, t, csr.n), staged_ctas_per_sm(t), c->counter,
+                           c->n_sm, st));
+    else if (t.visit == MLEM_VISIT_SORTED_CHUNKED)
+        CK(c, fused_chunked(csr, c->x, Bp, t.frame_tile, c->sino, c->update,
+                            chunk_rows_of(c, t, csr.n), chunk_ctas_per_sm(t), c->counter,
+                            c->n_sm, st));
+    else
+        for (uint32_t f0 = 0; f0 < Bp; f0 += T)
+            CK(c, fused_row(csr, c->x, Bp, f0, c->sino, c->update, cfg_of(c, t), st));
+    return MLEM_OK;
 }
 
 int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
@@ -555,6 +600,10 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
     } else {
         const LaunchCfg cfg = cfg_of(c, t);
         const uint32_t T = (uint32_t)t.frame_tile;
+        if (c->n_subsets > 1 && t.bk_mode != MLEM_BK_FUSED)
+            return fail(c, MLEM_ERR_STATE,
+                        "ordered subsets run on the one-pass method (MLEM_BK_FUSED), not mode %d",
+                        t.bk_mode);
         switch (t.bk_mode) {
             case MLEM_BK_CSC:
                 if (!c->has_csc) return fail(c, MLEM_ERR_STATE, "no CSC copy (MLEM_FLAG_NO_CSC)");
@@ -575,17 +624,18 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                 CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
                 break;
             case MLEM_BK_FUSED:
-                if (t.visit == MLEM_VISIT_SORTED_STAGED)
-                    CK(c, fused_staged(csr, c->x, Bp, t.frame_tile, c->sino, c->update,
-                                       chunk_rows_of(c, t), staged_ctas_per_sm(t), c->counter,
-                                       c->n_sm, st));
-                else if (t.visit == MLEM_VISIT_SORTED_CHUNKED)
-                    CK(c, fused_chunked(csr, c->x, Bp, t.frame_tile, c->sino, c->update,
-                                        chunk_rows_of(c, t), chunk_ctas_per_sm(t), c->counter,
-                                        c->n_sm, st));
-                else
-                    for (uint32_t f0 = 0; f0 < Bp; f0 += T)
-                        CK(c, fused_row(csr, c->x, Bp, f0, c->sino, c->update, cfg, st));
+                if (c->n_subsets > 1) {
+                    // ordered subsets: a one-pass sub-iteration and its update per subset
+                    for (uint32_t s = 0; s < c->n_subsets; ++s) {
+                        TRY(fused_pass(c, t, subset_view(c, t, s), st));
+                        CK(c, apply_update_subset(c->x, c->update, c->sub_norm + (size_t)s * c->C,
+                                                  c->norm, c->C, Bp, st));
+                    }
+                    TRY(mark(c, pe, 1));
+                    TRY(mark(c, pe, 2));
+                    break;
+                }
+                TRY(fused_pass(c, t, csr, st));
                 TRY(mark(c, pe, 1));
                 TRY(mark(c, pe, 2));
                 CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
@@ -638,6 +688,17 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
         bytes[1] = tiles * pass + B * (4.0 * S + 8.0 * C) + 4.0 * C;  // c per segment, x r/w, norm
         launches[0] = nt + 1;
         launches[1] = nt;
+        bytes[3] = 4.0 * C * B;
+        launches[3] = 2;
+        return;
+    }
+    if (mode == MLEM_BK_FUSED && !exact && c->n_subsets > 1) {
+        // ordered subsets: the matrix once, x and the update once per subset,
+        // and per subset an update pass (norm_s, norm, u and x r/w) inside phase 0
+        const double S = (double)c->n_subsets;
+        bytes[0] = tiles * csr_pass + B * 4.0 * R + S * B * 8.0 * C +
+                   S * (8.0 * C + B * 16.0 * C);
+        launches[0] = (int)S * ((chunk_visit(c->tuning.visit) ? 1 : nt) + 1);
         bytes[3] = 4.0 * C * B;
         launches[3] = 2;
         return;
@@ -868,7 +929,9 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->tmp_r[1], (void*)c->tmp_c[0], (void*)c->tmp_c[1], (void*)c->tmp_c[2],
                     (void*)c->tmp_sino, (void*)c->tmp_d, (void*)c->norm_nat, (void*)c->perm,
                     (void*)c->pscratch[0], (void*)c->pscratch[1], (void*)c->row_order,
-                    (void*)c->row_ranges, (void*)c->counter})
+                    (void*)c->row_ranges, (void*)c->counter, (void*)c->sub_norm,
+                    (void*)c->sub_file, (void*)c->sub_file_ranges, (void*)c->sub_sorted,
+                    (void*)c->sub_sorted_ranges})
         dev_free(p);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -908,6 +971,8 @@ int mlem_kernels_per_iteration(const mlem_ctx* c, int* n) {
     else if (c->tuning.bk_mode == MLEM_BK_CSC) k += 2 * tiles;
     else if (c->tuning.bk_mode == MLEM_BK_ATOMIC) k += 2 * tiles + 1;
     else if (c->tuning.bk_mode == MLEM_BK_REGION) k += 2 * tiles + 1;  // + correl
+    else if (c->n_subsets > 1)  // per subset: the one-pass launch(es) and the update
+        k += (int)c->n_subsets * ((chunk_visit(c->tuning.visit) ? 1 : tiles) + 1);
     else if (chunk_visit(c->tuning.visit)) k += 2;  // all tiles in one launch
     else k += tiles + 1;
     *n = k;
@@ -1219,6 +1284,9 @@ int mlem_set_tuning(mlem_ctx* c, const mlem_tuning* t) {
                     "sorted row visiting needs the row order (context made with MLEM_FLAG_NO_ROW_ORDER)");
     if (chunk_visit(n.visit) && n.group != 32)
         return fail(c, MLEM_ERR_INVALID, "the chunked row visits run 32 lanes per row (group 32)");
+    if (c->n_subsets > 1 && n.bk_mode != MLEM_BK_FUSED)
+        return fail(c, MLEM_ERR_INVALID,
+                    "ordered subsets run on the one-pass method (MLEM_BK_FUSED) only");
     if (n.bk_mode == MLEM_BK_REGION) {
         TRY(set_device(c));
         TRY(ensure_region(c, n.frame_tile));
@@ -1242,8 +1310,15 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
     TRY(dev_alloc(c, &saved, (size_t)c->C * c->Bp));
     CK(c, cudaMemcpyAsync(saved, c->x, xb, cudaMemcpyDeviceToDevice, c->stream));
     std::vector<int> modes;
-    if (c->has_csc) modes.push_back(MLEM_BK_CSC);
-    if (!deterministic_only) {
+    if (c->has_csc && c->n_subsets == 1) modes.push_back(MLEM_BK_CSC);
+    if (c->n_subsets > 1) {
+        if (deterministic_only) {
+            cudaFree(saved);
+            c->device_bytes -= xb;
+            return fail(c, MLEM_ERR_STATE, "ordered subsets have no deterministic method");
+        }
+        modes.push_back(MLEM_BK_FUSED);
+    } else if (!deterministic_only) {
         modes.push_back(MLEM_BK_ATOMIC);
         modes.push_back(MLEM_BK_FUSED);
         modes.push_back(MLEM_BK_REGION);
@@ -1303,6 +1378,109 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
     c->tuning = best;
     c->graph_dirty = true;
     if (best_out) *best_out = best;
+    return MLEM_OK;
+}
+
+// ---- ordered subsets ----------------------------------------------------------
+
+namespace {
+
+void free_subsets(mlem_ctx* c) {
+    for (void** p : {(void**)&c->sub_norm, (void**)&c->sub_file, (void**)&c->sub_file_ranges,
+                     (void**)&c->sub_sorted, (void**)&c->sub_sorted_ranges}) {
+        dev_free(*p);
+        *p = nullptr;
+    }
+    c->sub_off.clear();
+    c->n_subsets = 1;
+    c->device_bytes -= c->sub_bytes;
+    c->sub_bytes = 0;
+}
+
+// Upload a visiting list (every subset's rows back to back) and build its ranges.
+int upload_list(mlem_ctx* c, const std::vector<uint32_t>& list, uint32_t** order,
+                ulonglong2** ranges) {
+    TRY(dev_alloc(c, order, c->R));
+    TRY(dev_alloc(c, ranges, c->R));
+    CK(c, cudaMemcpyAsync(*order, list.data(), (size_t)c->R * 4, cudaMemcpyHostToDevice, c->stream));
+    CK(c, row_ranges_build(csr_view(c), *order, *ranges, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));  // `list` is freed by the caller
+    return MLEM_OK;
+}
+
+}  // namespace
+
+int mlem_set_subsets(mlem_ctx* c, uint32_t n) {
+    if (!c) return fail(nullptr, MLEM_ERR_INVALID, "null context");
+    if (n == 0) return fail(c, MLEM_ERR_INVALID, "at least one subset");
+    if (n > 1 && (c->flags & MLEM_FLAG_EXACT))
+        return fail(c, MLEM_ERR_INVALID, "ordered subsets do not run in the bit-exact mode");
+    if (n > 1 && n > c->R)
+        return fail(c, MLEM_ERR_INVALID, "%u subsets for %u rows", n, c->R);
+    TRY(set_device(c));
+    CK(c, cudaStreamSynchronize(c->stream));
+    free_subsets(c);
+    c->graph_dirty = true;
+    if (n == 1) return MLEM_OK;
+    const size_t before = c->device_bytes;
+    auto bail = [&](int s) {
+        c->sub_bytes = c->device_bytes - before;
+        free_subsets(c);
+        return s;
+    };
+    // column sums of every subset (device voxel order)
+    int s = dev_alloc(c, &c->sub_norm, (size_t)n * c->C);
+    if (s != MLEM_OK) return bail(s);
+    cudaError_t e = cudaSuccess;
+    if (c->has_csc) {
+        for (uint32_t k = 0; k < n && e == cudaSuccess; ++k)
+            e = subset_column_sums_exact(csc_view(c), n, k, c->sub_norm + (size_t)k * c->C, c->stream);
+    } else {
+        e = subset_column_sums_atomic(csr_view(c), n, c->C, c->sub_norm, c->stream);
+    }
+    if (e != cudaSuccess) return bail(fail(c, MLEM_ERR_CUDA, "subset column sums: %s", cudaGetErrorString(e)));
+    // visiting lists: subset k holds rows k, k + n, ... (file order), or those
+    // rows in the order of the row sort
+    c->sub_off.assign((size_t)n + 1, 0);
+    for (uint32_t k = 0; k < n; ++k)
+        c->sub_off[k + 1] = c->sub_off[k] + (k < c->R ? (c->R - k + n - 1) / n : 0);
+    std::vector<uint32_t> list(c->R);
+    for (uint32_t k = 0; k < n; ++k) {
+        uint64_t o = c->sub_off[k];
+        for (uint32_t r = k; r < c->R; r += n) list[o++] = r;
+    }
+    s = upload_list(c, list, &c->sub_file, &c->sub_file_ranges);
+    if (s != MLEM_OK) return bail(s);
+    if (c->row_order) {
+        std::vector<uint32_t> order(c->R);
+        e = cudaMemcpy(order.data(), c->row_order, (size_t)c->R * 4, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) return bail(fail(c, MLEM_ERR_CUDA, "row order: %s", cudaGetErrorString(e)));
+        std::vector<uint64_t> next(c->sub_off.begin(), c->sub_off.end() - 1);
+        for (uint32_t r : order) list[next[r % n]++] = r;  // stable partition by subset
+        s = upload_list(c, list, &c->sub_sorted, &c->sub_sorted_ranges);
+        if (s != MLEM_OK) return bail(s);
+    }
+    c->n_subsets = n;
+    c->sub_bytes = c->device_bytes - before;
+    return MLEM_OK;
+}
+
+int mlem_get_subsets(const mlem_ctx* c, uint32_t* n) {
+    if (!c || !n) return fail(const_cast<mlem_ctx*>(c), MLEM_ERR_INVALID, "null argument");
+    *n = c->n_subsets;
+    return MLEM_OK;
+}
+
+int mlem_subset_column_sums(mlem_ctx* c, uint32_t s, float* out) {
+    if (!c || !out) return fail(c, MLEM_ERR_INVALID, "null argument");
+    if (c->n_subsets < 2 || s >= c->n_subsets)
+        return fail(c, MLEM_ERR_INVALID, "subset %u of %u", s, c->n_subsets);
+    TRY(set_device(c));
+    const float* src = c->sub_norm + (size_t)s * c->C;
+    std::vector<float> dev(c->C);
+    CK(c, cudaMemcpyAsync(dev.data(), src, (size_t)c->C * 4, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    for (uint32_t i = 0; i < c->C; ++i) out[i] = dev[c->bricked ? c->perm_host[i] : i];
     return MLEM_OK;
 }
 
@@ -1665,6 +1843,8 @@ int batch_refresh(mlem_batch* b, int chunk) {
         mlem_ctx* c = b->ctx[i];
         if (!c->B || !c->images_ready)
             return bfail(b, MLEM_ERR_STATE, "context %zu: sinograms and images not set", i);
+        if (c->n_subsets > 1)
+            return bfail(b, MLEM_ERR_STATE, "context %zu: ordered subsets do not run in a batch", i);
         if (c->stream != b->stream) BCK(b, cudaStreamSynchronize(c->stream));
         TRY(bctx(b, c, ensure_history(c, chunk)));
         if (t.mats[i].Bp != c->Bp) reschedule = true;

@@ -253,6 +253,65 @@ __global__ void __launch_bounds__(256) k_colsum_exact(SparseView csc, float* __r
     }
 }
 
+// Column sums of the rows of subset s (row % S == s), in ascending row order:
+// the elements of other subsets enter the sequential sum as +0, which leaves
+// a non-negative float sum unchanged, so the result is calcColumnSums over the
+// subset's rows bit for bit.
+__global__ void __launch_bounds__(256) k_colsum_subset_exact(SparseView csc, uint32_t S, uint32_t s,
+                                                             float* __restrict__ norm) {
+    const uint2* el = reinterpret_cast<const uint2*>(csc.pairs);
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t col = warp; col < csc.n; col += nwarps) {
+        const uint64_t b = csc.ptr[col], e = csc.ptr[col + 1];
+        float acc = 0.0f;
+        for (uint64_t base = b; base < e; base += 32) {
+            float v = 0.0f;
+            if (base + lane < e) {
+                const uint2 q = el[base + lane];
+                if (q.x % S == s) v = __uint_as_float(q.y);
+            }
+            const int cnt = (int)min((uint64_t)32, e - base);
+            for (int j = 0; j < cnt; ++j) acc = __fadd_rn(acc, __shfl_sync(MLEM_FULL_MASK, v, j));
+        }
+        if (lane == 0) norm[col] = acc;
+    }
+}
+
+// Column sums of every subset at once by atomics (no CSC): norm[(r % S) * C + col].
+__global__ void k_colsum_subset_atomic(SparseView csr, uint32_t S, uint64_t C,
+                                       float* __restrict__ norm) {
+    const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
+    const int lane = threadIdx.x & 31;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t r = warp; r < csr.n; r += nwarps) {
+        float* ns = norm + (r % S) * C;
+        for (uint64_t k = csr.ptr[r] + lane; k < csr.ptr[r + 1]; k += 32) {
+            const uint2 q = el[k];
+            atomicAdd(ns + q.x, __uint_as_float(q.y));
+        }
+    }
+}
+
+// The ordered-subsets update: x *= norm_s != 0 ? u / norm_s : (norm != 0 ? 1 : u),
+// u = 0 afterwards.  A voxel the subset does not see keeps its value; with one
+// subset (norm_s == norm) this is calcUpdate.
+template <bool ONE_FRAME>
+__global__ void k_apply_update_subset(float* __restrict__ x, float* __restrict__ u,
+                                      const float* __restrict__ norm_s,
+                                      const float* __restrict__ norm, uint64_t n, uint32_t B) {
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t col = ONE_FRAME ? i : i / B;
+        const float ns = norm_s[col];
+        const float f = ns != 0.0f ? u[i] / ns : (norm[col] != 0.0f ? 1.0f : u[i]);
+        x[i] *= f;
+        u[i] = 0.0f;
+    }
+}
+
 __global__ void k_colsum_atomic(SparseView csr, float* __restrict__ norm) {
     const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
     for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < csr.nnz;
@@ -369,6 +428,33 @@ cudaError_t apply_update(float* x, float* u, const float* norm, uint32_t C, uint
     const int grid = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)kB200SMs * 16);
     if (B == 1) k_apply_update<true><<<grid, 256, 0, st>>>(x, u, norm, n, B, zero_u);
     else k_apply_update<false><<<grid, 256, 0, st>>>(x, u, norm, n, B, zero_u);
+    return cudaGetLastError();
+}
+
+cudaError_t apply_update_subset(float* x, float* u, const float* norm_s, const float* norm,
+                                uint32_t C, uint32_t B, cudaStream_t st) {
+    const uint64_t n = (uint64_t)C * B;
+    if (n == 0) return cudaSuccess;
+    const int grid = (int)std::min<uint64_t>((n + 255) / 256, (uint64_t)kB200SMs * 16);
+    if (B == 1) k_apply_update_subset<true><<<grid, 256, 0, st>>>(x, u, norm_s, norm, n, B);
+    else k_apply_update_subset<false><<<grid, 256, 0, st>>>(x, u, norm_s, norm, n, B);
+    return cudaGetLastError();
+}
+
+cudaError_t subset_column_sums_exact(const SparseView& csc, uint32_t S, uint32_t s, float* norm,
+                                     cudaStream_t st) {
+    if (S == 0 || s >= S) return cudaErrorInvalidValue;
+    if (csc.n == 0) return cudaSuccess;
+    k_colsum_subset_exact<<<kB200SMs * 8, 256, 0, st>>>(csc, S, s, norm);
+    return cudaGetLastError();
+}
+
+cudaError_t subset_column_sums_atomic(const SparseView& csr, uint32_t S, uint32_t C, float* norm,
+                                      cudaStream_t st) {
+    if (S == 0) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(norm, 0, (size_t)S * C * 4, st);
+    if (e != cudaSuccess || csr.n == 0) return e;
+    k_colsum_subset_atomic<<<kB200SMs * 8, 256, 0, st>>>(csr, S, C, norm);
     return cudaGetLastError();
 }
 

@@ -72,6 +72,18 @@ cudaError_t fused_row(const SparseView& csr, const float* x, uint32_t B, uint32_
 cudaError_t apply_update(float* x, float* u, const float* norm, uint32_t C, uint32_t B,
                          bool zero_u, cudaStream_t st);
 
+// ---- ordered subsets (row r in subset r % S) -------------------------------
+// x *= norm_s != 0 ? u / norm_s : (norm != 0 ? 1 : u); u = 0.
+cudaError_t apply_update_subset(float* x, float* u, const float* norm_s, const float* norm,
+                                uint32_t C, uint32_t B, cudaStream_t st);
+// Column sums of subset s over the CSC, in ascending row order (bit-exact
+// with calcColumnSums over the subset's rows).
+cudaError_t subset_column_sums_exact(const SparseView& csc, uint32_t S, uint32_t s, float* norm,
+                                     cudaStream_t st);
+// All S subsets' column sums by atomics over the CSR: norm[s * C + col].
+cudaError_t subset_column_sums_atomic(const SparseView& csr, uint32_t S, uint32_t C, float* norm,
+                                      cudaStream_t st);
+
 // ---- bit-exact kernels: the float operation order of seqcsr4mlem --------
 cudaError_t fwproj_exact(const SparseView& csr, const float* x, uint32_t B, const int32_t* sino,
                          float* c, float* y, cudaStream_t st);

@@ -117,6 +117,75 @@ done:
     return rc;
 }
 
+void oracle_subset_column_sums(uint32_t R, uint32_t C, const uint64_t* row_end,
+                               const oracle_elem* e, uint32_t n_subsets, uint32_t s,
+                               float* norm) {
+    /* seqcsr4mlem.cpp:41-47 over the subset's rows, ascending. */
+    memset(norm, 0, (size_t)C * sizeof(float));
+    for (uint32_t r = s; r < R; r += n_subsets)
+        for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+            norm[e[k].index] += e[k].value;
+}
+
+int oracle_osem(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_elem* e,
+                const int32_t* sino, uint64_t S, int n_iter, uint32_t n_subsets, int ftz,
+                const float* start_image, float* image, float* image_sums) {
+    if (S != R) return -1;
+    if (n_subsets == 0) return -3;
+#ifdef ORACLE_HAVE_MXCSR
+    unsigned int saved = _mm_getcsr();
+    if (ftz) _MM_SET_FLUSH_ZERO_MODE(_MM_FLUSH_ZERO_ON); /* seqcsr4mlem.cpp:194 */
+#else
+    (void)ftz;
+#endif
+    float* fw = (float*)malloc((size_t)R * sizeof(float) + 1);
+    float* up = (float*)malloc((size_t)C * sizeof(float) + 1);
+    float* norm = (float*)malloc((size_t)C * sizeof(float) + 1);
+    float* nsub = (float*)malloc((size_t)C * n_subsets * sizeof(float) + 1);
+    int rc = 0;
+    if (!fw || !up || !norm || !nsub) { rc = -2; goto done; }
+
+    oracle_column_sums(R, C, row_end, e, norm);
+    for (uint32_t s = 0; s < n_subsets; ++s)
+        oracle_subset_column_sums(R, C, row_end, e, n_subsets, s, nsub + (size_t)s * C);
+    if (start_image) {
+        memcpy(image, start_image, (size_t)C * sizeof(float));
+    } else {
+        float init = oracle_init_value(C, norm, S, sino, NULL, NULL);
+        for (uint32_t i = 0; i < C; ++i) image[i] = init;
+    }
+    for (int it = 0; it < n_iter; ++it) {
+        for (uint32_t s = 0; s < n_subsets; ++s) {
+            const float* ns = nsub + (size_t)s * C;
+            /* calcFwProj + calcCorrel (seqcsr4mlem.cpp:76-99) on the subset's rows */
+            for (uint32_t r = s; r < R; r += n_subsets) {
+                float res = 0.0f;
+                for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+                    res += e[k].value * image[e[k].index];
+                fw[r] = (res != 0.0) ? ((float)sino[r] / res) : 0.0f;
+            }
+            /* calcBkProj (seqcsr4mlem.cpp:113-119) on the subset's rows */
+            memset(up, 0, (size_t)C * sizeof(float));
+            for (uint32_t r = s; r < R; r += n_subsets)
+                for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+                    up[e[k].index] += e[k].value * fw[r];
+            for (uint32_t i = 0; i < C; ++i)
+                image[i] *= (ns[i] != 0.0) ? (up[i] / ns[i]) : ((norm[i] != 0.0) ? 1.0f : up[i]);
+        }
+        if (image_sums) {
+            float sum = 0.0f; /* seqcsr4mlem.cpp:174-176 */
+            for (uint32_t i = 0; i < C; ++i) sum += image[i];
+            image_sums[it] = sum;
+        }
+    }
+done:
+    free(fw); free(up); free(norm); free(nsub);
+#ifdef ORACLE_HAVE_MXCSR
+    _mm_setcsr(saved);
+#endif
+    return rc;
+}
+
 int oracle_mlem_f64(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_elem* e,
                     const int32_t* sino, uint64_t S, int n_iter, double* image) {
     if (S != R) return -1;

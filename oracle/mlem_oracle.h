@@ -64,6 +64,29 @@ int oracle_mlem(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_el
                 const int32_t* sino, uint64_t S, int n_iter, int ftz,
                 const float* start_image, float* image, float* image_sums);
 
+/*
+ * Ordered subsets (OSEM, Hudson & Larkin 1994), which the reference names as
+ * future work but does not implement: row r belongs to subset r % n_subsets,
+ * and every iteration runs the subsets in order 0, 1, ...  A sub-iteration is
+ * the reference iteration restricted to the subset's rows (seqcsr4mlem.cpp:
+ * 69-120 visiting only those rows, in ascending order), followed by the update
+ *   x *= norm_s != 0 ? u / norm_s : (norm != 0 ? 1 : u)
+ * with norm_s the subset's column sums (calcColumnSums over the subset's rows,
+ * seqcsr4mlem.cpp:37-49): a voxel the subset does not see keeps its value,
+ * and with one subset this is calcUpdate (seqcsr4mlem.cpp:123-134), so
+ * oracle_osem(..., 1, ...) equals oracle_mlem bit for bit.  The initial image
+ * is initImage over the full column sums.  image_sums (may be NULL) gets the
+ * float image sum after each full iteration.
+ */
+int oracle_osem(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_elem* e,
+                const int32_t* sino, uint64_t S, int n_iter, uint32_t n_subsets, int ftz,
+                const float* start_image, float* image, float* image_sums);
+
+/* Column sums over the rows of subset s (r % n_subsets == s), in row order. */
+void oracle_subset_column_sums(uint32_t R, uint32_t C, const uint64_t* row_end,
+                               const oracle_elem* e, uint32_t n_subsets, uint32_t s,
+                               float* norm);
+
 /* FP64 oracle: the same iteration with double norm, projections, ratios and image. */
 int oracle_mlem_f64(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_elem* e,
                     const int32_t* sino, uint64_t S, int n_iter, double* image);

@@ -41,6 +41,9 @@ def lib():
         L.oracle_update.argtypes = [u32, _vp, _vp, _vp]
         L.oracle_mlem.restype = i32
         L.oracle_mlem.argtypes = [u32, u32, _vp, _vp, _vp, u64, i32, i32, _vp, _vp, _vp]
+        L.oracle_osem.restype = i32
+        L.oracle_osem.argtypes = [u32, u32, _vp, _vp, _vp, u64, i32, u32, i32, _vp, _vp, _vp]
+        L.oracle_subset_column_sums.argtypes = [u32, u32, _vp, _vp, u32, u32, _vp]
         L.oracle_mlem_f64.restype = i32
         L.oracle_mlem_f64.argtypes = [u32, u32, _vp, _vp, _vp, u64, i32, _vp]
         L.oracle_mlem_relaxed_f64.argtypes = [u32, u32, _vp, _vp, _vp, _vp, _vp, i32, _vp]
@@ -116,6 +119,29 @@ def mlem(m, sino, n_iter, ftz=True, start_image=None):
     if rc != 0:
         raise ValueError(f"oracle_mlem failed ({rc})")
     return img, sums[:n_iter]
+
+
+def osem(m, sino, n_iter, n_subsets, ftz=True, start_image=None):
+    """Ordered subsets of interleaved rows: (image float32[C], per-iteration sums)."""
+    re, el = _mat(m)
+    sino = np.ascontiguousarray(sino, np.int32)
+    img = np.zeros(m.n_cols, np.float32)
+    sums = np.zeros(max(n_iter, 1), np.float32)
+    st = None if start_image is None else np.ascontiguousarray(start_image, np.float32)
+    rc = lib().oracle_osem(m.n_rows, m.n_cols, _ptr(re), _ptr(el), _ptr(sino), sino.size,
+                           n_iter, n_subsets, 1 if ftz else 0, None if st is None else _ptr(st),
+                           _ptr(img), _ptr(sums))
+    if rc != 0:
+        raise ValueError(f"oracle_osem failed ({rc})")
+    return img, sums[:n_iter]
+
+
+def subset_column_sums(m, n_subsets, s):
+    re, el = _mat(m)
+    out = np.zeros(m.n_cols, np.float32)
+    lib().oracle_subset_column_sums(m.n_rows, m.n_cols, _ptr(re), _ptr(el), n_subsets, s,
+                                    _ptr(out))
+    return out
 
 
 def mlem_f64(m, sino, n_iter):
