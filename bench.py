@@ -51,6 +51,7 @@ def parse_args():
     ap.add_argument("--mode", choices=["auto", "csc", "atomic", "fused", "region"], default="auto",
                     help="back-projection method; auto = autotuned")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-osem", action="store_true")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the uneven three-geometry batch (one GPU only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -353,6 +354,32 @@ def run_ours(a, rank, world, local_rank):
             "frame_tile": tb["frame_tile"], "row_visit": api.VISIT_NAMES[tb["visit"]],
             "phases_ms": [round(float(x), 4) for x in bph_ms],
         }
+
+    # --- ordered subsets: 8 interleaved row subsets, the plain sinogram ---
+    if not a.no_osem:
+        n_sub = 8
+        ctx.set_sinograms(frames.sinograms)
+        ctx.init_images()
+        ctx.set_subsets(n_sub)
+        to = ctx.autotune()
+        ctx.init_images()
+        ctx.iterate(a.warmup, stats=False)
+        ko = max(10, a.steps // 2)
+        barrier()
+        e0.record(stream)
+        ctx.iterate(ko, stats=False)
+        e1.record(stream)
+        barrier()
+        oms = e0.elapsed_time(e1) / ko
+        line["osem"] = {
+            "workload": "plain-full", "subsets": n_sub, "ms_per_iteration": round(oms, 4),
+            "sub_iterations_per_s": round(n_sub * 1e3 / oms, 2),
+            "iteration_time_vs_plain": round(oms / ms_per_step, 3),
+            "frame_tile": to["frame_tile"], "group": to["group"],
+            "row_visit": api.VISIT_NAMES[to["visit"]],
+            "gpu_launches_per_iteration": int(ctx.kernels_per_iteration()),
+        }
+        ctx.set_subsets(1)
 
     # --- CPU baseline: the reference's openmpcsr4mlem on this host (rank 0, N=1) ---
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
