@@ -59,6 +59,12 @@ struct mlem_ctx {
     ulonglong2* row_ranges = nullptr;  // element range of each visited row (row_ranges_build)
     unsigned int* counter = nullptr;  // work counter of the dynamically scheduled kernels
 
+    // Rows longer than kLongRowElems, cut into segments (k_long.cu) for the
+    // one-pass method; f_long holds their forward sums (n_long x Bp).
+    LongSeg* long_segs = nullptr;
+    uint32_t n_long_segs = 0, n_long = 0;
+    float* f_long = nullptr;
+
     // Ordered subsets (mlem_set_subsets): row r in subset r % n_subsets.
     // sub_norm[s * C ...]: subset column sums (device voxel order); the visiting
     // lists hold every subset's rows back to back (subset s at sub_off[s]), in
@@ -309,6 +315,31 @@ bool region_ready(const mlem_ctx* c, int frame_tile) {
     return c->rb.el_fw && c->rb.rlog == rlog && c->rb.sblog == sblog && c->rb.gpw == gpw;
 }
 
+// The segment table of the rows longer than kLongRowElems (one-pass method).
+int build_long_rows(mlem_ctx* c) {
+    std::vector<uint64_t> rp((size_t)c->R + 1);
+    CK(c, cudaMemcpyAsync(rp.data(), c->row_ptr, rp.size() * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    std::vector<LongSeg> segs;
+    uint32_t n_long = 0;
+    for (uint32_t r = 0; r < c->R; ++r) {
+        const uint64_t b = rp[r], e = rp[(size_t)r + 1];
+        if (e - b <= kLongRowElems) continue;
+        for (uint64_t k = b; k < e; k += kLongSegElems)
+            segs.push_back(LongSeg{k, std::min(e, k + kLongSegElems), n_long, r});
+        ++n_long;
+    }
+    if (segs.size() > 0xffffffffull) return fail(c, MLEM_ERR_INVALID, "too many long-row segments");
+    if (segs.empty()) return MLEM_OK;
+    TRY(dev_alloc(c, &c->long_segs, segs.size()));
+    CK(c, cudaMemcpyAsync(c->long_segs, segs.data(), segs.size() * sizeof(LongSeg),
+                          cudaMemcpyHostToDevice, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    c->n_long_segs = (uint32_t)segs.size();
+    c->n_long = n_long;
+    return MLEM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Setup common to all create paths: validate, voxel order, CSC, column sums.
 // ---------------------------------------------------------------------------
@@ -385,6 +416,7 @@ int finish_create(mlem_ctx* c) {
         TRY(dev_alloc(c, &c->row_ranges, c->R));
         CK(c, row_ranges_build(csr_view(c), c->row_order, c->row_ranges, c->stream));
     }
+    if (c->max_row_len > kLongRowElems) TRY(build_long_rows(c));
     default_tuning(c);
     return MLEM_OK;
 }
@@ -449,10 +481,10 @@ int ensure_stage(mlem_ctx* c, size_t bytes) {
 
 void free_frames(mlem_ctx* c) {
     for (void* p : {(void*)c->sino, (void*)c->x, (void*)c->correl, (void*)c->update,
-                    (void*)c->stats_scratch, (void*)c->inits_dev})
+                    (void*)c->stats_scratch, (void*)c->inits_dev, (void*)c->f_long})
         dev_free(p);
     c->sino = nullptr; c->x = nullptr; c->correl = nullptr; c->update = nullptr;
-    c->stats_scratch = nullptr; c->inits_dev = nullptr;
+    c->stats_scratch = nullptr; c->inits_dev = nullptr; c->f_long = nullptr;
     c->B = c->Bp = 0;
     c->images_ready = false;
 }
@@ -470,6 +502,7 @@ int alloc_frames(mlem_ctx* c, uint32_t B) {
     TRY(dev_alloc(c, &c->update, (size_t)c->C * Bp));
     TRY(dev_alloc(c, &c->stats_scratch, stats_scratch_bytes(Bp)));
     TRY(dev_alloc(c, &c->inits_dev, Bp));
+    if (c->n_long) TRY(dev_alloc(c, &c->f_long, (size_t)c->n_long * Bp));
     CK(c, cudaMemsetAsync(c->sino, 0, (size_t)c->R * Bp * 4, c->stream));
     CK(c, cudaMemsetAsync(c->x, 0, (size_t)c->C * Bp * 4, c->stream));
     CK(c, cudaMemsetAsync(c->correl, 0, (size_t)c->R * Bp * 4, c->stream));
@@ -635,7 +668,16 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                     TRY(mark(c, pe, 2));
                     break;
                 }
-                TRY(fused_pass(c, t, csr, st));
+                if (c->n_long) {
+                    // the long rows are cut into segments for their own kernels
+                    SparseView v = csr;
+                    v.long_len = kLongRowElems;
+                    TRY(fused_pass(c, t, v, st));
+                    CK(c, long_rows_pass(csr, c->long_segs, c->n_long_segs, c->n_long, c->x, Bp,
+                                         t.frame_tile, c->sino, c->f_long, c->update, c->n_sm, st));
+                } else {
+                    TRY(fused_pass(c, t, csr, st));
+                }
                 TRY(mark(c, pe, 1));
                 TRY(mark(c, pe, 2));
                 CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
@@ -706,6 +748,7 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
     if (mode == MLEM_BK_FUSED) {
         bytes[0] = tiles * csr_pass + B * (4.0 * C + 4.0 * R + 4.0 * C);  // x, sino, update
         launches[0] = (!exact && chunk_visit(c->tuning.visit)) ? 1 : nt;
+        if (!exact && c->n_long) launches[0] += 2;  // the long-row kernels
     } else {
         bytes[0] = tiles * csr_pass + B * (4.0 * C + 4.0 * R + 4.0 * R);  // x, sino, correl
         launches[0] = exact ? 1 : nt;
@@ -929,7 +972,7 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->tmp_r[1], (void*)c->tmp_c[0], (void*)c->tmp_c[1], (void*)c->tmp_c[2],
                     (void*)c->tmp_sino, (void*)c->tmp_d, (void*)c->norm_nat, (void*)c->perm,
                     (void*)c->pscratch[0], (void*)c->pscratch[1], (void*)c->row_order,
-                    (void*)c->row_ranges, (void*)c->counter, (void*)c->sub_norm,
+                    (void*)c->row_ranges, (void*)c->counter, (void*)c->long_segs, (void*)c->sub_norm,
                     (void*)c->sub_file, (void*)c->sub_file_ranges, (void*)c->sub_sorted,
                     (void*)c->sub_sorted_ranges})
         dev_free(p);
@@ -973,8 +1016,8 @@ int mlem_kernels_per_iteration(const mlem_ctx* c, int* n) {
     else if (c->tuning.bk_mode == MLEM_BK_REGION) k += 2 * tiles + 1;  // + correl
     else if (c->n_subsets > 1)  // per subset: the one-pass launch(es) and the update
         k += (int)c->n_subsets * ((chunk_visit(c->tuning.visit) ? 1 : tiles) + 1);
-    else if (chunk_visit(c->tuning.visit)) k += 2;  // all tiles in one launch
-    else k += tiles + 1;
+    else if (chunk_visit(c->tuning.visit)) k += 2 + (c->n_long ? 2 : 0);  // all tiles in one launch
+    else k += tiles + 1 + (c->n_long ? 2 : 0);
     *n = k;
     return MLEM_OK;
 }

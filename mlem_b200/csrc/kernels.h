@@ -27,6 +27,9 @@ struct SparseView {
     // With `order`: vrange[k] = {ptr[order[k]], ptr[order[k] + 1]}, the
     // element range of the k-th visited row in one load (no order -> ptr chain).
     const ulonglong2* vrange = nullptr;
+    // The one-pass row walks treat a row with more elements as empty: it is
+    // left to the long-row kernels (k_long.cu).  Every other kernel ignores it.
+    uint64_t long_len = ~0ull;
 };
 
 // Row index of visiting position v.
@@ -67,6 +70,24 @@ cudaError_t bkproj_scatter(const SparseView& csr, const float* c, uint32_t B, ui
 // ---- one pass per row: forward projection, correlation, scatter ---------
 cudaError_t fused_row(const SparseView& csr, const float* x, uint32_t B, uint32_t f0,
                       const int32_t* sino, float* u, const LaunchCfg& cfg, cudaStream_t st);
+
+// ---- rows too long for one warp (k_long.cu) ------------------------------
+// Rows longer than kLongRowElems are cut into segments of at most
+// kLongSegElems elements: elements [b, e) of row `row`, the slot-th long row.
+constexpr uint64_t kLongRowElems = 4096;
+constexpr uint64_t kLongSegElems = 4096;
+struct LongSeg {
+    uint64_t b, e;
+    uint32_t slot, row;
+};
+// u += the one-pass contribution of the long rows: f_long (n_long x B floats)
+// is zeroed, the segments' partial sums are added into it, then every
+// segment scatters value x calcCorrel(count, f) into u (all B frames, in
+// passes of frame_tile).
+cudaError_t long_rows_pass(const SparseView& csr, const LongSeg* segs, uint32_t n_seg,
+                           uint32_t n_long, const float* x, uint32_t B, int frame_tile,
+                           const int32_t* sino, float* f_long, float* u, int sm_count,
+                           cudaStream_t st);
 
 // x[i] *= factor(u[i], norm[i/B]); u[i] = 0 when zero_u.
 cudaError_t apply_update(float* x, float* u, const float* norm, uint32_t C, uint32_t B,

@@ -213,6 +213,7 @@ __device__ __forceinline__ void fused_row_range(const SparseView& csr, const flo
                 e = csr.ptr[r + 1];
             }
         }
+        if (e - b > csr.long_len) e = b;  // left to the long-row kernels
         float acc[VW];
         uint2 kept[kBatch];
         const bool in_regs =

@@ -39,6 +39,12 @@ __device__ __forceinline__ void cp_wait() {
     asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
+// A range longer than long_len as an empty one: the long-row kernels take it.
+__device__ __forceinline__ ulonglong2 clamp_long(ulonglong2 q, uint64_t long_len) {
+    if (q.y - q.x > long_len) q.y = q.x;
+    return q;
+}
+
 // Whole 16-byte pairs covering elements [q.x, q.y): first pair, pair count.
 __device__ __forceinline__ bool stage_fits(ulonglong2 q) {
     const uint64_t a0 = q.x & ~1ull;
@@ -138,7 +144,7 @@ __device__ __forceinline__ void staged_walk(const SparseView& csr, const float* 
 #pragma unroll
     for (int i = 0; i < NS; ++i) {
         const uint64_t p = p0 + (uint64_t)i * S;
-        qr[i] = p < p_end ? csr.vrange[p] : make_ulonglong2(0ull, 0ull);
+        qr[i] = p < p_end ? clamp_long(csr.vrange[p], csr.long_len) : make_ulonglong2(0ull, 0ull);
         rr[i] = p < p_end ? csr.order[p] : 0u;
     }
 #pragma unroll
@@ -156,7 +162,7 @@ __device__ __forceinline__ void staged_walk(const SparseView& csr, const float* 
         const int sl = (stage + NS - 1) % NS;
         stage_issue(csr.pairs, qr[NS - 1], pl < p_end, sa + (uint32_t)sl * (kStageCap * 8), lane, ps);
         const uint64_t pn = pl + S;
-        const ulonglong2 qn = pn < p_end ? csr.vrange[pn] : make_ulonglong2(0ull, 0ull);
+        const ulonglong2 qn = pn < p_end ? clamp_long(csr.vrange[pn], csr.long_len) : make_ulonglong2(0ull, 0ull);
         const uint32_t rn = pn < p_end ? csr.order[pn] : 0u;
         int32_t s_nxt[VW];
         if (p + S < p_end) {

@@ -231,6 +231,37 @@ def test_skewed_matrix_long_rows_and_columns(golden):
                 assert ob.rel_l2(other.get_images()[0], want_o) <= TOL_MLEM
 
 
+@pytest.mark.parametrize("visit", [api.VISIT_FILE, api.VISIT_SORTED, api.VISIT_SORTED_CHUNKED,
+                                   api.VISIT_SORTED_STAGED])
+def test_long_rows_split_into_segments(visit):
+    """Rows longer than 4096 elements run as segments (k_long.cu) in the
+    one-pass method: rows at, just above and far above the limit, several
+    frames and frame tiles, against the oracle."""
+    rng = np.random.default_rng(11)
+    R, C = 2000, 4096
+    lens = rng.integers(0, 60, size=R)
+    lens[[3, 500, 501, 1999]] = [70000, 4096, 4097, 8193]
+    rows = [rng.integers(0, C, size=int(n)) for n in lens]
+    row_end = np.cumsum(lens).astype(np.uint64)
+    el = np.zeros(int(row_end[-1]), api.ELEM_DTYPE)
+    el["index"] = np.concatenate(rows).astype(np.uint32)
+    el["value"] = rng.uniform(0.1, 1.7, el.size).astype(np.float32)
+    m = formats.Csr4(R, C, row_end, el)
+    sinos = rng.poisson(40, (3, R)).astype(np.int32)
+    want = [ob.mlem(m, sinos[b], 6)[0] for b in range(3)]
+    with api.Context.from_matrix(m) as ctx:
+        ctx.set_sinograms(sinos)
+        for tile in (1, 2, 4):
+            ctx.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=tile, blocks_per_sm=4,
+                           visit=visit)
+            assert ctx.kernels_per_iteration() >= 6  # one-pass, two long-row kernels, update, stats
+            ctx.init_images()
+            ctx.iterate(6)
+            got = ctx.get_images()
+            for b in range(3):
+                assert ob.rel_l2(got[b], want[b]) <= TOL_MLEM, (tile, b)
+
+
 def test_invalid_inputs_raise():
     re_ = np.array([2, 3], np.uint64)
     el = np.zeros(3, api.ELEM_DTYPE)
