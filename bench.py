@@ -52,6 +52,7 @@ def parse_args():
                     help="back-projection method; auto = autotuned")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-osem", action="store_true")
+    ap.add_argument("--no-skewed", action="store_true")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the uneven three-geometry batch (one GPU only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -381,6 +382,10 @@ def run_ours(a, rank, world, local_rank):
         }
         ctx.set_subsets(1)
 
+    # --- a skewed matrix: the long rows run as segments (k_long.cu) ---
+    if not a.no_skewed:
+        line["skewed"] = skewed_line(a, stream, barrier)
+
     # --- CPU baseline: the reference's openmpcsr4mlem on this host (rank 0, N=1) ---
     if rank == 0 and world == 1 and not a.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_from_ctx(ctx, frames.sinograms[0], g, a.cpu_iters)
@@ -396,6 +401,48 @@ def run_ours(a, rank, world, local_rank):
     if dist is not None:
         dist.destroy_process_group()
     return line
+
+
+def skewed_line(a, stream, barrier):
+    """1,048,576 rows of 100-199 random elements plus 64 rows of 500,000 over
+    1,048,576 voxels (1.9e8 elements, seeded): the one-pass iteration with
+    the long rows cut into segments, autotuned, device-timed."""
+    import numpy as np
+    import torch
+
+    from mlem_b200 import api, formats
+
+    rng = np.random.default_rng(3)
+    R = C = 1 << 20
+    lens = rng.integers(100, 200, size=R)
+    lens[rng.choice(R, 64, replace=False)] = 500_000
+    row_end = np.cumsum(lens).astype(np.uint64)
+    Z = int(row_end[-1])
+    el = np.zeros(Z, api.ELEM_DTYPE)
+    el["index"] = rng.integers(0, C, size=Z, dtype=np.uint32)
+    el["value"] = rng.uniform(0.1, 1.7, Z).astype(np.float32)
+    sino = rng.poisson(30, R).astype(np.int32)
+    with api.Context.from_matrix(formats.Csr4(R, C, row_end, el), flags=api.FLAG_NO_CSC) as ctx:
+        del el
+        ctx.set_stream(stream.cuda_stream)
+        ctx.set_sinograms(sino)
+        ctx.init_images()
+        t = ctx.autotune()
+        ctx.init_images()
+        ctx.iterate(a.warmup, stats=False)
+        k = max(10, a.steps // 2)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(stream)
+        ctx.iterate(k, stats=False)
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1) / k
+        return {"workload": "skewed", "n_rows": R, "n_cols": C, "nnz": Z,
+                "long_rows": 64, "long_row_elements": 500_000, "ms_per_iteration": round(ms, 4),
+                "elements_per_s": round(Z / (ms / 1e3), 1),
+                "bk_mode": api.BK_NAMES[t["bk_mode"]], "row_visit": api.VISIT_NAMES[t["visit"]],
+                "gpu_launches_per_iteration": int(ctx.kernels_per_iteration())}
 
 
 def cpu_baseline_from_ctx(ctx, sino, g, iters):
