@@ -58,6 +58,10 @@ extern "C" {
 #define MLEM_FLAG_CHECKED 0x4u  /* accepted for compatibility: offsets and column indices are always validated */
 #define MLEM_FLAG_NATURAL_LAYOUT 0x8u /* keep the natural voxel order on the device (no Morton layout) */
 #define MLEM_FLAG_NO_ROW_ORDER 0x10u  /* visit rows in file order (no entry/exit-voxel sort of the rows) */
+#define MLEM_FLAG_EXPAND_SYMMETRY 0x20u /* mlem_create_from_file: regenerate the elements a
+                                           symmetry-compressed file omits (mlem_create_symmetric);
+                                           without it the symmetry flags are ignored, as the
+                                           reference's MLEM ignores them */
 
 /* ---- back-projection strategies ---------------------------------------- */
 #define MLEM_BK_AUTO 0    /* the autotuner's choice (CSC when not tuned) */
@@ -133,6 +137,28 @@ int mlem_create_grid(mlem_ctx** out, const uint64_t* row_end, const void* elems,
 /* Same, from a CSR4 file (the command-line driver's path; the grid comes
  * from the file's scanner block). */
 int mlem_create_from_file(mlem_ctx** out, const char* csr4_path, uint32_t flags, int device);
+
+/* Scanner symmetries of a symmetry-compressed CSR4 matrix (header flags @5:
+ * x = 1, y = 2, z = 4, csr4matrix.cpp:62-65) and the geometry they act on:
+ * rows are LORs d1 * n_crystals + d2 (n_rows = n_crystals^2, n_crystals =
+ * block_size * n_blocks * n_layers * n_rings) and columns voxels
+ * ix + nx * (iy + ny * iz) of the grid (n_cols = nx * ny * nz). */
+typedef struct {
+    uint32_t sym;
+    uint32_t n_layers, n_blocks, block_size, n_rings;
+    uint32_t grid[3];
+} mlem_symmetry;
+/* A context on the full matrix of a symmetry-compressed one: for every
+ * symmetry the flags allow (all combinations of x, y and z mirrors but the
+ * identity, x outermost, in the order of visualizematrix/symhandler.hpp:
+ * generateSyms), every stored row r adds its elements, with mirrored voxels,
+ * to row transformLor(r) (symhandler.hpp/.cpp: detector mirror tables).  In a
+ * full row the stored elements come first, then each symmetry's in that
+ * order, source rows ascending.  The expansion runs on the device; the stored
+ * arrays are read only during the call.  With sym == 0 this is mlem_create_grid. */
+int mlem_create_symmetric(mlem_ctx** out, const uint64_t* row_end, const void* elems,
+                          uint32_t n_rows, uint32_t n_cols, uint64_t nnz,
+                          const mlem_symmetry* sym, uint32_t flags, int device);
 
 /* Synthetic Siddon matrix generated on the device (bit-identical to the host
  * generator of mlem_b200/gen); the reference relies on an external generator. */
@@ -361,6 +387,7 @@ typedef struct {
     float voxel_size[3];
     uint64_t file_size;
     uint64_t data_offset; /* byte offset of the row END offsets */
+    uint32_t n_layers, n_blocks, block_size, n_rings; /* detector of the scanner block */
 } mlem_csr4_header;
 
 /* Parse and validate a CSR4 header like csr4matrix.cpp:32-138, with 64-bit

@@ -29,7 +29,15 @@ class MlemCsr4Header(ctypes.Structure):
                 ("nnz", ctypes.c_uint64), ("version", ctypes.c_uint8), ("flags", ctypes.c_uint8),
                 ("scan_config_bytes", ctypes.c_uint32), ("grid", ctypes.c_uint32 * 3),
                 ("voxel_size", ctypes.c_float * 3), ("file_size", ctypes.c_uint64),
-                ("data_offset", ctypes.c_uint64)]
+                ("data_offset", ctypes.c_uint64), ("n_layers", ctypes.c_uint32),
+                ("n_blocks", ctypes.c_uint32), ("block_size", ctypes.c_uint32),
+                ("n_rings", ctypes.c_uint32)]
+
+
+class MlemSymmetry(ctypes.Structure):
+    _fields_ = [("sym", ctypes.c_uint32), ("n_layers", ctypes.c_uint32),
+                ("n_blocks", ctypes.c_uint32), ("block_size", ctypes.c_uint32),
+                ("n_rings", ctypes.c_uint32), ("grid", ctypes.c_uint32 * 3)]
 
 
 _SCALARS = {
@@ -39,6 +47,7 @@ _SCALARS = {
 _STRUCT_PTRS = {
     "mlem_info*": ctypes.POINTER(MlemInfo), "mlem_tuning*": ctypes.POINTER(MlemTuning),
     "mlem_csr4_header*": ctypes.POINTER(MlemCsr4Header),
+    "mlem_symmetry*": ctypes.POINTER(MlemSymmetry),
 }
 
 

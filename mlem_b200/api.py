@@ -39,6 +39,7 @@ FLAG_NO_CSC = 0x2
 FLAG_CHECKED = 0x4
 FLAG_NATURAL_LAYOUT = 0x8
 FLAG_NO_ROW_ORDER = 0x10
+FLAG_EXPAND_SYMMETRY = 0x20
 
 BK_AUTO, BK_CSC, BK_ATOMIC, BK_FUSED, BK_REGION = 0, 1, 2, 3, 4
 BATCH_INTERLEAVED, BATCH_ITEMS = 0, 1
@@ -128,6 +129,22 @@ class Context:
     def from_file(cls, path: str, flags: int = 0, device: int = 0) -> "Context":
         h = ctypes.c_void_p()
         _raise(core_lib().mlem_create_from_file(ctypes.byref(h), str(path).encode(), flags, device))
+        return cls._wrap(h)
+
+    @classmethod
+    def symmetric(cls, m, flags: int = 0, device: int = 0) -> "Context":
+        """The full matrix of a symmetry-compressed formats.Csr4 (its header
+        flags select the mirrors, its scanner block and grid the geometry):
+        mlem_create_symmetric."""
+        n_layers, n_blocks, block_size, n_rings = m.scanner
+        sym = sig.MlemSymmetry(int(m.flags) & 7, n_layers, n_blocks, block_size, n_rings,
+                               (ctypes.c_uint32 * 3)(*m.grid))
+        re_ = np.ascontiguousarray(m.row_end, dtype=np.uint64)
+        el = np.ascontiguousarray(m.elems)
+        h = ctypes.c_void_p()
+        _raise(core_lib().mlem_create_symmetric(ctypes.byref(h), _p(re_), _p(el), m.n_rows,
+                                                m.n_cols, int(re_[-1]) if m.n_rows else 0,
+                                                ctypes.byref(sym), flags, device))
         return cls._wrap(h)
 
     @classmethod

@@ -440,7 +440,7 @@ int new_ctx(mlem_ctx** out, uint32_t R, uint32_t C, uint64_t Z, uint32_t flags, 
     if (device < 0 || device >= n_dev)
         return fail(nullptr, MLEM_ERR_INVALID, "device %d out of range (%d devices)", device, n_dev);
     if (flags & ~(MLEM_FLAG_EXACT | MLEM_FLAG_NO_CSC | MLEM_FLAG_CHECKED | MLEM_FLAG_NATURAL_LAYOUT |
-                  MLEM_FLAG_NO_ROW_ORDER))
+                  MLEM_FLAG_NO_ROW_ORDER | MLEM_FLAG_EXPAND_SYMMETRY))
         return fail(nullptr, MLEM_ERR_INVALID, "unknown flags 0x%x", flags);
     if ((flags & MLEM_FLAG_EXACT) && (flags & MLEM_FLAG_NO_CSC))
         return fail(nullptr, MLEM_ERR_INVALID, "MLEM_FLAG_EXACT needs the CSC copy");
@@ -892,6 +892,119 @@ int mlem_create_grid(mlem_ctx** out, const uint64_t* row_end, const void* elems,
             e = cudaMemcpyAsync(c->elems, elems, nnz * 8, cudaMemcpyHostToDevice, c->stream);
         if (e != cudaSuccess) s = fail(c, MLEM_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
     }
+    if (s == MLEM_OK) s = finish_create(c);
+    if (s != MLEM_OK) {
+        global_error() = c->err;
+        mlem_destroy(c);
+        return s;
+    }
+    *out = c;
+    return MLEM_OK;
+}
+
+int mlem_create_symmetric(mlem_ctx** out, const uint64_t* row_end, const void* elems,
+                          uint32_t n_rows, uint32_t n_cols, uint64_t nnz, const mlem_symmetry* sym,
+                          uint32_t flags, int device) {
+    if (!out || !sym) return fail(nullptr, MLEM_ERR_INVALID, "null argument");
+    *out = nullptr;
+    if (sym->sym == 0)
+        return mlem_create_grid(out, row_end, elems, n_rows, n_cols, nnz, sym->grid, flags, device);
+    if (sym->sym > 7u) return fail(nullptr, MLEM_ERR_INVALID, "symmetry flags 0x%x", sym->sym);
+    if ((n_rows && !row_end) || (nnz && !elems))
+        return fail(nullptr, MLEM_ERR_INVALID, "null matrix arrays");
+    const uint64_t nC = (uint64_t)sym->block_size * sym->n_blocks * sym->n_layers * sym->n_rings;
+    if (nC == 0 || nC * nC != n_rows)
+        return fail(nullptr, MLEM_ERR_MATRIX,
+                    "%u rows are not the %llu x %llu LORs of the scanner block", n_rows,
+                    (unsigned long long)nC, (unsigned long long)nC);
+    const uint64_t gC = (uint64_t)sym->grid[0] * sym->grid[1] * sym->grid[2];
+    if (gC == 0 || gC != n_cols)
+        return fail(nullptr, MLEM_ERR_MATRIX, "%u columns are not the %llu voxels of the grid",
+                    n_cols, (unsigned long long)gC);
+    uint64_t prev = 0;
+    for (uint32_t r = 0; r < n_rows; ++r) {
+        if (row_end[r] < prev) return fail(nullptr, MLEM_ERR_MATRIX, "row offsets decrease at row %u", r);
+        prev = row_end[r];
+    }
+    if (prev != nnz)
+        return fail(nullptr, MLEM_ERR_MATRIX, "last row END offset %llu differs from nnz %llu",
+                    (unsigned long long)prev, (unsigned long long)nnz);
+    mlem_ctx* c = nullptr;
+    TRY(new_ctx(&c, n_rows, n_cols, 0, flags, device));
+    const uint64_t base_bytes = c->device_bytes;
+    for (int i = 0; i < 3; ++i) c->grid[i] = sym->grid[i];
+    std::vector<uint32_t> lut;
+    sym_detector_luts(sym->n_layers, sym->n_blocks, sym->block_size, sym->n_rings, lut);
+    const std::vector<uint32_t> mirrors = sym_mirrors(sym->sym);
+    int s = MLEM_OK;
+    uint64_t* sptr = nullptr;
+    uint2* sel = nullptr;
+    uint32_t* dlut = nullptr;
+    unsigned long long* counts = nullptr;
+    void* scratch = nullptr;
+    unsigned int* bad = nullptr;
+    const size_t sb = scan_scratch_bytes(n_rows);
+    do {
+        // the stored matrix on the device, its columns checked before mirroring
+        if ((s = dev_alloc(c, &sptr, (size_t)n_rows + 1)) != MLEM_OK) break;
+        if ((s = dev_alloc(c, &sel, std::max<uint64_t>(nnz, 1))) != MLEM_OK) break;
+        if ((s = dev_alloc(c, &dlut, lut.size())) != MLEM_OK) break;
+        if ((s = dev_alloc(c, &counts, std::max<uint32_t>(n_rows, 1))) != MLEM_OK) break;
+        if ((s = dev_alloc(c, &scratch, sb)) != MLEM_OK) break;
+        if ((s = dev_alloc(c, &bad, 1)) != MLEM_OK) break;
+        cudaError_t e = cudaMemsetAsync(sptr, 0, 8, c->stream);
+        if (e == cudaSuccess && n_rows)
+            e = cudaMemcpyAsync(sptr + 1, row_end, (size_t)n_rows * 8, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess && nnz)
+            e = cudaMemcpyAsync(sel, elems, nnz * 8, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(dlut, lut.data(), lut.size() * 4, cudaMemcpyHostToDevice, c->stream);
+        const SparseView stored{sptr, reinterpret_cast<const uint4*>(sel), n_rows, nnz};
+        if (e == cudaSuccess) e = validate_csr(stored, n_cols, bad, c->stream);
+        unsigned int hbad = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&hbad, bad, 4, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) { s = fail(c, MLEM_ERR_CUDA, "symmetry upload: %s", cudaGetErrorString(e)); break; }
+        if (hbad & 4u) { s = fail(c, MLEM_ERR_MATRIX, "a column index is >= the number of columns"); break; }
+        // full row lengths, offsets, then the elements mirror by mirror
+        const SymExpand sx{sptr, sel, n_rows, dlut, (uint32_t)nC,
+                           {sym->grid[0], sym->grid[1], sym->grid[2]}};
+        e = cudaMemsetAsync(counts, 0, (size_t)n_rows * 8, c->stream);
+        if (e == cudaSuccess) e = sym_count(sx, 0, counts, c->stream);
+        for (uint32_t m : mirrors)
+            if (e == cudaSuccess) e = sym_count(sx, m, counts, c->stream);
+        if ((s = dev_alloc(c, &c->row_ptr, (size_t)n_rows + 1)) != MLEM_OK) break;
+        if (e == cudaSuccess)
+            e = exclusive_scan_u64(reinterpret_cast<const uint64_t*>(counts), c->row_ptr, n_rows,
+                                   scratch, sb, c->stream);
+        uint64_t Z = 0;
+        if (e == cudaSuccess) e = cudaMemcpyAsync(&Z, c->row_ptr + n_rows, 8, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) { s = fail(c, MLEM_ERR_CUDA, "symmetry count: %s", cudaGetErrorString(e)); break; }
+        c->Z = Z;
+        if ((s = dev_alloc(c, &c->elems, Z + 2)) != MLEM_OK) break;
+        if ((s = dev_alloc(c, &c->norm, std::max<uint32_t>(c->C, 1))) != MLEM_OK) break;
+        e = cudaMemsetAsync(c->elems + Z, 0, 2 * sizeof(uint2), c->stream);
+        // the cursors start at the full rows' offsets (the counts buffer is reused)
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(counts, c->row_ptr, (size_t)n_rows * 8, cudaMemcpyDeviceToDevice, c->stream);
+        if (e == cudaSuccess) e = sym_fill(sx, 0, counts, c->elems, c->stream);
+        for (uint32_t m : mirrors)
+            if (e == cudaSuccess) e = sym_fill(sx, m, counts, c->elems, c->stream);
+        std::vector<uint64_t> rp((size_t)n_rows + 1);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(rp.data(), c->row_ptr, rp.size() * 8, cudaMemcpyDeviceToHost, c->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) { s = fail(c, MLEM_ERR_CUDA, "symmetry fill: %s", cudaGetErrorString(e)); break; }
+        uint64_t mr = 0;
+        for (uint32_t r = 0; r < n_rows; ++r) mr = std::max(mr, rp[r + 1] - rp[r]);
+        c->max_row_len = (uint32_t)std::min<uint64_t>(mr, 0xffffffffu);
+    } while (0);
+    for (void* p : {(void*)sptr, (void*)sel, (void*)dlut, (void*)counts, scratch, (void*)bad}) dev_free(p);
+    // only the full matrix stays
+    c->device_bytes = base_bytes + (c->row_ptr ? ((uint64_t)n_rows + 1) * 8 : 0) +
+                      (c->elems ? (c->Z + 2) * 8 : 0) +
+                      (c->norm ? (uint64_t)std::max<uint32_t>(c->C, 1) * 4 : 0);
     if (s == MLEM_OK) s = finish_create(c);
     if (s != MLEM_OK) {
         global_error() = c->err;

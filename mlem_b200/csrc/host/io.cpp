@@ -127,7 +127,7 @@ int parse_header(const char* path, int fd, mlem_csr4_header* h) {
         return err(MLEM_ERR_FORMAT, "Error reading scanner geometry configuration");
     p += 20ull * n_layers;
     if (!need_bytes(8)) return err(MLEM_ERR_FORMAT, "Error reading scanner geometry configuration");
-    p += 4;  // nBlocks
+    const uint32_t n_blocks = rd<uint32_t>(p); p += 4;
     const uint32_t blocksize = rd<uint32_t>(p); p += 4;
     const uint64_t block_gaps = blocksize ? blocksize - 1ull : 0;
     if (block_gaps * 4 + 4 > (uint64_t)(end - p))
@@ -143,6 +143,10 @@ int parse_header(const char* path, int fd, mlem_csr4_header* h) {
     if ((uint64_t)(p - (head + kHeaderBytes)) != h->scan_config_bytes)
         return err(MLEM_ERR_FORMAT, "Error reading scanner geometry configuration");
     h->data_offset = kHeaderBytes + h->scan_config_bytes;
+    h->n_layers = n_layers;
+    h->n_blocks = n_blocks;
+    h->block_size = blocksize;
+    h->n_rings = n_rings;
     return MLEM_OK;
 }
 
@@ -351,7 +355,17 @@ int mlem_create_from_file(mlem_ctx** out, const char* path, uint32_t flags, int 
         std::memcpy(aligned.data(), base + h.data_offset, 8ull * h.n_rows);
         row_end = aligned.data();
     }
-    s = mlem_create_grid(out, row_end, elems, h.n_rows, h.n_cols, h.nnz, h.grid, flags, device);
+    if ((flags & MLEM_FLAG_EXPAND_SYMMETRY) && (h.flags & 7u)) {
+        // regenerate the elements the symmetries omitted (the reference's MLEM
+        // would use the stored ones only)
+        mlem_symmetry sym{h.flags & 7u, h.n_layers, h.n_blocks, h.block_size, h.n_rings,
+                          {h.grid[0], h.grid[1], h.grid[2]}};
+        s = mlem_create_symmetric(out, row_end, elems, h.n_rows, h.n_cols, h.nnz, &sym,
+                                  flags & ~MLEM_FLAG_EXPAND_SYMMETRY, device);
+    } else {
+        s = mlem_create_grid(out, row_end, elems, h.n_rows, h.n_cols, h.nnz, h.grid,
+                             flags & ~MLEM_FLAG_EXPAND_SYMMETRY, device);
+    }
     if (map) ::munmap(map, h.file_size);
     return s;
 }

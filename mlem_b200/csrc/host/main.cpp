@@ -20,7 +20,10 @@
 // (bit-exact kernels), MLEM_B200_AUTOTUNE=1 (tune the kernels for this
 // matrix before iterating; deterministic CSC back projection unless
 // MLEM_B200_AUTOTUNE=any), MLEM_B200_CSV=1 (print "iter,elapsed" lines like
-// openmpcsr4mlem built with -DMESSUNG, openmpcsr4mlem.cpp:217).
+// openmpcsr4mlem built with -DMESSUNG, openmpcsr4mlem.cpp:217),
+// MLEM_B200_EXPAND_SYMMETRY=1 (reconstruct with the full matrix of a
+// symmetry-compressed file; by default its symmetry flags are ignored, as the
+// reference's drivers ignore them).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -108,6 +111,7 @@ int run(int argc, char** argv) {
         if (o.has_checkpointing) std::cout << "Checkpointing: " << o.checkpointing << std::endl;
     }
     uint32_t flags = env_int("MLEM_B200_EXACT", 0) ? MLEM_FLAG_EXACT : 0u;
+    if (env_int("MLEM_B200_EXPAND_SYMMETRY", 0)) flags |= MLEM_FLAG_EXPAND_SYMMETRY;
     const int device = env_int("MLEM_B200_DEVICE", 0);
 
     auto t0 = std::chrono::steady_clock::now();

@@ -13,6 +13,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <vector>
+
 namespace mlem {
 
 struct SparseView {
@@ -70,6 +72,29 @@ cudaError_t bkproj_scatter(const SparseView& csr, const float* c, uint32_t B, ui
 // ---- one pass per row: forward projection, correlation, scatter ---------
 cudaError_t fused_row(const SparseView& csr, const float* x, uint32_t B, uint32_t f0,
                       const int32_t* sino, float* u, const LaunchCfg& cfg, cudaStream_t st);
+
+// ---- symmetry-compressed matrices (k_sym.cu) -----------------------------
+// The stored CSR (ptr R+1 with a leading 0, elements) and the mirror tables:
+// lut[m * n_crystals + d] = detector d mirrored by m (bit 0 x, 1 y, 2 z).
+struct SymExpand {
+    const uint64_t* ptr;
+    const uint2* el;
+    uint32_t R;
+    const uint32_t* lut;
+    uint32_t n_crystals;
+    uint32_t grid[3];
+};
+// Host: the 8 x n_crystals mirror tables (symhandler.cpp:33-114).
+void sym_detector_luts(uint32_t n_layers, uint32_t n_blocks, uint32_t block_size,
+                       uint32_t n_rings, std::vector<uint32_t>& lut);
+// Host: the mirrors a header's flags allow, in generateSyms order.
+std::vector<uint32_t> sym_mirrors(uint32_t sym);
+// counts[full row] += stored row length, for mirror m (0: the stored rows).
+cudaError_t sym_count(const SymExpand& s, uint32_t mirror, unsigned long long* counts,
+                      cudaStream_t st);
+// Copy mirror m's elements to the full rows' cursors, then advance them.
+cudaError_t sym_fill(const SymExpand& s, uint32_t mirror, unsigned long long* cursor, uint2* out,
+                     cudaStream_t st);
 
 // ---- rows too long for one warp (k_long.cu) ------------------------------
 // Rows longer than kLongRowElems are cut into segments of at most

@@ -46,6 +46,8 @@ class Csr4:
     flags: int = 0
     grid: tuple = (0, 0, 0)
     voxel_size: tuple = (1.0, 1.0, 1.0)
+    # detector of the scanner block: (n_layers, n_blocks, block_size, n_rings)
+    scanner: tuple = (1, 1, 1, 1)
 
     @property
     def nnz(self) -> int:
@@ -66,16 +68,22 @@ class Csr4:
         return self.elems["value"]
 
 
-def scanner_config_block(grid=(0, 0, 0), voxel_size=(1.0, 1.0, 1.0)) -> bytes:
-    """The minimal 60-byte scanner-geometry block csr4matrix.cpp:100-138 parses:
-    one layer (5 floats), one block of size 1 (no gaps), one ring (no gaps),
-    the voxel size and the voxel grid."""
-    b = struct.pack("<I5f", 1, 1.0, 1.0, 1.0, 1.0, 0.0)
-    b += struct.pack("<II", 1, 1)  # nBlocks, blocksize (blocksize-1 = 0 gaps)
-    b += struct.pack("<I", 1)  # nRings (0 gaps)
+def scanner_config_block(grid=(0, 0, 0), voxel_size=(1.0, 1.0, 1.0),
+                         scanner=(1, 1, 1, 1)) -> bytes:
+    """The scanner-geometry block csr4matrix.cpp:100-138 parses: n_layers
+    layers (5 floats each), n_blocks, block_size with block_size - 1 gaps,
+    n_rings with n_rings - 1 gaps, the voxel size and the voxel grid.  The
+    default is the minimal 60-byte block (one layer, one block of size 1, one
+    ring).  Crystal dimensions and gaps are written as 1.0 / 0.0: only the
+    counts matter to the MLEM path."""
+    n_layers, n_blocks, block_size, n_rings = scanner
+    b = struct.pack("<I", n_layers) + struct.pack("<5f", 1.0, 1.0, 1.0, 1.0, 0.0) * n_layers
+    b += struct.pack("<II", n_blocks, block_size) + struct.pack("<f", 0.0) * (block_size - 1)
+    b += struct.pack("<I", n_rings) + struct.pack("<f", 0.0) * (n_rings - 1)
     b += struct.pack("<3f", *voxel_size)
     b += struct.pack("<3I", *grid)
-    assert len(b) == CSR4_MIN_SCANCONFIG_BYTES
+    if scanner == (1, 1, 1, 1):
+        assert len(b) == CSR4_MIN_SCANCONFIG_BYTES
     return b
 
 
@@ -85,7 +93,7 @@ def csr4_header(n_rows: int, n_cols: int, nnz: int, scan: bytes, flags: int = 0)
 
 
 def write_csr4(path, n_rows, n_cols, row_end, elems, grid=(0, 0, 0),
-               voxel_size=(1.0, 1.0, 1.0), flags=0) -> None:
+               voxel_size=(1.0, 1.0, 1.0), flags=0, scanner=(1, 1, 1, 1)) -> None:
     row_end = np.ascontiguousarray(row_end, dtype=np.uint64)
     elems = np.ascontiguousarray(elems)
     if elems.dtype != ELEM_DTYPE:
@@ -95,7 +103,7 @@ def write_csr4(path, n_rows, n_cols, row_end, elems, grid=(0, 0, 0),
     nnz = int(row_end[-1]) if n_rows else 0
     if elems.shape[0] != nnz:
         raise ValueError("element count does not match the last row END offset")
-    scan = scanner_config_block(grid, voxel_size)
+    scan = scanner_config_block(grid, voxel_size, scanner)
     with open(path, "wb") as f:
         f.write(csr4_header(n_rows, n_cols, nnz, scan, flags))
         f.write(scan)
@@ -125,7 +133,7 @@ def read_csr4(path, mmap: bool = True) -> Csr4:
         raise ValueError("Cannot find scanner geometry configuration")
     p = CSR4_HEADER_BYTES
     (n_layers,) = struct.unpack_from("<I", head, p); p += 4 + 20 * n_layers
-    p += 4  # nBlocks
+    (n_blocks,) = struct.unpack_from("<I", head, p); p += 4
     (blocksize,) = struct.unpack_from("<I", head, p); p += 4 + 4 * max(blocksize - 1, 0)
     (n_rings,) = struct.unpack_from("<I", head, p); p += 4 + 4 * max(n_rings - 1, 0)
     voxel_size = struct.unpack_from("<3f", head, p); p += 12
@@ -142,7 +150,8 @@ def read_csr4(path, mmap: bool = True) -> Csr4:
             f.seek(off)
             row_end = np.fromfile(f, dtype=np.uint64, count=n_rows)
             elems = np.fromfile(f, dtype=ELEM_DTYPE, count=nnz)
-    return Csr4(n_rows, n_cols, row_end, elems, flags, tuple(grid), tuple(voxel_size))
+    return Csr4(n_rows, n_cols, row_end, elems, flags, tuple(grid), tuple(voxel_size),
+                (n_layers, n_blocks, blocksize, n_rings))
 
 
 def read_vector(path, dtype) -> np.ndarray:

@@ -186,6 +186,91 @@ done:
     return rc;
 }
 
+/* symhandler.cpp:33-114 initLUTs: crystal c = v + layer * per_layer + ring * per_ring. */
+static uint32_t sym_detector(uint32_t c, uint32_t m, uint32_t n_layers, uint32_t n_blocks,
+                             uint32_t block_size, uint32_t n_rings) {
+    const uint32_t per_layer = block_size * n_blocks, per_ring = per_layer * n_layers;
+    /* lut 7 = z(y(x)), 3 = y(x), 5 = z(x), 6 = z(y): apply x, then y, then z */
+    if (m & 1u) {
+        uint32_t v = c % per_layer, rest = c - v;
+        c = (per_layer - v + block_size - 1) % per_layer + rest;
+    }
+    if (m & 2u) {
+        uint32_t v = c % per_layer, rest = c - v;
+        c = (per_layer - v + block_size * (n_blocks / 2 + 1) - 1) % per_layer + rest;
+    }
+    if (m & 4u) {
+        uint32_t ring = c / per_ring, v = c % per_ring;
+        c = v + (n_rings - 1 - ring) * per_ring;
+    }
+    return c;
+}
+
+static uint32_t sym_lor(uint32_t r, uint32_t m, uint32_t nc, uint32_t n_layers, uint32_t n_blocks,
+                        uint32_t block_size, uint32_t n_rings) {
+    /* symhandler.hpp transformLor: mirror both detectors, smaller one first */
+    uint32_t d1 = sym_detector(r / nc, m, n_layers, n_blocks, block_size, n_rings);
+    uint32_t d2 = sym_detector(r % nc, m, n_layers, n_blocks, block_size, n_rings);
+    return d1 < d2 ? d1 * nc + d2 : d2 * nc + d1;
+}
+
+static uint32_t sym_voxel(uint32_t v, uint32_t m, uint32_t nx, uint32_t ny, uint32_t nz) {
+    /* symhandler.hpp transformVoxel */
+    uint32_t slice = nx * ny, z = v / slice, y = (v % slice) / nx, x = v % nx;
+    if (m & 1u) x = nx - 1 - x;
+    if (m & 2u) y = ny - 1 - y;
+    if (m & 4u) z = nz - 1 - z;
+    return z * slice + y * nx + x;
+}
+
+uint64_t oracle_expand_symmetries(uint32_t R, const uint64_t* row_end, const oracle_elem* e,
+                                  uint32_t sym, uint32_t n_layers, uint32_t n_blocks,
+                                  uint32_t block_size, uint32_t n_rings, uint32_t nx,
+                                  uint32_t ny, uint32_t nz, uint64_t* row_end_out,
+                                  oracle_elem* e_out) {
+    const uint32_t nc = block_size * n_blocks * n_layers * n_rings;
+    uint32_t mirrors[8], nm = 0;
+    for (uint32_t x = 0; x <= (sym & 1u); ++x) /* generateSyms, symhandler.hpp:37-51 */
+        for (uint32_t y = 0; y <= ((sym >> 1) & 1u); ++y)
+            for (uint32_t z = 0; z <= ((sym >> 2) & 1u); ++z)
+                if (x || y || z) mirrors[nm++] = x | (y << 1) | (z << 2);
+    uint64_t* len = (uint64_t*)calloc((size_t)R + 1, sizeof(uint64_t));
+    if (!len) return 0;
+    for (uint32_t r = 0; r < R; ++r) len[r] = row_end[r] - row_begin(row_end, r);
+    uint64_t* full = (uint64_t*)calloc((size_t)R + 1, sizeof(uint64_t));
+    if (!full) { free(len); return 0; }
+    for (uint32_t r = 0; r < R; ++r) full[r] += len[r];
+    for (uint32_t i = 0; i < nm; ++i)
+        for (uint32_t r = 0; r < R; ++r)
+            full[sym_lor(r, mirrors[i], nc, n_layers, n_blocks, block_size, n_rings)] += len[r];
+    uint64_t total = 0;
+    for (uint32_t r = 0; r < R; ++r) total += full[r];
+    if (row_end_out && e_out) {
+        uint64_t* cur = full; /* reused as the write cursor of each full row */
+        uint64_t acc = 0;
+        for (uint32_t r = 0; r < R; ++r) {
+            uint64_t n = cur[r];
+            cur[r] = acc;
+            acc += n;
+            row_end_out[r] = acc;
+        }
+        for (uint32_t r = 0; r < R; ++r)
+            for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k) e_out[cur[r]++] = e[k];
+        for (uint32_t i = 0; i < nm; ++i)
+            for (uint32_t r = 0; r < R; ++r) {
+                uint32_t t = sym_lor(r, mirrors[i], nc, n_layers, n_blocks, block_size, n_rings);
+                for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k) {
+                    oracle_elem q = e[k];
+                    q.index = sym_voxel(q.index, mirrors[i], nx, ny, nz);
+                    e_out[cur[t]++] = q;
+                }
+            }
+    }
+    free(len);
+    free(full);
+    return total;
+}
+
 int oracle_mlem_f64(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_elem* e,
                     const int32_t* sino, uint64_t S, int n_iter, double* image) {
     if (S != R) return -1;

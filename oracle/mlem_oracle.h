@@ -87,6 +87,24 @@ void oracle_subset_column_sums(uint32_t R, uint32_t C, const uint64_t* row_end,
                                const oracle_elem* e, uint32_t n_subsets, uint32_t s,
                                float* norm);
 
+/*
+ * The full matrix of a symmetry-compressed CSR4 matrix, as the reference's
+ * matrix viewer regenerates it (visualizematrix/dispcsr4spy.cpp:123-140 with
+ * symhandler.hpp/.cpp): for each mirror the flags allow (sym bits x = 1,
+ * y = 2, z = 4; generateSyms order, x outermost, identity excluded) and each
+ * stored row r, the elements of r with voxels mirrored (transformVoxel) go to
+ * row transformLor(r).  Full row t holds its stored elements first, then each
+ * mirror's contributions, source rows ascending.  Rows are LORs
+ * d1 * n_crystals + d2; columns voxels of the nx x ny x nz grid.  Returns the
+ * full element count; row_end_out (R) and e_out receive the matrix when
+ * non-NULL.
+ */
+uint64_t oracle_expand_symmetries(uint32_t R, const uint64_t* row_end, const oracle_elem* e,
+                                  uint32_t sym, uint32_t n_layers, uint32_t n_blocks,
+                                  uint32_t block_size, uint32_t n_rings, uint32_t nx,
+                                  uint32_t ny, uint32_t nz, uint64_t* row_end_out,
+                                  oracle_elem* e_out);
+
 /* FP64 oracle: the same iteration with double norm, projections, ratios and image. */
 int oracle_mlem_f64(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_elem* e,
                     const int32_t* sino, uint64_t S, int n_iter, double* image);

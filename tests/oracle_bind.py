@@ -44,6 +44,8 @@ def lib():
         L.oracle_osem.restype = i32
         L.oracle_osem.argtypes = [u32, u32, _vp, _vp, _vp, u64, i32, u32, i32, _vp, _vp, _vp]
         L.oracle_subset_column_sums.argtypes = [u32, u32, _vp, _vp, u32, u32, _vp]
+        L.oracle_expand_symmetries.restype = u64
+        L.oracle_expand_symmetries.argtypes = [u32, _vp, _vp] + [u32] * 8 + [_vp, _vp]
         L.oracle_mlem_f64.restype = i32
         L.oracle_mlem_f64.argtypes = [u32, u32, _vp, _vp, _vp, u64, i32, _vp]
         L.oracle_mlem_relaxed_f64.argtypes = [u32, u32, _vp, _vp, _vp, _vp, _vp, i32, _vp]
@@ -134,6 +136,20 @@ def osem(m, sino, n_iter, n_subsets, ftz=True, start_image=None):
     if rc != 0:
         raise ValueError(f"oracle_osem failed ({rc})")
     return img, sums[:n_iter]
+
+
+def expand_symmetries(m):
+    """The full matrix of a symmetry-compressed formats.Csr4 (flags, scanner, grid)."""
+    from mlem_b200 import formats
+    re, el = _mat(m)
+    nl, nb, bs, nr = m.scanner
+    nx, ny, nz = m.grid
+    args = (m.n_rows, _ptr(re), _ptr(el), int(m.flags) & 7, nl, nb, bs, nr, nx, ny, nz)
+    z = lib().oracle_expand_symmetries(*args, None, None)
+    out_re = np.zeros(m.n_rows, np.uint64)
+    out_el = np.zeros(z, formats.ELEM_DTYPE)
+    lib().oracle_expand_symmetries(*args, _ptr(out_re), _ptr(out_el))
+    return formats.Csr4(m.n_rows, m.n_cols, out_re, out_el, 0, tuple(m.grid))
 
 
 def subset_column_sums(m, n_subsets, s):
