@@ -50,6 +50,10 @@ def parse_args():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--mode", choices=["auto", "csc", "atomic", "fused", "region"], default="auto",
                     help="back-projection method; auto = autotuned")
+    ap.add_argument("--visit", choices=["file", "sorted", "chunked", "staged"], default="file",
+                    help="row visit with a fixed --mode (32 lanes per row, one-frame tile)")
+    ap.add_argument("--blocks-per-sm", type=int, default=8,
+                    help="resident blocks (chunked/staged: CTAs) per SM with a fixed --mode")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-osem", action="store_true")
     ap.add_argument("--no-skewed", action="store_true")
@@ -221,7 +225,10 @@ def run_ours(a, rank, world, local_rank):
     if a.mode == "auto":
         tuning = ctx.autotune()
     else:
-        ctx.set_tuning(bk_mode=mode_map[a.mode], group=32, frame_tile=1, blocks_per_sm=8)
+        visit = {"file": api.VISIT_FILE, "sorted": api.VISIT_SORTED,
+                 "chunked": api.VISIT_SORTED_CHUNKED, "staged": api.VISIT_SORTED_STAGED}[a.visit]
+        ctx.set_tuning(bk_mode=mode_map[a.mode], group=32, frame_tile=1,
+                       blocks_per_sm=a.blocks_per_sm, visit=visit)
         tuning = ctx.tuning()
     ctx.init_images()
     ctx.iterate(a.warmup, stats=False)
