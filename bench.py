@@ -57,6 +57,7 @@ def parse_args():
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-osem", action="store_true")
     ap.add_argument("--no-skewed", action="store_true")
+    ap.add_argument("--no-differentiable", action="store_true")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the uneven three-geometry batch (one GPU only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -389,6 +390,10 @@ def run_ours(a, rank, world, local_rank):
         }
         ctx.set_subsets(1)
 
+    # --- differentiable MLEM: 10 unrolled iterations, gradient of an MSE loss ---
+    if not a.no_differentiable:
+        line["differentiable"] = differentiable_line(ctx, a, stream, barrier)
+
     # --- a skewed matrix: the long rows run as segments (k_long.cu) ---
     if not a.no_skewed:
         line["skewed"] = skewed_line(a, stream, barrier)
@@ -408,6 +413,50 @@ def run_ours(a, rank, world, local_rank):
     if dist is not None:
         dist.destroy_process_group()
     return line
+
+
+def differentiable_line(ctx, a, stream, barrier):
+    """The plain-full matrix: K = 10 relaxed MLEM iterations from a uniform
+    start through torch_ext.unrolled_mlem, loss = mean squared error of the
+    last image against the phantom, gradients with respect to the start image
+    and the per-iteration exponents.  One step = forward + backward (the
+    backward recomputes each iteration's projections from the saved images)."""
+    import numpy as np
+    import torch
+
+    from mlem_b200 import synth, torch_ext
+
+    w = synth.WORKLOADS["differentiable"]
+    fr = synth.make_frames(w, ctx.project_f64)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    sino = torch.from_numpy(fr.sinograms[0]).to(dev)
+    x_true = torch.from_numpy(fr.phantoms[0].astype(np.float32)).to(dev)
+    norm = torch_ext.norm_tensor(ctx, dev)
+    init = float(sino.double().sum() / norm.double().sum())
+    K = 10
+
+    def step():
+        x0 = torch.full((ctx.n_cols,), init, dtype=torch.float32, device=dev, requires_grad=True)
+        omega = torch.ones(K, dtype=torch.float32, device=dev, requires_grad=True)
+        loss = torch.mean((torch_ext.unrolled_mlem(x0, omega, sino, ctx, norm) - x_true) ** 2)
+        loss.backward()
+        return loss, x0.grad, omega.grad
+
+    for _ in range(max(1, a.warmup)):
+        step()
+    n = 3
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    for _ in range(n):
+        loss, gx, gw = step()
+    e1.record(stream)
+    barrier()
+    ms = e0.elapsed_time(e1) / n
+    return {"workload": "differentiable", "unrolled_iterations": K, "ms_per_gradient_step": round(ms, 3),
+            "projections_per_step": 6 * K, "ms_per_projection": round(ms / (6 * K), 4),
+            "loss": float(loss.item()), "grad_x0_norm": float(gx.norm().item()),
+            "grad_omega": [round(float(v), 6) for v in gw.tolist()]}
 
 
 def skewed_line(a, stream, barrier):

@@ -137,9 +137,12 @@ class _UnrolledMLEM(torch.autograd.Function):
             dr = torch.where(pos, g * xk * omega[k] * rs ** (omega[k] - 1), torch.zeros_like(r))
             du = torch.where(norm != 0, dr / torch.where(norm != 0, norm, torch.ones_like(norm)), dr)
             dc = _fw(ctx, du)                                   # adjoint of A^T
-            fnz = f != 0
-            fs = torch.where(fnz, f, torch.ones_like(f))
-            df = torch.where(fnz, -dc * sino_f / (fs * fs), torch.zeros_like(f))
+            # c = s / f where f != 0: dc/df = -s / f^2.  A row with zero counts
+            # has c = 0 whatever f is (no gradient), and f^2 is never formed:
+            # for a tiny nonzero f it underflows to 0 (0 / 0 in a zero-count row)
+            live = (f != 0) & (sino_f != 0)
+            fs = torch.where(live, f, torch.ones_like(f))
+            df = torch.where(live, -(dc * (sino_f / fs)) / fs, torch.zeros_like(f))
             gx = gx + _bk(ctx, df)                              # adjoint of A
             g = gx
         return g, d_omega, None, None, None

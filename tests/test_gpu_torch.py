@@ -97,3 +97,23 @@ def test_unrolled_mlem_gradients_match_fp64_finite_differences(small):
         w_gpu.append(float(gw @ v))
     w_gpu, w_fd = np.array(w_gpu), np.array(w_fd)
     assert np.linalg.norm(w_gpu - w_fd) <= 1e-3 * np.linalg.norm(w_fd)
+
+
+def test_unrolled_mlem_gradients_finite_with_tiny_projections(small):
+    """Rows with zero counts whose projection is tiny but nonzero (a start
+    image of 1e-25: f^2 underflows to 0 in float32) give no gradient through
+    calcCorrel instead of 0 / 0."""
+    m, sino, ctx = small
+    rng = np.random.default_rng(4)
+    s = sino.copy()
+    s[rng.random(s.size) < 0.3] = 0
+    K = 3
+    xt = torch.full((m.n_cols,), 1e-25, device="cuda", dtype=torch.float32, requires_grad=True)
+    wt = torch.ones(K, device="cuda", dtype=torch.float32, requires_grad=True)
+    x_true = torch.tensor(synth.phantom(32, 32, 16, 5, 0), device="cuda", dtype=torch.float32)
+    xK = torch_ext.unrolled_mlem(xt, wt, torch.tensor(s, device="cuda"), ctx)
+    loss = torch.mean((xK - x_true) ** 2)
+    loss.backward()
+    assert torch.isfinite(xK).all()
+    assert torch.isfinite(xt.grad).all() and torch.isfinite(wt.grad).all()
+    assert float(wt.grad.abs().sum()) > 0
