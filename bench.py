@@ -362,6 +362,7 @@ def run_ours(a, rank, world, local_rank):
             "bk_mode": api.BK_NAMES[tb["bk_mode"]], "group": tb["group"],
             "frame_tile": tb["frame_tile"], "row_visit": api.VISIT_NAMES[tb["visit"]],
             "phases_ms": [round(float(x), 4) for x in bph_ms],
+            "parity": batched_parity(ctx, fb.sinograms, tb, 10),
         }
 
     # --- ordered subsets: 8 interleaved row subsets, the plain sinogram ---
@@ -501,6 +502,33 @@ def skewed_line(a, stream, barrier):
                 "gpu_launches_per_iteration": int(ctx.kernels_per_iteration())}
 
 
+def rel_l2(a, b):
+    import numpy as np
+    a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def batched_parity(ctx, sinograms, tuning, iters):
+    """Every frame of a batched reconstruction against its own single-frame
+    run (same tuning method and visit), after `iters` iterations."""
+    from mlem_b200 import api
+
+    ctx.set_sinograms(sinograms)
+    ctx.init_images()
+    ctx.iterate(iters, stats=False)
+    batch = ctx.get_images()
+    worst = 0.0
+    for b in range(sinograms.shape[0]):
+        ctx.set_sinograms(sinograms[b:b + 1])
+        ctx.set_tuning(bk_mode=tuning["bk_mode"], group=tuning["group"], frame_tile=1,
+                       blocks_per_sm=tuning["blocks_per_sm"], visit=tuning["visit"])
+        ctx.init_images()
+        ctx.iterate(iters, stats=False)
+        worst = max(worst, rel_l2(batch[b], ctx.get_images()[0]))
+    return {"iterations": iters, "max_rel_l2_frame_vs_single_run": worst, "tolerance": 1e-4,
+            "single_run_visit": api.VISIT_NAMES[tuning["visit"]]}
+
+
 def cpu_baseline_from_ctx(ctx, sino, g, iters):
     if not os.path.exists(REF_MESSUNG):
         return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
@@ -517,11 +545,21 @@ def cpu_baseline_from_ctx(ctx, sino, g, iters):
         threads = host_threads()
         secs, wall = run_reference_binary(mp, sp, iters, threads)
         per = statistics.mean(secs[1:]) if len(secs) > 1 else secs[0]
+        # the reference's image after these iterations against ours from the same inputs
+        import numpy as np
+
+        from mlem_b200 import api
+        ref_img = np.fromfile(os.path.join(d, "image.out"), dtype=np.float32)
+        ctx.set_sinograms(sino)
+        ctx.init_images()
+        ctx.iterate(iters, stats=False)
+        parity = {"iterations": iters, "rel_l2_vs_reference_image": rel_l2(ctx.get_images()[0], ref_img),
+                  "tolerance": 1e-4, "method": api.BK_NAMES[ctx.tuning()["bk_mode"]]}
         return {"value": round(1.0 / per, 4), "unit": UNIT, "cores": threads, "kind": "reference",
                 "sample": f"{iters} full iterations of openmpcsr4mlem (reference source, -O3 -fopenmp "
                           f"-DMESSUNG) on the same plain-full CSR4 file; mean of iterations 2..{iters}; "
                           f"wall {wall:.1f} s incl. load and serial column sums",
-                "iteration_seconds": secs}
+                "iteration_seconds": secs, "parity": parity}
     finally:
         shutil.rmtree(d, ignore_errors=True)
 
