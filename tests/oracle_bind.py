@@ -221,3 +221,25 @@ def rel_l2(a, b):
     b = np.asarray(b, np.float64)
     d = np.linalg.norm(b)
     return float(np.linalg.norm(a - b) / d) if d > 0 else float(np.linalg.norm(a - b))
+
+
+REF_CUDA_SO = os.path.join(REF_DIR, "libref_cuda.so")
+
+
+def ref_cuda_mlem(m, sino, n_iter, variant):
+    """The reference's own CUDA kernels (oracle/ref_cuda/harness.cu over
+    mlem_cuda/helper_files/cudaKernels.cu): (image float32[C], ms[6] per
+    iteration: clear, forward, correlation, back projection, update, all)."""
+    L = ctypes.CDLL(REF_CUDA_SO)
+    L.ref_cuda_mlem.restype = ctypes.c_int
+    L.ref_cuda_mlem.argtypes = [_vp, _vp, ctypes.c_uint32, ctypes.c_uint32, _vp, ctypes.c_int,
+                                ctypes.c_int, _vp, _vp]
+    re, el = _mat(m)
+    sino = np.ascontiguousarray(sino, np.int32)
+    img = np.zeros(m.n_cols, np.float32)
+    ms = np.zeros(6, np.float64)
+    rc = L.ref_cuda_mlem(_ptr(re), _ptr(el), m.n_rows, m.n_cols, _ptr(sino), n_iter, variant,
+                         _ptr(img), _ptr(ms))
+    if rc != 0:
+        raise RuntimeError(f"ref_cuda_mlem failed ({rc})")
+    return img, ms
