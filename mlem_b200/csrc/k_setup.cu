@@ -334,12 +334,6 @@ __global__ void k_remap_columns(uint2* __restrict__ el, uint64_t nnz,
         el[k].x = perm[el[k].x];
 }
 
-__global__ void k_fill(float* __restrict__ p, float v, uint64_t n) {
-    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
-         i += (uint64_t)gridDim.x * blockDim.x)
-        p[i] = v;
-}
-
 // ---------------------------------------------------------------------------
 // Synthetic Siddon generator (thread per row), bit-identical to the host build.
 // ---------------------------------------------------------------------------
@@ -581,12 +575,6 @@ cudaError_t permute_to_natural(const float* in, float* out, const uint32_t* perm
 cudaError_t remap_columns(uint2* elems, uint64_t nnz, const uint32_t* perm, cudaStream_t st) {
     if (nnz == 0) return cudaSuccess;
     k_remap_columns<<<elementwise_grid(nnz), 256, 0, st>>>(elems, nnz, perm);
-    return cudaGetLastError();
-}
-
-cudaError_t fill_f32(float* p, float v, uint64_t n, cudaStream_t st) {
-    if (n == 0) return cudaSuccess;
-    k_fill<<<elementwise_grid(n), 256, 0, st>>>(p, v, n);
     return cudaGetLastError();
 }
 

@@ -167,7 +167,6 @@ cudaError_t permute_to_natural(const float* in, float* out, const uint32_t* perm
                                uint32_t B, cudaStream_t st);
 // Relabel the column (voxel) index of every element: e.x = perm[e.x].
 cudaError_t remap_columns(uint2* elems, uint64_t nnz, const uint32_t* perm, cudaStream_t st);
-cudaError_t fill_f32(float* p, float v, uint64_t n, cudaStream_t st);
 // x[i][b] = b < B ? vals[b] : 0 for the Bp-interleaved image (vals: device, B floats).
 cudaError_t fill_frames(float* x, uint64_t n, uint32_t Bp, uint32_t B, const float* vals,
                         cudaStream_t st);
