@@ -266,6 +266,15 @@ int mlem_bkproj_d(mlem_ctx* ctx, const float* y, float* x, uint32_t n_frames, vo
 /* correl[R][B] = calcCorrel(sino[R][B], A x[C][B])  (fused). */
 int mlem_fwproj_correl_d(mlem_ctx* ctx, const float* x, const int32_t* sino, float* correl,
                          uint32_t n_frames, void* stream);
+/* update[C][B] = A^T calcCorrel(sino[R][B], A x[C][B]) in one pass over the
+ * matrix (the one-pass kernels, with the context's row visit when it is tuned
+ * to MLEM_BK_FUSED, else sorted rows in chunks): the partial update of a row
+ * shard (mlem_mpi/fusedmpimlem.cpp:205-225) or the numerator of calcUpdate.
+ * Summation order varies from run to run (float atomics).  Not in the
+ * bit-exact mode; must not run concurrently with the context's own
+ * iterations. */
+int mlem_fused_update_d(mlem_ctx* ctx, const float* x, const int32_t* sino, float* update,
+                        uint32_t n_frames, void* stream);
 /* x[C][B] *= calcUpdate factor(A^T correl[R][B], norm)  (fused, CSC). */
 int mlem_bkproj_update_d(mlem_ctx* ctx, const float* correl, float* x, uint32_t n_frames,
                          void* stream);

@@ -361,6 +361,11 @@ class Context:
         self._chk(core_lib().mlem_fwproj_correl_d(self._h, x_ptr, sino_ptr, correl_ptr, n_frames,
                                                   stream))
 
+    def fused_update_d(self, x_ptr, sino_ptr, update_ptr, n_frames=1, stream=0) -> None:
+        """update = A^T calcCorrel(sino, A x) in one pass over the matrix."""
+        self._chk(core_lib().mlem_fused_update_d(self._h, x_ptr, sino_ptr, update_ptr, n_frames,
+                                                 stream))
+
     def bkproj_update_d(self, correl_ptr, x_ptr, n_frames=1, stream=0) -> None:
         self._chk(core_lib().mlem_bkproj_update_d(self._h, correl_ptr, x_ptr, n_frames, stream))
 

@@ -64,6 +64,8 @@ struct mlem_ctx {
     LongSeg* long_segs = nullptr;
     uint32_t n_long_segs = 0, n_long = 0;
     float* f_long = nullptr;
+    float* f_long_d = nullptr;  // the same for mlem_fused_update_d (any frame count)
+    size_t f_long_d_floats = 0;
 
     // Ordered subsets (mlem_set_subsets): row r in subset r % n_subsets.
     // sub_norm[s * C ...]: subset column sums (device voxel order); the visiting
@@ -601,22 +603,26 @@ SparseView subset_view(const mlem_ctx* c, const mlem_tuning& t, uint32_t s) {
     return v;
 }
 
-// One-pass method over the rows of `csr` (all rows, or one subset's).
-int fused_pass(mlem_ctx* c, const mlem_tuning& t, const SparseView& csr, cudaStream_t st) {
-    const uint32_t Bp = c->Bp;
+// One-pass method over the rows of `csr` (all rows, or one subset's): u +=
+// A^T calcCorrel(sino, A x) for B interleaved frames.  `counter` is the work
+// counter of the chunked and staged walks.
+int fused_pass(mlem_ctx* c, const mlem_tuning& t, const SparseView& csr, const float* x,
+               const int32_t* sino, float* u, uint32_t B, unsigned int* counter,
+               cudaStream_t st) {
     const uint32_t T = (uint32_t)t.frame_tile;
     if (t.visit == MLEM_VISIT_SORTED_STAGED)
-        CK(c, fused_staged(csr, c->x, Bp, t.frame_tile, c->sino, c->update,
-                           chunk_rows_of(c, t, csr.n), staged_ctas_per_sm(t), c->counter,
-                           c->n_sm, st));
+        CK(c, fused_staged(csr, x, B, t.frame_tile, sino, u, chunk_rows_of(c, t, csr.n),
+                           staged_ctas_per_sm(t), counter, c->n_sm, st));
     else if (t.visit == MLEM_VISIT_SORTED_CHUNKED)
-        CK(c, fused_chunked(csr, c->x, Bp, t.frame_tile, c->sino, c->update,
-                            chunk_rows_of(c, t, csr.n), chunk_ctas_per_sm(t), c->counter,
-                            c->n_sm, st));
+        CK(c, fused_chunked(csr, x, B, t.frame_tile, sino, u, chunk_rows_of(c, t, csr.n),
+                            chunk_ctas_per_sm(t), counter, c->n_sm, st));
     else
-        for (uint32_t f0 = 0; f0 < Bp; f0 += T)
-            CK(c, fused_row(csr, c->x, Bp, f0, c->sino, c->update, cfg_of(c, t), st));
+        for (uint32_t f0 = 0; f0 < B; f0 += T)
+            CK(c, fused_row(csr, x, B, f0, sino, u, cfg_of(c, t), st));
     return MLEM_OK;
+}
+int fused_pass(mlem_ctx* c, const mlem_tuning& t, const SparseView& csr, cudaStream_t st) {
+    return fused_pass(c, t, csr, c->x, c->sino, c->update, c->Bp, c->counter, st);
 }
 
 int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
@@ -1085,7 +1091,8 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->tmp_r[1], (void*)c->tmp_c[0], (void*)c->tmp_c[1], (void*)c->tmp_c[2],
                     (void*)c->tmp_sino, (void*)c->tmp_d, (void*)c->norm_nat, (void*)c->perm,
                     (void*)c->pscratch[0], (void*)c->pscratch[1], (void*)c->row_order,
-                    (void*)c->row_ranges, (void*)c->counter, (void*)c->long_segs, (void*)c->sub_norm,
+                    (void*)c->row_ranges, (void*)c->counter, (void*)c->long_segs, (void*)c->f_long_d,
+                    (void*)c->sub_norm,
                     (void*)c->sub_file, (void*)c->sub_file_ranges, (void*)c->sub_sorted,
                     (void*)c->sub_sorted_ranges})
         dev_free(p);
@@ -1695,6 +1702,51 @@ int mlem_fwproj_correl_d(mlem_ctx* c, const float* x, const int32_t* sino, float
     const LaunchCfg cfg = cfg_for_frames(c, B);
     for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
         CK(c, fwproj(csr_visit(c, c->tuning), xd, B, f0, sino, correl, nullptr, cfg, st));
+    return MLEM_OK;
+}
+
+int mlem_fused_update_d(mlem_ctx* c, const float* x, const int32_t* sino, float* u, uint32_t B,
+                        void* stream) {
+    if (!c || !x || !sino || !u || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
+    if (c->flags & MLEM_FLAG_EXACT)
+        return fail(c, MLEM_ERR_STATE, "the one-pass method does not run in the bit-exact mode");
+    TRY(set_device(c));
+    cudaStream_t st = (cudaStream_t)stream;
+    // the context's one-pass tuning when it has one, else sorted rows in chunks
+    mlem_tuning t = c->tuning;
+    if (t.bk_mode != MLEM_BK_FUSED) {
+        t.visit = c->row_order ? MLEM_VISIT_SORTED_CHUNKED : MLEM_VISIT_FILE;
+        t.blocks_per_sm = c->row_order ? 4 : 8;
+        t.group = 32;
+    }
+    t.bk_mode = MLEM_BK_FUSED;
+    t.frame_tile = cfg_for_frames(c, B).frame_tile;
+    if (chunk_visit(t.visit)) t.group = 32;
+    const float* xd = x;
+    float* ud = u;
+    if (c->bricked) {
+        TRY(perm_scratch(c, (size_t)c->C * B));
+        CK(c, permute_to_device(x, c->pscratch[0], c->perm, c->C, B, st));
+        xd = c->pscratch[0];
+        ud = c->pscratch[1];
+    }
+    if (c->n_long && c->f_long_d_floats < (size_t)c->n_long * B) {
+        dev_free(c->f_long_d);
+        c->f_long_d = nullptr;
+        c->f_long_d_floats = 0;
+        TRY(dev_alloc(c, &c->f_long_d, (size_t)c->n_long * B));
+        c->f_long_d_floats = (size_t)c->n_long * B;
+    }
+    CK(c, cudaMemsetAsync(ud, 0, (size_t)c->C * B * 4, st));
+    SparseView v = csr_visit(c, t);
+    if (c->n_long) v.long_len = kLongRowElems;
+    // a counter of its own (a cache sector from the iteration's), so that this
+    // call and the context's graph never share one
+    TRY(fused_pass(c, t, v, xd, sino, ud, B, c->counter + 8, st));
+    if (c->n_long)
+        CK(c, long_rows_pass(csr_view(c), c->long_segs, c->n_long_segs, c->n_long, xd, B,
+                             t.frame_tile, sino, c->f_long_d, ud, c->n_sm, st));
+    if (c->bricked) CK(c, permute_to_natural(ud, u, c->perm, c->C, B, st));
     return MLEM_OK;
 }
 

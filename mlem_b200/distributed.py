@@ -57,6 +57,7 @@ class Shard(Protocol):
     def local_count_sum(self) -> float: ...    # double sum of the block's sinogram
     def project_correl(self, x): ...           # correlation of the block's rows
     def backproject(self, correl): ...         # partial update, float32[C]
+    # optional: partial_update(x) = backproject(project_correl(x)) in one step
     def apply(self, update, x) -> None: ...    # x *= calcUpdate factor(update, norm)
     def fill(self, value: float): ...          # new image filled with value
     def to_host(self, x) -> np.ndarray: ...
@@ -83,9 +84,12 @@ def reconstruct(shard: Shard, n_iter: int, dist, group=None, start_image=None):
     else:
         x = shard.fill(0.0)
         x.copy_(torch.as_tensor(np.asarray(start_image, np.float32)).to(x.device))
+    one_step = getattr(shard, "partial_update", None)
     for _ in range(n_iter):
-        correl = shard.project_correl(x)
-        update = shard.backproject(correl)
+        if one_step is not None:
+            update = one_step(x)  # fusedmpimlem.cpp:205-225 in one pass over the block
+        else:
+            update = shard.backproject(shard.project_correl(x))
         dist.all_reduce(update, op=dist.ReduceOp.SUM, group=group)  # fusedmpimlem.cpp:227
         shard.apply(update, x)
     return shard.to_host(x)
@@ -131,6 +135,16 @@ class CudaShard:
     def backproject(self, correl):
         if self.n_rows:
             self.ctx.bkproj_d(correl.data_ptr(), self.update.data_ptr(), 1, self.stream.cuda_stream)
+        else:
+            self.update.zero_()
+        return self.update
+
+    def partial_update(self, x):
+        """The block's partial update A_b^T calcCorrel(s_b, A_b x) in one pass
+        over its rows (the one-pass kernels)."""
+        if self.n_rows:
+            self.ctx.fused_update_d(x.data_ptr(), self.sino.data_ptr(), self.update.data_ptr(), 1,
+                                    self.stream.cuda_stream)
         else:
             self.update.zero_()
         return self.update

@@ -95,26 +95,26 @@ def norm_tensor(ctx: "api.Context", device) -> torch.Tensor:
     return torch.from_numpy(ctx.column_sums()).to(device)
 
 
-def _ratio(ctx, x, sino_f, norm):
-    """(f, u, r): f = A x, u = A^T (s / f), r = calcUpdate factor(u, norm)."""
-    f = _fw(ctx, x)
-    c = torch.where(f != 0, sino_f / torch.where(f != 0, f, torch.ones_like(f)), torch.zeros_like(f))
-    u = _bk(ctx, c)
-    r = torch.where(norm != 0, u / torch.where(norm != 0, norm, torch.ones_like(norm)), u)
-    return f, u, r
+def _fused_ratio(ctx, x, sino_i, norm):
+    """calcUpdate factor of A^T (s / A x) from the one-pass kernels (one pass
+    over the matrix instead of a forward and a back projection)."""
+    u = torch.empty_like(x)
+    ctx.fused_update_d(x.data_ptr(), sino_i.data_ptr(), u.data_ptr(), 1, _stream())
+    return torch.where(norm != 0, u / torch.where(norm != 0, norm, torch.ones_like(norm)), u)
 
 
 class _UnrolledMLEM(torch.autograd.Function):
     @staticmethod
-    def forward(fctx, x0, omega, sino_f, norm, ctx):
+    def forward(fctx, x0, omega, sino_f, norm, ctx, sino_i):
         K = omega.shape[0]
         xs = [x0.detach()]
-        x = x0.detach()
+        x = x0.detach().contiguous()
         for k in range(K):
-            _, _, r = _ratio(ctx, x, sino_f, norm)
+            r = _fused_ratio(ctx, x, sino_i, norm)
             x = x * torch.where(r > 0, r.clamp_min(1e-38) ** omega[k], torch.zeros_like(r))
             xs.append(x)
         fctx.mctx = ctx
+        fctx.sino_i = sino_i
         fctx.save_for_backward(torch.stack(xs[:-1]), omega, sino_f, norm, x)
         return x
 
@@ -126,8 +126,9 @@ class _UnrolledMLEM(torch.autograd.Function):
         g = g.contiguous()
         d_omega = torch.zeros_like(omega)
         for k in range(K - 1, -1, -1):
-            xk = xs[k]
-            f, u, r = _ratio(ctx, xk, sino_f, norm)           # recompute from the checkpoint
+            xk = xs[k].contiguous()
+            f = _fw(ctx, xk)                                    # recompute from the checkpoint
+            r = _fused_ratio(ctx, xk, fctx.sino_i, norm)
             pos = r > 0
             rs = torch.where(pos, r, torch.ones_like(r))
             p = torch.where(pos, rs ** omega[k], torch.zeros_like(r))  # r^w
@@ -145,7 +146,7 @@ class _UnrolledMLEM(torch.autograd.Function):
             df = torch.where(live, -(dc * (sino_f / fs)) / fs, torch.zeros_like(f))
             gx = gx + _bk(ctx, df)                              # adjoint of A
             g = gx
-        return g, d_omega, None, None, None
+        return g, d_omega, None, None, None, None
 
 
 def unrolled_mlem(x0: torch.Tensor, omega: torch.Tensor, sino: torch.Tensor,
@@ -154,5 +155,7 @@ def unrolled_mlem(x0: torch.Tensor, omega: torch.Tensor, sino: torch.Tensor,
     _check(x0, ctx.n_cols, "x0")
     if norm is None:
         norm = norm_tensor(ctx, x0.device)
-    sino_f = sino.to(device=x0.device, dtype=torch.float32)
-    return _UnrolledMLEM.apply(x0, omega.to(device=x0.device, dtype=torch.float32), sino_f, norm, ctx)
+    sino_i = sino.to(device=x0.device, dtype=torch.int32).contiguous()
+    sino_f = sino_i.to(torch.float32)
+    return _UnrolledMLEM.apply(x0, omega.to(device=x0.device, dtype=torch.float32), sino_f, norm,
+                               ctx, sino_i)

@@ -47,8 +47,10 @@ def test_two_row_blocks_sum_to_the_whole_matrix(golden):
             sumnorm += v
         init = float(np.float32(sumin / sumnorm))
         xs = [s.fill(init) for s in shards]
-        for _ in range(iters):
-            updates = [s.backproject(s.project_correl(x)).clone() for s, x in zip(shards, xs)]
+        for it in range(iters):
+            # both ways a shard computes its partial update: two passes, or one
+            updates = [(s.backproject(s.project_correl(x)) if it % 2 else s.partial_update(x)).clone()
+                       for s, x in zip(shards, xs)]
             total = updates[0] + updates[1]  # what the all-reduce delivers to every rank
             for s, x in zip(shards, xs):
                 s.apply(total, x)

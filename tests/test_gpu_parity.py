@@ -365,3 +365,36 @@ def test_device_pointer_api_in_natural_order(small_ctx=None):
     assert res[0] == res[1]
     want = ob.fwproj(hm, x.cpu().numpy())
     assert ob.rel_l2(np.frombuffer(res[0][0], np.float32), want) < TOL_PROJ
+
+
+@pytest.mark.parametrize("flags", [0, api.FLAG_NATURAL_LAYOUT])
+@pytest.mark.parametrize("frames", [1, 3])
+@pytest.mark.parametrize("long_row", [False, True])
+def test_fused_update_d_matches_two_step(golden, flags, frames, long_row):
+    """mlem_fused_update_d (one pass) equals mlem_fwproj_correl_d followed by
+    mlem_bkproj_d (two passes) within float rounding, in both voxel layouts,
+    with several frames and with a row above the long-row limit."""
+    torch = pytest.importorskip("torch")
+    g = synth.Geometry(16, 16, 8, 3000, 5, 40, seed=7)
+    hm = synth.host_matrix(g)
+    if long_row:  # append one row of 6000 elements
+        rng = np.random.default_rng(2)
+        extra = np.zeros(6000, api.ELEM_DTYPE)
+        extra["index"] = rng.integers(0, hm.n_cols, 6000)
+        extra["value"] = rng.uniform(0.1, 1.5, 6000).astype(np.float32)
+        row_end = np.concatenate([hm.row_end, [hm.row_end[-1] + 6000]]).astype(np.uint64)
+        hm = formats.Csr4(hm.n_rows + 1, hm.n_cols, row_end, np.concatenate([hm.elems, extra]),
+                          0, hm.grid)
+    rng = np.random.default_rng(3)
+    x = torch.rand(hm.n_cols * frames, device="cuda") + 0.1
+    s = torch.tensor(rng.poisson(5, hm.n_rows * frames).astype(np.int32), device="cuda")
+    with api.Context.from_matrix(hm, flags=flags) as ctx:
+        st = torch.cuda.current_stream().cuda_stream
+        c = torch.empty(hm.n_rows * frames, device="cuda")
+        u2 = torch.empty_like(x)
+        ctx.fwproj_correl_d(x.data_ptr(), s.data_ptr(), c.data_ptr(), frames, st)
+        ctx.bkproj_d(c.data_ptr(), u2.data_ptr(), frames, st)
+        u1 = torch.full_like(x, 7.0)  # overwritten, not accumulated into
+        ctx.fused_update_d(x.data_ptr(), s.data_ptr(), u1.data_ptr(), frames, st)
+        torch.cuda.synchronize()
+        assert ob.rel_l2(u1.cpu().numpy(), u2.cpu().numpy()) <= 1e-5
