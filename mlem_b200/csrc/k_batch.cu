@@ -132,7 +132,7 @@ __global__ void __launch_bounds__(1024, 1) k_fused_chunked(SparseView csr,
                                                                      unsigned int* __restrict__ counter) {
     __shared__ uint32_t s_chunk;
     const uint64_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const uint64_t nchunks = (csr.n + chunk - 1) / chunk;
+    const uint64_t nchunks = ((uint64_t)csr.n + chunk - 1) / chunk;
     for (;;) {
         if (threadIdx.x == 0) s_chunk = atomicAdd(counter, 1u);
         __syncthreads();
@@ -152,7 +152,7 @@ cudaError_t fused_chunked(const SparseView& csr, const float* x, uint32_t B, int
                           const int32_t* sino, float* u, uint32_t chunk_rows, int ctas_per_sm,
                           unsigned int* counter, int sm_count, cudaStream_t st) {
     if (csr.n == 0) return cudaSuccess;
-    if (chunk_rows == 0 || (uint64_t)(csr.n + chunk_rows - 1) / chunk_rows > 0xffffffffull)
+    if (chunk_rows == 0 || ((uint64_t)csr.n + chunk_rows - 1) / chunk_rows > 0xffffffffull)
         return cudaErrorInvalidValue;
     if (ctas_per_sm != 1 && ctas_per_sm != 2 && ctas_per_sm != 4) return cudaErrorInvalidValue;
     if (!csr.order || !csr.vrange) return cudaErrorInvalidValue;  // a sorted visit

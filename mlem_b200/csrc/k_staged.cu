@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(kStagedThreads, 4) k_fused_staged(SparseView c
     const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const uint2* stages = reinterpret_cast<const uint2*>(s_stage) + (size_t)warp * kStages * kStageCap;
     const uint32_t sa = (uint32_t)__cvta_generic_to_shared(stages);
-    const uint64_t nchunks = (csr.n + chunk - 1) / chunk;
+    const uint64_t nchunks = ((uint64_t)csr.n + chunk - 1) / chunk;
     for (;;) {
         if (threadIdx.x == 0) s_chunk = atomicAdd(counter, 1u);
         __syncthreads();
@@ -70,7 +70,7 @@ cudaError_t fused_staged(const SparseView& csr, const float* x, uint32_t B, int 
                          const int32_t* sino, float* u, uint32_t chunk_rows, int ctas_per_sm,
                          unsigned int* counter, int sm_count, cudaStream_t st) {
     if (csr.n == 0) return cudaSuccess;
-    if (chunk_rows == 0 || (uint64_t)(csr.n + chunk_rows - 1) / chunk_rows > 0xffffffffull)
+    if (chunk_rows == 0 || ((uint64_t)csr.n + chunk_rows - 1) / chunk_rows > 0xffffffffull)
         return cudaErrorInvalidValue;
     if (ctas_per_sm < 1 || ctas_per_sm > 4) return cudaErrorInvalidValue;
     if (!csr.order || !csr.vrange) return cudaErrorInvalidValue;  // a sorted visit
