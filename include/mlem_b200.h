@@ -358,7 +358,8 @@ const char* mlem_batch_last_error(const mlem_batch* b);
  * MLEM_VISIT_SORTED for every matrix, or MLEM_VISIT_SORTED_STAGED with the
  * items schedule (sorted needs every context's row order; with the items
  * schedule a sorted item is a run of neighbouring rows; staged pipelines each
- * warp's rows of an item through shared memory, at most 4 blocks per SM). */
+ * warp's rows of an item through shared memory, at most 4 blocks per SM).
+ * Every context takes the batch's visit again (see mlem_batch_set_visits). */
 int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
                             int blocks_per_sm, int frame_tile, int visit);
 /* A frame tile for each context (n_ctx entries): 0 follows the batch's tile,
@@ -369,13 +370,22 @@ int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
 int mlem_batch_set_tiles(mlem_batch* b, const int* tiles);
 /* The frame tile each context runs with (n_ctx entries). */
 int mlem_batch_get_tiles(const mlem_batch* b, int* tiles);
+/* A row visit for each context (n_ctx entries): -1 follows the batch's visit,
+ * else MLEM_VISIT_FILE, MLEM_VISIT_SORTED or, with the items schedule,
+ * MLEM_VISIT_SORTED_STAGED (the sorted visits need the context's row order).
+ * The contexts that share a frame tile and a visit share one kernel per
+ * iteration. */
+int mlem_batch_set_visits(mlem_batch* b, const int* visits);
+/* The row visit each context runs with (n_ctx entries). */
+int mlem_batch_get_visits(const mlem_batch* b, int* visits);
 /* Current schedule; any pointer may be NULL.  n_items: 0 for the interleaved
  * schedule.  ms_per_iter: from the last autotune, else 0. */
 int mlem_batch_get_schedule(const mlem_batch* b, int* policy, uint32_t* items_per_block,
                             int* blocks_per_sm, int* frame_tile, int* visit, uint32_t* n_items,
                             double* ms_per_iter);
-/* Time real iterations over schedules, frame tiles and resident blocks and
- * keep the fastest; the images are restored afterwards. */
+/* Time real iterations over schedules, frame tiles, row visits and resident
+ * blocks, then a tile and a visit per context, and keep the fastest; the
+ * images are restored afterwards. */
 int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter);
 /* n iterations of every context.  sums may be NULL, or hold n_ctx pointers
  * (each NULL or n x n_frames doubles, iteration-major) for the image sums. */

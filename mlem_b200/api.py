@@ -440,6 +440,21 @@ class Batch:
         self._chk(core_lib().mlem_batch_get_tiles(self._h, arr))
         return list(arr)
 
+    def set_visits(self, visits) -> None:
+        """A row visit per context (-1: the batch's visit); contexts sharing a
+        frame tile and a visit share one kernel per iteration."""
+        visits = [int(v) for v in visits]
+        if len(visits) != len(self.contexts):
+            raise MlemError(MLEM_ERR_INVALID, "one row visit per context")
+        arr = (ctypes.c_int * len(visits))(*visits)
+        self._chk(core_lib().mlem_batch_set_visits(self._h, arr))
+
+    def visits(self) -> list:
+        """The row visit each context runs with."""
+        arr = (ctypes.c_int * len(self.contexts))()
+        self._chk(core_lib().mlem_batch_get_visits(self._h, arr))
+        return list(arr)
+
     def schedule(self) -> dict:
         pol, ipb, bps = ctypes.c_int(), ctypes.c_uint32(), ctypes.c_int()
         tile, visit, n, ms = ctypes.c_int(), ctypes.c_int(), ctypes.c_uint32(), ctypes.c_double()
@@ -449,7 +464,7 @@ class Batch:
                                                      ctypes.byref(ms)))
         return dict(policy=pol.value, items_per_block=ipb.value, blocks_per_sm=bps.value,
                     frame_tile=tile.value, visit=visit.value, n_items=n.value,
-                    ms_per_iter=ms.value, tiles=self.tiles())
+                    ms_per_iter=ms.value, tiles=self.tiles(), visits=self.visits())
 
     def autotune(self) -> dict:
         ms = ctypes.c_double()

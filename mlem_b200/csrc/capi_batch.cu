@@ -32,16 +32,19 @@ struct mlem_batch {
     int visit = MLEM_VISIT_FILE;
     int tile = 0;  // frames per pass of every context without a tile of its own
     std::vector<int> tiles;  // per context: 0 = the batch tile, else its own frame tile
+    std::vector<int> visits;  // per context: -1 = the batch visit, else its own row visit
     uint32_t items_per_block = 4;
     int blocks_per_sm = 4;  // k_batch_fused is bounded to 64 registers: 4 x 256 threads per SM
     double ms_per_iter = 0.0;
 
-    // The contexts that share a frame tile form a group: one kernel per group
-    // and iteration, heaviest group first.  A group's table is the kernels'
-    // parameter; its items are b->items[item0, item0 + n_items), with `mat`
-    // indexing the group's table; ctx_of maps the table back to contexts.
+    // The contexts that share a frame tile and a row visit form a group: one
+    // kernel per group and iteration, heaviest group first.  A group's table
+    // is the kernels' parameter; its items are b->items[item0, item0 +
+    // n_items), with `mat` indexing the group's table; ctx_of maps the table
+    // back to contexts.
     struct Group {
         int tile = 1;
+        int visit = MLEM_VISIT_FILE;
         double cost = 0.0;
         BatchTable table{};
         std::vector<size_t> ctx_of;
@@ -116,9 +119,13 @@ int batch_default_tile(const mlem_batch* b) {
 }
 
 int eff_tile(const mlem_batch* b, size_t i) { return b->tiles[i] ? b->tiles[i] : b->tile; }
+int eff_visit(const mlem_batch* b, size_t i) { return b->visits[i] >= 0 ? b->visits[i] : b->visit; }
 
-// Per-group counters sit a cache sector apart (the counter buffer holds 64 uints).
+// Per-group counters sit a cache sector apart.  Groups are distinct (tile,
+// visit) pairs: at most 5 tiles x 3 visits.
 constexpr uint32_t kCounterStride = 8;
+constexpr uint32_t kMaxGroups = 16;
+static_assert(5 * 3 <= kMaxGroups, "one counter per (frame tile, row visit) group");
 
 // Cost of rows [r0, r1) of context i: element bytes once per frame-tile
 // pass, one gather and one scatter of 4 bytes per element and frame, and the
@@ -126,24 +133,26 @@ constexpr uint32_t kCounterStride = 8;
 double item_cost(const mlem_batch* b, size_t i, uint32_t r0, uint32_t r1) {
     const mlem_ctx* c = b->ctx[i];
     const std::vector<uint64_t>& pre =
-        (b->visit != MLEM_VISIT_FILE && !b->pre_sorted[i].empty()) ? b->pre_sorted[i] : b->pre_file[i];
+        (eff_visit(b, i) != MLEM_VISIT_FILE && !b->pre_sorted[i].empty()) ? b->pre_sorted[i] : b->pre_file[i];
     const double nnz = (double)(pre[r1] - pre[r0]);
     const double passes = (double)(c->Bp / (uint32_t)eff_tile(b, i));
     return nnz * (8.0 * passes + 8.0 * c->Bp) + (double)(r1 - r0) * (16.0 + 8.0 * c->Bp);
 }
 
-// Group the contexts by frame tile (heaviest group first) with each group's
+// Group the contexts by frame tile and row visit (heaviest group first) with each group's
 // table taken from b->table.  Returns true when the grouping differs from
 // the current one (the items must then be cut again); the item ranges of an
 // unchanged grouping are kept.
 bool build_groups(mlem_batch* b) {
     std::vector<mlem_batch::Group> gs;
     for (size_t i = 0; i < b->ctx.size(); ++i) {
-        const int t = eff_tile(b, i);
-        auto it = std::find_if(gs.begin(), gs.end(), [&](const mlem_batch::Group& g) { return g.tile == t; });
+        const int t = eff_tile(b, i), v = eff_visit(b, i);
+        auto it = std::find_if(gs.begin(), gs.end(),
+                               [&](const mlem_batch::Group& g) { return g.tile == t && g.visit == v; });
         if (it == gs.end()) {
             gs.emplace_back();
             gs.back().tile = t;
+            gs.back().visit = v;
             gs.back().table.n = 0;
             gs.back().table.row_base[0] = 0;
             it = gs.end() - 1;
@@ -160,7 +169,8 @@ bool build_groups(mlem_batch* b) {
     });
     bool same = gs.size() == b->groups.size();
     for (size_t g = 0; same && g < gs.size(); ++g)
-        same = gs[g].tile == b->groups[g].tile && gs[g].ctx_of == b->groups[g].ctx_of;
+        same = gs[g].tile == b->groups[g].tile && gs[g].visit == b->groups[g].visit &&
+               gs[g].ctx_of == b->groups[g].ctx_of;
     if (same)
         for (size_t g = 0; g < gs.size(); ++g) {
             gs[g].item0 = b->groups[g].item0;
@@ -256,7 +266,7 @@ int batch_refresh(mlem_batch* b, int chunk) {
         TRY(bctx(b, c, ensure_history(c, chunk)));
         if (t.mats[i].Bp != c->Bp) reschedule = true;
         SparseView v = csr_view(c);
-        if (b->visit == MLEM_VISIT_FILE) {
+        if (eff_visit(b, i) == MLEM_VISIT_FILE) {
             v.order = nullptr;
             v.vrange = nullptr;
         }
@@ -302,14 +312,14 @@ int batch_enqueue(mlem_batch* b, bool stats, const PhaseEvents* pe = nullptr) {
         const mlem_batch::Group& g = b->groups[gi];
         unsigned int* counter = b->counter + gi * kCounterStride;
         const BatchItem* items = b->items_d + g.item0;
-        if (b->policy == MLEM_BATCH_ITEMS && b->visit == MLEM_VISIT_SORTED_STAGED)
+        if (b->policy == MLEM_BATCH_ITEMS && g.visit == MLEM_VISIT_SORTED_STAGED)
             BCK(b, batch_staged(g.table, items, g.n_items, counter, g.tile, b->n_sm,
                                 b->blocks_per_sm, st));
         else if (b->policy == MLEM_BATCH_ITEMS)
             BCK(b, batch_fused(g.table, items, g.n_items, counter, g.tile,
-                               b->visit == MLEM_VISIT_SORTED, b->n_sm, b->blocks_per_sm, st));
+                               g.visit == MLEM_VISIT_SORTED, b->n_sm, b->blocks_per_sm, st));
         else
-            BCK(b, batch_interleaved(g.table, g.tile, b->visit == MLEM_VISIT_SORTED, b->n_sm,
+            BCK(b, batch_interleaved(g.table, g.tile, g.visit == MLEM_VISIT_SORTED, b->n_sm,
                                      b->blocks_per_sm, st));
     }
     TRY(bmark(b, pe, 1));
@@ -402,6 +412,7 @@ int mlem_batch_create(mlem_batch** out, mlem_ctx* const* ctxs, uint32_t n_ctx) {
     mlem_batch* b = new mlem_batch();
     b->ctx.assign(ctxs, ctxs + n_ctx);
     b->tiles.assign(n_ctx, 0);
+    b->visits.assign(n_ctx, -1);
     b->device = ctxs[0]->device;
     b->n_sm = ctxs[0]->n_sm;
     b->stream = ctxs[0]->stream;
@@ -436,7 +447,7 @@ int mlem_batch_create(mlem_batch** out, mlem_ctx* const* ctxs, uint32_t n_ctx) {
             for (uint32_t k = 0; k < c->R; ++k) ps[k + 1] = ps[k] + (pre[order[k] + 1] - pre[order[k]]);
         }
     }
-    if (cudaMalloc(&b->counter, 256) != cudaSuccess) {
+    if (cudaMalloc(&b->counter, kMaxGroups * kCounterStride * sizeof(unsigned int)) != cudaSuccess) {
         cudaGetLastError();
         return bail(bfail(b, MLEM_ERR_NOMEM, "batch descriptors: cudaMalloc failed"));
     }
@@ -478,6 +489,7 @@ int mlem_batch_set_schedule(mlem_batch* b, int policy, uint32_t items_per_block,
     BCK(b, cudaSetDevice(b->device));
     b->policy = policy;
     b->visit = visit;
+    std::fill(b->visits.begin(), b->visits.end(), -1);  // one visit for every context again
     b->items_per_block = items_per_block;
     b->blocks_per_sm = blocks_per_sm;
     if (frame_tile != 0) {  // one tile for every context again
@@ -526,6 +538,32 @@ int mlem_batch_set_tiles(mlem_batch* b, const int* tiles) {
 int mlem_batch_get_tiles(const mlem_batch* b, int* tiles) {
     if (!b || !tiles) return bfail(const_cast<mlem_batch*>(b), MLEM_ERR_INVALID, "null argument");
     for (size_t i = 0; i < b->ctx.size(); ++i) tiles[i] = eff_tile(b, i);
+    return MLEM_OK;
+}
+
+int mlem_batch_set_visits(mlem_batch* b, const int* visits) {
+    if (!b || !visits) return bfail(b, MLEM_ERR_INVALID, "null argument");
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+        const int v = visits[i];
+        if (v != -1 && v != MLEM_VISIT_FILE && v != MLEM_VISIT_SORTED &&
+            !(v == MLEM_VISIT_SORTED_STAGED && b->policy == MLEM_BATCH_ITEMS))
+            return bfail(b, MLEM_ERR_INVALID,
+                         "context %zu: row visiting order %d is not a batch order for schedule %d", i,
+                         v, b->policy);
+        if (v > MLEM_VISIT_FILE && !b->ctx[i]->row_order)
+            return bfail(b, MLEM_ERR_INVALID,
+                         "sorted row visiting: context %zu has no row order (MLEM_FLAG_NO_ROW_ORDER)", i);
+    }
+    BCK(b, cudaSetDevice(b->device));
+    b->visits.assign(visits, visits + b->ctx.size());
+    b->scheduled = false;
+    b->graph_dirty = true;
+    return batch_refresh(b, 1);
+}
+
+int mlem_batch_get_visits(const mlem_batch* b, int* visits) {
+    if (!b || !visits) return bfail(const_cast<mlem_batch*>(b), MLEM_ERR_INVALID, "null argument");
+    for (size_t i = 0; i < b->ctx.size(); ++i) visits[i] = eff_visit(b, i);
     return MLEM_OK;
 }
 
@@ -597,8 +635,9 @@ int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter) {
             if (s == MLEM_OK && (v == MLEM_VISIT_FILE || sorted_ok))
                 s = trial(MLEM_BATCH_ITEMS, ipb, 4, best_tile, v);
     // Then, with that schedule, a frame tile of its own for each context,
-    // heaviest first (contexts sharing a tile share a kernel).
-    std::vector<int> best_tiles(b->ctx.size(), 0);
+    // heaviest first, and then a row visit of its own (contexts sharing a
+    // tile and a visit share a kernel).
+    std::vector<int> best_tiles(b->ctx.size(), 0), best_visits(b->ctx.size(), -1);
     if (s == MLEM_OK && b->ctx.size() > 1) {
         s = mlem_batch_set_schedule(b, best_policy, best_ipb, best_bps, best_tile, best_visit);
         std::vector<size_t> order(b->ctx.size());
@@ -621,6 +660,23 @@ int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter) {
                     best_tiles = cand;
                 }
             }
+        if (s == MLEM_OK) s = mlem_batch_set_tiles(b, best_tiles.data());
+        for (size_t i : order)
+            for (int v : {MLEM_VISIT_FILE, MLEM_VISIT_SORTED, MLEM_VISIT_SORTED_STAGED}) {
+                if (s != MLEM_OK || v == (best_visits[i] >= 0 ? best_visits[i] : best_visit)) continue;
+                if (v != MLEM_VISIT_FILE && !b->ctx[i]->row_order) continue;
+                if (v == MLEM_VISIT_SORTED_STAGED && best_policy != MLEM_BATCH_ITEMS) continue;
+                std::vector<int> cand = best_visits;
+                cand[i] = v;
+                s = mlem_batch_set_visits(b, cand.data());
+                double ms = 0.0;
+                if (s == MLEM_OK) s = batch_time(b, 2, e0, e1, &ms);
+                if (s == MLEM_OK) s = restore();
+                if (s == MLEM_OK && ms < best) {
+                    best = ms;
+                    best_visits = cand;
+                }
+            }
     }
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
@@ -631,6 +687,7 @@ int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter) {
     if (s != MLEM_OK) return s;
     TRY(mlem_batch_set_schedule(b, best_policy, best_ipb, best_bps, best_tile, best_visit));
     TRY(mlem_batch_set_tiles(b, best_tiles.data()));
+    TRY(mlem_batch_set_visits(b, best_visits.data()));
     b->ms_per_iter = best;
     if (ms_per_iter) *ms_per_iter = best;
     return MLEM_OK;
@@ -704,7 +761,7 @@ int mlem_batch_profile(mlem_batch* b, int n, double* ms, double* bytes, int* lau
             tl[p] += pl[p];
         }
     }
-    tl[MLEM_PHASE_PROJECT] = (int)b->groups.size();  // one kernel per frame-tile group
+    tl[MLEM_PHASE_PROJECT] = (int)b->groups.size();  // one kernel per (frame tile, row visit) group
     for (int p = 0; p < MLEM_N_PHASES; ++p) {
         if (ms) ms[p] = acc[p] / n;
         if (bytes) bytes[p] = tb[p];

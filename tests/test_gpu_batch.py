@@ -109,6 +109,41 @@ def test_batch_tiles_per_context(members, policy, visit, tiles):
             c.close()
 
 
+@pytest.mark.parametrize("policy,batch_visit,visits,tiles", [
+    (IT, SORTED, [STAGED, SORTED, FILE], [0, 0, 0]),
+    (IT, SORTED, [-1, STAGED, -1], [4, 4, 2]),
+    (IT, STAGED, [FILE, -1, SORTED], [4, 0, 4]),
+    (IL, SORTED, [FILE, SORTED, -1], [0, 0, 0]),
+    (IL, FILE, [SORTED, -1, SORTED], [1, 4, 2]),
+])
+def test_batch_visits_per_context(members, policy, batch_visit, visits, tiles):
+    """Contexts with row visits of their own: one kernel per (frame tile,
+    visit) group, every image equal to the oracle's."""
+    ctxs = _contexts(members)
+    try:
+        with api.Batch(ctxs) as b:
+            b.set_schedule(policy, 4, 4, 4, batch_visit)
+            b.set_tiles(tiles)
+            b.set_visits(visits)
+            eff_v = [v if v >= 0 else batch_visit for v in visits]
+            eff_t = [t if t else 4 for t in tiles]
+            assert b.visits() == eff_v and b.tiles() == eff_t
+            assert b.schedule()["visits"] == eff_v
+            b.iterate(ITERS)
+            _, _, launches = b.profile(1)
+            assert launches[0] == len(set(zip(eff_t, eff_v)))
+            b.set_schedule(policy, 4, 4, 0, FILE)  # a batch visit again: every context follows it
+            assert b.visits() == [FILE] * 3
+        for c, (m, sinos, want) in zip(ctxs, members):  # the profiled iteration is one more
+            want1 = np.stack([ob.mlem(m, sinos[f], ITERS + 1)[0] for f in range(sinos.shape[0])])
+            got = c.get_images()
+            for f in range(sinos.shape[0]):
+                assert ob.rel_l2(got[f], want1[f]) <= TOL_MLEM, (m.n_rows, f)
+    finally:
+        for c in ctxs:
+            c.close()
+
+
 def test_batch_sums_and_chunking(members):
     """70 iterations (one 64-iteration graph plus 6 single launches) give
     the same images as 70 iterations of each context on its own, and the
@@ -142,6 +177,8 @@ def test_batch_autotune_restores_images(members):
             assert sched["frame_tile"] in (1, 2, 4)  # must divide 4, 8 and 16
             for t, padded in zip(sched["tiles"], (4, 16, 8)):
                 assert t in (1, 2, 4, 8, 16) and padded % t == 0
+            for v in sched["visits"]:
+                assert v in (FILE, SORTED) or (v == STAGED and sched["policy"] == IT)
             for c, x in zip(ctxs, before):
                 assert c.get_images().tobytes() == x.tobytes()
             b.iterate(ITERS)
@@ -210,6 +247,18 @@ def test_batch_rejects_bad_input(members):
                 b.set_tiles([4, 3, 0])
             with pytest.raises(api.MlemError):
                 b.set_tiles([4, 4])
+            b.set_schedule(IL, 4, 4, 0, FILE)
+            with pytest.raises(api.MlemError):  # staged: the items schedule only
+                b.set_visits([STAGED, -1, -1])
+            with pytest.raises(api.MlemError):
+                b.set_visits([-1, 9, -1])
+            with pytest.raises(api.MlemError):
+                b.set_visits([-2, -1, -1])
+            with pytest.raises(api.MlemError):  # a single-matrix order only
+                b.set_visits([-1, -1, api.VISIT_SORTED_CHUNKED])
+            with pytest.raises(api.MlemError):
+                b.set_visits([-1, -1])
+            assert b.visits() == [FILE] * 3
             b.iterate(ITERS)  # still usable after the rejected calls
         _check(ctxs, members)
         with api.Batch([unsorted] + ctxs[1:]) as b:
@@ -217,6 +266,10 @@ def test_batch_rejects_bad_input(members):
                 b.set_schedule(IL, 4, 4, 0, SORTED)
             with pytest.raises(api.MlemError):
                 b.set_schedule(IT, 4, 4, 0, STAGED)
+            with pytest.raises(api.MlemError):
+                b.set_visits([SORTED, -1, -1])
+            b.set_visits([FILE, SORTED, -1])  # the contexts with a row order may sort
+            assert b.visits() == [FILE, SORTED, FILE]
     finally:
         for c in ctxs + [exact, bare, unsorted]:
             c.close()
