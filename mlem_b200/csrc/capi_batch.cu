@@ -266,6 +266,7 @@ int batch_refresh(mlem_batch* b, int chunk) {
         TRY(bctx(b, c, ensure_history(c, chunk)));
         if (t.mats[i].Bp != c->Bp) reschedule = true;
         SparseView v = csr_view(c);
+        if (c->n_long) v.long_len = kLongRowElems;  // long rows: segments in their own kernels
         if (eff_visit(b, i) == MLEM_VISIT_FILE) {
             v.order = nullptr;
             v.vrange = nullptr;
@@ -321,6 +322,12 @@ int batch_enqueue(mlem_batch* b, bool stats, const PhaseEvents* pe = nullptr) {
         else
             BCK(b, batch_interleaved(g.table, g.tile, g.visit == MLEM_VISIT_SORTED, b->n_sm,
                                      b->blocks_per_sm, st));
+    }
+    for (size_t i = 0; i < b->ctx.size(); ++i) {
+        mlem_ctx* c = b->ctx[i];
+        if (c->n_long)
+            BCK(b, long_rows_pass(csr_view(c), c->long_segs, c->n_long_segs, c->n_long, c->x, c->Bp,
+                                  eff_tile(b, i), c->sino, c->f_long, c->update, b->n_sm, st));
     }
     TRY(bmark(b, pe, 1));
     TRY(bmark(b, pe, 2));
@@ -440,6 +447,15 @@ int mlem_batch_create(mlem_batch** out, mlem_ctx* const* ctxs, uint32_t n_ctx) {
         if (e != cudaSuccess)
             return bail(bfail(b, MLEM_ERR_CUDA, "row offsets of context %u: %s", i,
                               cudaGetErrorString(e)));
+        if (c->n_long) {  // rows above the long-row limit run in their own kernels: no item cost
+            uint64_t prev = pre[0];
+            for (uint32_t r = 0; r < c->R; ++r) {
+                const uint64_t end = pre[r + 1];
+                const uint64_t len = end - prev;
+                prev = end;
+                pre[r + 1] = pre[r] + (len > kLongRowElems ? 0 : len);
+            }
+        }
         if (c->row_order) {  // element prefix in sorted order (for the sorted visits)
             std::vector<uint64_t>& ps = b->pre_sorted[i];
             ps.resize((size_t)c->R + 1);
@@ -762,6 +778,8 @@ int mlem_batch_profile(mlem_batch* b, int n, double* ms, double* bytes, int* lau
         }
     }
     tl[MLEM_PHASE_PROJECT] = (int)b->groups.size();  // one kernel per (frame tile, row visit) group
+    for (const mlem_ctx* c : b->ctx)
+        if (c->n_long) tl[MLEM_PHASE_PROJECT] += 2;  // the long-row kernels
     for (int p = 0; p < MLEM_N_PHASES; ++p) {
         if (ms) ms[p] = acc[p] / n;
         if (bytes) bytes[p] = tb[p];

@@ -212,7 +212,7 @@ def test_skewed_matrix_long_rows_and_columns(golden):
             ctx.init_images()
             ctx.iterate(5)
             assert ob.rel_l2(ctx.get_images()[0], want) <= TOL_MLEM
-        # a batch with a regular matrix: items cut around the long rows
+        # a batch with a regular matrix: the long rows run as segments after the batch kernel
         small_m, small_sino, _, _, _ = golden.case("tiny_it10")
         with api.Context.from_matrix(small_m) as other:
             other.set_sinograms(small_sino)
@@ -223,6 +223,8 @@ def test_skewed_matrix_long_rows_and_columns(golden):
                                   (api.BATCH_INTERLEAVED, api.VISIT_FILE)):
                 with api.Batch([ctx, other]) as b:
                     b.set_schedule(policy, 64, 4, 1, visit)
+                    _, _, launches = b.profile(1)
+                    assert launches[0] == 1 + 2  # one group, then the long rows' two kernels
                     ctx.init_images()
                     other.init_images()
                     b.iterate(5)
