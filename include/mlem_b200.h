@@ -62,6 +62,11 @@ extern "C" {
                                            symmetry-compressed file omits (mlem_create_symmetric);
                                            without it the symmetry flags are ignored, as the
                                            reference's MLEM ignores them */
+#define MLEM_FLAG_MIRROR_KERNELS 0x40u /* with mlem_create_symmetric or a symmetry-compressed
+                                          file: keep only the stored elements on the device and
+                                          apply the mirrors inside the projection kernels
+                                          (MLEM_BK_MIRRORED): the full matrix's results with
+                                          about 1/|mirrors| of its device memory */
 
 /* ---- back-projection strategies ---------------------------------------- */
 #define MLEM_BK_AUTO 0    /* the autotuner's choice (CSC when not tuned) */
@@ -69,6 +74,8 @@ extern "C" {
 #define MLEM_BK_ATOMIC 2  /* atomic scatter over the CSR (reference GPU drivers' method) */
 #define MLEM_BK_FUSED 3   /* one pass per row: fwproj, correl and atomic scatter together */
 #define MLEM_BK_REGION 4  /* region-blocked copy: shared-memory image/update tiles per region */
+#define MLEM_BK_MIRRORED 5 /* mirrors applied in the kernels: a forward pass into per-row sums,
+                              then a scatter (contexts made with MLEM_FLAG_MIRROR_KERNELS only) */
 
 typedef struct mlem_ctx mlem_ctx;
 

@@ -40,14 +40,16 @@ FLAG_CHECKED = 0x4
 FLAG_NATURAL_LAYOUT = 0x8
 FLAG_NO_ROW_ORDER = 0x10
 FLAG_EXPAND_SYMMETRY = 0x20
+FLAG_MIRROR_KERNELS = 0x40
 
-BK_AUTO, BK_CSC, BK_ATOMIC, BK_FUSED, BK_REGION = 0, 1, 2, 3, 4
+BK_AUTO, BK_CSC, BK_ATOMIC, BK_FUSED, BK_REGION, BK_MIRRORED = 0, 1, 2, 3, 4, 5
 BATCH_INTERLEAVED, BATCH_ITEMS = 0, 1
 VISIT_FILE, VISIT_SORTED, VISIT_SORTED_CHUNKED, VISIT_SORTED_STAGED = 0, 1, 2, 3
 VISIT_NAMES = {VISIT_FILE: "file", VISIT_SORTED: "sorted", VISIT_SORTED_CHUNKED: "sorted-chunked",
                VISIT_SORTED_STAGED: "sorted-staged"}
 BATCH_NAMES = {BATCH_INTERLEAVED: "interleaved", BATCH_ITEMS: "items"}
-BK_NAMES = {BK_CSC: "csc", BK_ATOMIC: "atomic", BK_FUSED: "fused", BK_REGION: "region"}
+BK_NAMES = {BK_CSC: "csc", BK_ATOMIC: "atomic", BK_FUSED: "fused", BK_REGION: "region",
+            BK_MIRRORED: "mirrored"}
 
 ELEM_DTYPE = np.dtype([("index", "<u4"), ("value", "<f4")])
 

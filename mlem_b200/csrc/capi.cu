@@ -255,6 +255,26 @@ int build_long_rows(mlem_ctx* c) {
     return MLEM_OK;
 }
 
+// The natural-order and host copies of the column sums (c->norm, device
+// order) and initImage's sum of them (seqcsr4mlem.cpp:55-56: a sequential
+// double sum).
+int norm_views(mlem_ctx* c) {
+    if (c->bricked)
+        CK(c, permute_to_natural(c->norm, c->norm_nat, c->perm, c->C, 1, c->stream));
+    else if (c->C)
+        CK(c, cudaMemcpyAsync(c->norm_nat, c->norm, (size_t)c->C * 4, cudaMemcpyDeviceToDevice,
+                              c->stream));
+    c->norm_host.resize(c->C);
+    if (c->C)
+        CK(c, cudaMemcpyAsync(c->norm_host.data(), c->norm_nat, (size_t)c->C * 4,
+                              cudaMemcpyDeviceToHost, c->stream));
+    CK(c, cudaStreamSynchronize(c->stream));
+    double s = 0.0;
+    for (uint32_t i = 0; i < c->C; ++i) s += c->norm_host[i];
+    c->sumnorm = s;
+    return MLEM_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Setup common to all create paths: validate, voxel order, CSC, column sums.
 // ---------------------------------------------------------------------------
@@ -302,20 +322,7 @@ int finish_create(mlem_ctx* c) {
         CK(c, column_sums_atomic(csr_view(c), c->C, c->norm, c->stream));
     }
     TRY(dev_alloc(c, &c->norm_nat, std::max<uint32_t>(c->C, 1)));
-    if (c->bricked)
-        CK(c, permute_to_natural(c->norm, c->norm_nat, c->perm, c->C, 1, c->stream));
-    else if (c->C)
-        CK(c, cudaMemcpyAsync(c->norm_nat, c->norm, (size_t)c->C * 4, cudaMemcpyDeviceToDevice,
-                              c->stream));
-    c->norm_host.resize(c->C);
-    if (c->C)
-        CK(c, cudaMemcpyAsync(c->norm_host.data(), c->norm_nat, (size_t)c->C * 4,
-                              cudaMemcpyDeviceToHost, c->stream));
-    CK(c, cudaStreamSynchronize(c->stream));
-    // initImage's sum (seqcsr4mlem.cpp:55-56): sequential double sum of the norm.
-    double s = 0.0;
-    for (uint32_t i = 0; i < c->C; ++i) s += c->norm_host[i];
-    c->sumnorm = s;
+    TRY(norm_views(c));
     TRY(dev_alloc(c, &c->counter, 64));
     // Row visiting order, from the device column indices (after the remap).
     if (!(c->flags & MLEM_FLAG_NO_ROW_ORDER) && c->R > 1) {
@@ -355,10 +362,14 @@ int new_ctx(mlem_ctx** out, uint32_t R, uint32_t C, uint64_t Z, uint32_t flags, 
     if (device < 0 || device >= n_dev)
         return fail(nullptr, MLEM_ERR_INVALID, "device %d out of range (%d devices)", device, n_dev);
     if (flags & ~(MLEM_FLAG_EXACT | MLEM_FLAG_NO_CSC | MLEM_FLAG_CHECKED | MLEM_FLAG_NATURAL_LAYOUT |
-                  MLEM_FLAG_NO_ROW_ORDER | MLEM_FLAG_EXPAND_SYMMETRY))
+                  MLEM_FLAG_NO_ROW_ORDER | MLEM_FLAG_EXPAND_SYMMETRY | MLEM_FLAG_MIRROR_KERNELS))
         return fail(nullptr, MLEM_ERR_INVALID, "unknown flags 0x%x", flags);
     if ((flags & MLEM_FLAG_EXACT) && (flags & MLEM_FLAG_NO_CSC))
         return fail(nullptr, MLEM_ERR_INVALID, "MLEM_FLAG_EXACT needs the CSC copy");
+    if ((flags & MLEM_FLAG_EXACT) && (flags & MLEM_FLAG_MIRROR_KERNELS))
+        return fail(nullptr, MLEM_ERR_INVALID,
+                    "MLEM_FLAG_EXACT needs the full matrix (MLEM_FLAG_EXPAND_SYMMETRY), not "
+                    "MLEM_FLAG_MIRROR_KERNELS");
     mlem_ctx* c = new mlem_ctx();
     c->device = device;
     c->R = R;
@@ -552,6 +563,10 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
             return fail(c, MLEM_ERR_STATE,
                         "ordered subsets run on the one-pass method (MLEM_BK_FUSED), not mode %d",
                         t.bk_mode);
+        if (c->mirrored != (t.bk_mode == MLEM_BK_MIRRORED))
+            return fail(c, MLEM_ERR_STATE, c->mirrored
+                            ? "a context made with MLEM_FLAG_MIRROR_KERNELS runs MLEM_BK_MIRRORED only"
+                            : "MLEM_BK_MIRRORED needs a context made with MLEM_FLAG_MIRROR_KERNELS");
         switch (t.bk_mode) {
             case MLEM_BK_CSC:
                 if (!c->has_csc) return fail(c, MLEM_ERR_STATE, "no CSC copy (MLEM_FLAG_NO_CSC)");
@@ -610,6 +625,19 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                     CK(c, region_bkproj_update(c->rb, c->correl, Bp, f0, c->C, c->norm, c->x, cfg, st));
                 TRY(mark(c, pe, 2));
                 break;
+            case MLEM_BK_MIRRORED:
+                // per-row sums of the full matrix (correl holds them), then the scatter
+                CK(c, cudaMemsetAsync(c->correl, 0, (size_t)c->R * Bp * 4, st));
+                for (uint32_t f0 = 0; f0 < Bp; f0 += T)
+                    CK(c, mirror_fwproj(csr, c->mirror, c->x, Bp, f0, t.frame_tile, c->correl,
+                                        c->n_sm, t.blocks_per_sm, st));
+                TRY(mark(c, pe, 1));
+                for (uint32_t f0 = 0; f0 < Bp; f0 += T)
+                    CK(c, mirror_bkproj(csr, c->mirror, c->correl, c->sino, Bp, f0, t.frame_tile,
+                                        c->update, c->n_sm, t.blocks_per_sm, st));
+                TRY(mark(c, pe, 2));
+                CK(c, apply_update(c->x, c->update, c->norm, c->C, Bp, true, st));
+                break;
             default:
                 return fail(c, MLEM_ERR_INVALID, "unknown back-projection mode %d", t.bk_mode);
         }
@@ -650,6 +678,19 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
         launches[1] = nt;
         bytes[3] = 4.0 * C * B;
         launches[3] = 2;
+        return;
+    }
+    if (mode == MLEM_BK_MIRRORED) {
+        // the stored matrix once per pass and frame tile; forward: x, the row
+        // sums zeroed and written; backward: sinogram and row sums, update
+        bytes[0] = tiles * csr_pass + B * (4.0 * C + 8.0 * R);
+        bytes[1] = tiles * csr_pass + B * (8.0 * R + 4.0 * C);
+        launches[0] = nt;
+        launches[1] = nt;
+        bytes[3] = 4.0 * C * B;
+        launches[3] = 2;
+        bytes[2] = 4.0 * C + B * (4.0 * C + 8.0 * C + 4.0 * C);  // norm, update, x r/w, zeroing
+        launches[2] = 1;
         return;
     }
     if (mode == MLEM_BK_FUSED && !exact && c->n_subsets > 1) {
@@ -756,6 +797,81 @@ LaunchCfg cfg_for_frames(const mlem_ctx* c, uint32_t B) {
     return cfg;
 }
 
+// Mirrors applied in the kernels (MLEM_FLAG_MIRROR_KERNELS), set up on a
+// context that holds the stored matrix: the detector maps of the identity
+// and the header's mirrors (generateSyms order), the device voxel maps, and
+// the full matrix's column sums in place of the stored matrix's.
+int mirror_setup(mlem_ctx* c, const mlem_symmetry& sym, uint32_t nC) {
+    std::vector<uint32_t> lut8;
+    sym_detector_luts(sym.n_layers, sym.n_blocks, sym.block_size, sym.n_rings, lut8);
+    std::vector<uint32_t> ids = {0u};
+    for (uint32_t m : sym_mirrors(sym.sym)) ids.push_back(m);
+    MirrorView mv;
+    mv.n = (uint32_t)ids.size();
+    mv.n_crystals = nC;
+    mv.C = c->C;
+    std::vector<uint32_t> lut((size_t)mv.n * nC);
+    for (uint32_t j = 0; j < mv.n; ++j)
+        std::copy(lut8.begin() + (size_t)ids[j] * nC, lut8.begin() + (size_t)(ids[j] + 1) * nC,
+                  lut.begin() + (size_t)j * nC);
+    TRY(dev_alloc(c, &c->mirror_lut, lut.size()));
+    CK(c, cudaMemcpyAsync(c->mirror_lut, lut.data(), lut.size() * 4, cudaMemcpyHostToDevice,
+                          c->stream));
+    mv.lut = c->mirror_lut;
+    const uint32_t nx = c->grid[0], ny = c->grid[1], nz = c->grid[2];
+    int bits[3] = {0, 0, 0};
+    bool pow2 = true;
+    for (int i = 0; i < 3; ++i) {
+        while ((1ull << bits[i]) < c->grid[i]) ++bits[i];
+        pow2 = pow2 && (1ull << bits[i]) == c->grid[i];
+    }
+    std::vector<uint32_t> vox;
+    if (c->bricked && pow2) {
+        // the device index is the Morton code itself: a mirror flips one axis's bits
+        const uint64_t mx = morton_code(nx - 1, 0, 0, bits), my = morton_code(0, ny - 1, 0, bits),
+                       mz = morton_code(0, 0, nz - 1, bits);
+        for (uint32_t j = 0; j < mv.n; ++j)
+            mv.xor_mask[j] = (uint32_t)(((ids[j] & 1u) ? mx : 0) | ((ids[j] & 2u) ? my : 0) |
+                                        ((ids[j] & 4u) ? mz : 0));
+    } else {
+        vox.resize((size_t)mv.n * c->C);
+        const uint64_t slice = (uint64_t)nx * ny;
+        for (uint32_t j = 0; j < mv.n; ++j)
+            for (uint32_t d = 0; d < c->C; ++d) {
+                const uint32_t v = c->bricked ? c->iperm_host[d] : d;
+                uint32_t z = (uint32_t)(v / slice);
+                const uint32_t rem = (uint32_t)(v - z * slice);
+                uint32_t y = rem / nx, x = rem - y * nx;
+                if (ids[j] & 1u) x = nx - 1 - x;
+                if (ids[j] & 2u) y = ny - 1 - y;
+                if (ids[j] & 4u) z = nz - 1 - z;
+                const uint32_t w = (uint32_t)(z * slice + (uint64_t)y * nx + x);
+                vox[(size_t)j * c->C + d] = c->bricked ? c->perm_host[w] : w;
+            }
+        TRY(dev_alloc(c, &c->mirror_vox, vox.size()));
+        CK(c, cudaMemcpyAsync(c->mirror_vox, vox.data(), vox.size() * 4, cudaMemcpyHostToDevice,
+                              c->stream));
+        mv.vox = c->mirror_vox;
+    }
+    c->mirror = mv;
+    float* full = nullptr;
+    TRY(dev_alloc(c, &full, std::max<uint32_t>(c->C, 1)));
+    cudaError_t e = mirror_norm(c->norm, mv, full, c->stream);
+    if (e == cudaSuccess && c->C)
+        e = cudaMemcpyAsync(c->norm, full, (size_t)c->C * 4, cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);  // lut and vox leave scope
+    dev_free(full);
+    c->device_bytes -= (uint64_t)std::max<uint32_t>(c->C, 1) * 4;
+    CK(c, e);
+    TRY(norm_views(c));
+    c->mirrored = true;
+    c->tuning.bk_mode = MLEM_BK_MIRRORED;
+    c->tuning.group = 32;
+    c->tuning.visit = c->row_order ? MLEM_VISIT_SORTED : MLEM_VISIT_FILE;
+    c->tuning.blocks_per_sm = 8;
+    return MLEM_OK;
+}
+
 }  // namespace
 
 // ===========================================================================
@@ -856,6 +972,19 @@ int mlem_create_symmetric(mlem_ctx** out, const uint64_t* row_end, const void* e
     if (prev != nnz)
         return fail(nullptr, MLEM_ERR_MATRIX, "last row END offset %llu differs from nnz %llu",
                     (unsigned long long)prev, (unsigned long long)nnz);
+    if (flags & MLEM_FLAG_MIRROR_KERNELS) {
+        // the stored elements as an ordinary matrix on the grid, then the mirrors
+        mlem_ctx* c = nullptr;
+        TRY(mlem_create_grid(&c, row_end, elems, n_rows, n_cols, nnz, sym->grid, flags, device));
+        const int s = mirror_setup(c, *sym, (uint32_t)nC);
+        if (s != MLEM_OK) {
+            global_error() = c->err;
+            mlem_destroy(c);
+            return s;
+        }
+        *out = c;
+        return MLEM_OK;
+    }
     mlem_ctx* c = nullptr;
     TRY(new_ctx(&c, n_rows, n_cols, 0, flags, device));
     const uint64_t base_bytes = c->device_bytes;
@@ -1015,7 +1144,8 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->row_ranges, (void*)c->counter, (void*)c->long_segs, (void*)c->f_long_d,
                     (void*)c->sub_norm,
                     (void*)c->sub_file, (void*)c->sub_file_ranges, (void*)c->sub_sorted,
-                    (void*)c->sub_sorted_ranges})
+                    (void*)c->sub_sorted_ranges, (void*)c->mirror_lut, (void*)c->mirror_vox,
+                    (void*)c->f_mirror_d})
         dev_free(p);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -1055,6 +1185,7 @@ int mlem_kernels_per_iteration(const mlem_ctx* c, int* n) {
     else if (c->tuning.bk_mode == MLEM_BK_CSC) k += 2 * tiles;
     else if (c->tuning.bk_mode == MLEM_BK_ATOMIC) k += 2 * tiles + 1;
     else if (c->tuning.bk_mode == MLEM_BK_REGION) k += 2 * tiles + 1;  // + correl
+    else if (c->tuning.bk_mode == MLEM_BK_MIRRORED) k += 2 * tiles + 1;  // + update
     else if (c->n_subsets > 1)  // per subset: the one-pass launch(es) and the update
         k += (int)c->n_subsets * ((chunk_visit(c->tuning.visit) ? 1 : tiles) + 1);
     else if (chunk_visit(c->tuning.visit)) k += 2 + (c->n_long ? 2 : 0);  // all tiles in one launch
@@ -1130,11 +1261,16 @@ int mlem_calc_fwproj(mlem_ctx* c, const float* image, float* out) {
         CK(c, permute_to_device(c->tmp_c[0], c->tmp_c[1], c->perm, c->C, 1, c->stream));
         xd = c->tmp_c[1];
     }
-    if (c->flags & MLEM_FLAG_EXACT)
+    if (c->flags & MLEM_FLAG_EXACT) {
         CK(c, fwproj_exact(csr_view(c), xd, 1, nullptr, nullptr, c->tmp_r[0], c->stream));
-    else
+    } else if (c->mirrored) {
+        CK(c, cudaMemsetAsync(c->tmp_r[0], 0, (size_t)c->R * 4, c->stream));
+        CK(c, mirror_fwproj(csr_visit(c, c->tuning), c->mirror, xd, 1, 0, 1, c->tmp_r[0], c->n_sm,
+                            c->tuning.blocks_per_sm, c->stream));
+    } else {
         CK(c, fwproj(csr_visit(c, c->tuning), xd, 1, 0, nullptr, nullptr, c->tmp_r[0], cfg_for_frames(c, 1),
                      c->stream));
+    }
     CK(c, cudaMemcpyAsync(out, c->tmp_r[0], (size_t)c->R * 4, cudaMemcpyDeviceToHost, c->stream));
     CK(c, cudaStreamSynchronize(c->stream));
     return MLEM_OK;
@@ -1163,6 +1299,10 @@ int mlem_calc_bkproj(mlem_ctx* c, const float* correl, float* update) {
     float* ud = c->bricked ? c->tmp_c[1] : c->tmp_c[0];
     if (c->flags & MLEM_FLAG_EXACT) {
         CK(c, bkproj_exact(csc_view(c), c->tmp_r[0], 1, nullptr, nullptr, ud, c->stream));
+    } else if (c->mirrored) {
+        CK(c, cudaMemsetAsync(ud, 0, (size_t)c->C * 4, c->stream));
+        CK(c, mirror_bkproj(csr_visit(c, c->tuning), c->mirror, c->tmp_r[0], nullptr, 1, 0, 1, ud,
+                            c->n_sm, c->tuning.blocks_per_sm, c->stream));
     } else if (c->has_csc) {
         CK(c, bkproj_csc(csc_view(c), c->tmp_r[0], 1, 0, nullptr, nullptr, ud,
                          cfg_for_frames(c, 1), c->stream));
@@ -1346,11 +1486,20 @@ int mlem_get_tuning(const mlem_ctx* c, mlem_tuning* out) {
 int mlem_set_tuning(mlem_ctx* c, const mlem_tuning* t) {
     if (!c || !t) return fail(c, MLEM_ERR_INVALID, "null argument");
     mlem_tuning n = *t;
-    if (n.bk_mode == MLEM_BK_AUTO) n.bk_mode = c->has_csc ? MLEM_BK_CSC : MLEM_BK_ATOMIC;
+    if (n.bk_mode == MLEM_BK_AUTO)
+        n.bk_mode = c->mirrored ? MLEM_BK_MIRRORED : c->has_csc ? MLEM_BK_CSC : MLEM_BK_ATOMIC;
     if (n.bk_mode == MLEM_BK_CSC && !c->has_csc)
         return fail(c, MLEM_ERR_INVALID, "MLEM_BK_CSC needs the CSC copy");
-    if (n.bk_mode < MLEM_BK_CSC || n.bk_mode > MLEM_BK_REGION)
+    if (n.bk_mode < MLEM_BK_CSC || n.bk_mode > MLEM_BK_MIRRORED)
         return fail(c, MLEM_ERR_INVALID, "unknown back-projection mode %d", n.bk_mode);
+    if (c->mirrored != (n.bk_mode == MLEM_BK_MIRRORED))
+        return fail(c, MLEM_ERR_INVALID, c->mirrored
+                        ? "a context made with MLEM_FLAG_MIRROR_KERNELS runs MLEM_BK_MIRRORED only"
+                        : "MLEM_BK_MIRRORED needs a context made with MLEM_FLAG_MIRROR_KERNELS");
+    if (n.bk_mode == MLEM_BK_MIRRORED &&
+        (n.group != 32 || (n.visit != MLEM_VISIT_FILE && n.visit != MLEM_VISIT_SORTED)))
+        return fail(c, MLEM_ERR_INVALID,
+                    "MLEM_BK_MIRRORED runs 32 lanes per row (group 32) in file or sorted order");
     LaunchCfg cfg;
     cfg.group = n.group;
     cfg.frame_tile = n.frame_tile;
@@ -1394,18 +1543,25 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
     TRY(dev_alloc(c, &saved, (size_t)c->C * c->Bp));
     CK(c, cudaMemcpyAsync(saved, c->x, xb, cudaMemcpyDeviceToDevice, c->stream));
     std::vector<int> modes;
-    if (c->has_csc && c->n_subsets == 1) modes.push_back(MLEM_BK_CSC);
-    if (c->n_subsets > 1) {
+    if (c->mirrored) {  // one method; mlem_set_subsets refuses mirrored contexts
+        if (deterministic_only) {
+            cudaFree(saved);
+            c->device_bytes -= xb;
+            return fail(c, MLEM_ERR_STATE,
+                        "the mirrored kernels (MLEM_FLAG_MIRROR_KERNELS) have no deterministic method");
+        }
+        modes.push_back(MLEM_BK_MIRRORED);
+    } else if (c->n_subsets > 1) {
         if (deterministic_only) {
             cudaFree(saved);
             c->device_bytes -= xb;
             return fail(c, MLEM_ERR_STATE, "ordered subsets have no deterministic method");
         }
         modes.push_back(MLEM_BK_FUSED);
-    } else if (!deterministic_only) {
-        modes.push_back(MLEM_BK_ATOMIC);
-        modes.push_back(MLEM_BK_FUSED);
-        modes.push_back(MLEM_BK_REGION);
+    } else {
+        if (c->has_csc) modes.push_back(MLEM_BK_CSC);
+        if (!deterministic_only)
+            for (int m : {MLEM_BK_ATOMIC, MLEM_BK_FUSED, MLEM_BK_REGION}) modes.push_back(m);
     }
     cudaEvent_t e0, e1;
     CK(c, cudaEventCreate(&e0));
@@ -1430,6 +1586,7 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
                     if (visit != MLEM_VISIT_FILE && (!c->row_order || mode == MLEM_BK_REGION))
                         continue;
                     if (chunk_visit(visit) && mode != MLEM_BK_FUSED) continue;
+                    if (mode == MLEM_BK_MIRRORED && group != 32) continue;
                     // chunked: warp-wide rows; CTAs per SM 4 (bps 4) or 1 (bps 8 -> 1 below);
                     // staged: 4 or 3 CTAs of 256 threads
                     if (chunk_visit(visit) && group != 32) continue;
@@ -1499,6 +1656,9 @@ int mlem_set_subsets(mlem_ctx* c, uint32_t n) {
     if (n == 0) return fail(c, MLEM_ERR_INVALID, "at least one subset");
     if (n > 1 && (c->flags & MLEM_FLAG_EXACT))
         return fail(c, MLEM_ERR_INVALID, "ordered subsets do not run in the bit-exact mode");
+    if (n > 1 && c->mirrored)
+        return fail(c, MLEM_ERR_INVALID,
+                    "ordered subsets run over the full matrix's rows, not with MLEM_FLAG_MIRROR_KERNELS");
     if (n > 1 && n > c->R)
         return fail(c, MLEM_ERR_INVALID, "%u subsets for %u rows", n, c->R);
     TRY(set_device(c));
@@ -1582,6 +1742,13 @@ int mlem_fwproj_d(mlem_ctx* c, const float* x, float* y, uint32_t B, void* strea
         xd = c->pscratch[0];
     }
     const LaunchCfg cfg = cfg_for_frames(c, B);
+    if (c->mirrored) {
+        CK(c, cudaMemsetAsync(y, 0, (size_t)c->R * B * 4, st));
+        for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
+            CK(c, mirror_fwproj(csr_visit(c, c->tuning), c->mirror, xd, B, f0, cfg.frame_tile, y,
+                                c->n_sm, c->tuning.blocks_per_sm, st));
+        return MLEM_OK;
+    }
     for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
         CK(c, fwproj(csr_visit(c, c->tuning), xd, B, f0, nullptr, nullptr, y, cfg, st));
     return MLEM_OK;
@@ -1598,7 +1765,11 @@ int mlem_bkproj_d(mlem_ctx* c, const float* y, float* x, uint32_t B, void* strea
         xd = c->pscratch[0];
     }
     for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile) {
-        if (c->has_csc) {
+        if (c->mirrored) {
+            if (f0 == 0) CK(c, cudaMemsetAsync(xd, 0, (size_t)c->C * B * 4, st));
+            CK(c, mirror_bkproj(csr_visit(c, c->tuning), c->mirror, y, nullptr, B, f0,
+                                cfg.frame_tile, xd, c->n_sm, c->tuning.blocks_per_sm, st));
+        } else if (c->has_csc) {
             CK(c, bkproj_csc(csc_view(c), y, B, f0, nullptr, nullptr, xd, cfg, st));
         } else {
             if (f0 == 0) CK(c, cudaMemsetAsync(xd, 0, (size_t)c->C * B * 4, st));
@@ -1621,6 +1792,14 @@ int mlem_fwproj_correl_d(mlem_ctx* c, const float* x, const int32_t* sino, float
         xd = c->pscratch[0];
     }
     const LaunchCfg cfg = cfg_for_frames(c, B);
+    if (c->mirrored) {  // the full rows' sums, then calcCorrel in place
+        CK(c, cudaMemsetAsync(correl, 0, (size_t)c->R * B * 4, st));
+        for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
+            CK(c, mirror_fwproj(csr_visit(c, c->tuning), c->mirror, xd, B, f0, cfg.frame_tile,
+                                correl, c->n_sm, c->tuning.blocks_per_sm, st));
+        CK(c, correl_inplace(correl, sino, (uint64_t)c->R * B, st));
+        return MLEM_OK;
+    }
     for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
         CK(c, fwproj(csr_visit(c, c->tuning), xd, B, f0, sino, correl, nullptr, cfg, st));
     return MLEM_OK;
@@ -1633,6 +1812,35 @@ int mlem_fused_update_d(mlem_ctx* c, const float* x, const int32_t* sino, float*
         return fail(c, MLEM_ERR_STATE, "the one-pass method does not run in the bit-exact mode");
     TRY(set_device(c));
     cudaStream_t st = (cudaStream_t)stream;
+    if (c->mirrored) {  // the full rows' sums in a buffer of the context, then the scatter
+        const LaunchCfg cfg = cfg_for_frames(c, B);
+        const float* xd = x;
+        float* ud = u;
+        if (c->bricked) {
+            TRY(perm_scratch(c, (size_t)c->C * B));
+            CK(c, permute_to_device(x, c->pscratch[0], c->perm, c->C, B, st));
+            xd = c->pscratch[0];
+            ud = c->pscratch[1];
+        }
+        if (c->f_mirror_d_floats < (size_t)c->R * B) {
+            dev_free(c->f_mirror_d);
+            c->f_mirror_d = nullptr;
+            c->f_mirror_d_floats = 0;
+            TRY(dev_alloc(c, &c->f_mirror_d, (size_t)c->R * B));
+            c->f_mirror_d_floats = (size_t)c->R * B;
+        }
+        const SparseView v = csr_visit(c, c->tuning);
+        CK(c, cudaMemsetAsync(c->f_mirror_d, 0, (size_t)c->R * B * 4, st));
+        CK(c, cudaMemsetAsync(ud, 0, (size_t)c->C * B * 4, st));
+        for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
+            CK(c, mirror_fwproj(v, c->mirror, xd, B, f0, cfg.frame_tile, c->f_mirror_d, c->n_sm,
+                                c->tuning.blocks_per_sm, st));
+        for (uint32_t f0 = 0; f0 < B; f0 += (uint32_t)cfg.frame_tile)
+            CK(c, mirror_bkproj(v, c->mirror, c->f_mirror_d, sino, B, f0, cfg.frame_tile, ud,
+                                c->n_sm, c->tuning.blocks_per_sm, st));
+        if (c->bricked) CK(c, permute_to_natural(ud, u, c->perm, c->C, B, st));
+        return MLEM_OK;
+    }
     // the context's one-pass tuning when it has one, else sorted rows in chunks
     mlem_tuning t = c->tuning;
     if (t.bk_mode != MLEM_BK_FUSED) {
@@ -1673,7 +1881,8 @@ int mlem_fused_update_d(mlem_ctx* c, const float* x, const int32_t* sino, float*
 
 int mlem_bkproj_update_d(mlem_ctx* c, const float* correl, float* x, uint32_t B, void* stream) {
     if (!c || !x || !correl || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
-    if (!c->has_csc) return fail(c, MLEM_ERR_STATE, "fused back projection needs the CSC copy");
+    if (!c->has_csc || c->mirrored)
+        return fail(c, MLEM_ERR_STATE, "fused back projection needs the CSC copy of the full matrix");
     TRY(set_device(c));
     cudaStream_t st = (cudaStream_t)stream;
     float* xd = x;
@@ -1721,6 +1930,9 @@ int mlem_set_norm_d(mlem_ctx* c, const float* norm, void* stream) {
 
 int mlem_project_f64(mlem_ctx* c, const float* x, double* out) {
     if (!c || !x || !out) return fail(c, MLEM_ERR_INVALID, "null argument");
+    if (c->mirrored)
+        return fail(c, MLEM_ERR_STATE, "the FP64 projection reads the full matrix "
+                    "(MLEM_FLAG_EXPAND_SYMMETRY), not the stored one");
     TRY(set_device(c));
     TRY(ensure_tmp(c));
     if (!c->tmp_d) TRY(dev_alloc(c, &c->tmp_d, std::max<uint32_t>(c->R, 1)));

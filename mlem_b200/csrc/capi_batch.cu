@@ -413,6 +413,10 @@ int mlem_batch_create(mlem_batch** out, mlem_ctx* const* ctxs, uint32_t n_ctx) {
         if (c->flags & MLEM_FLAG_EXACT)
             return bfail(nullptr, MLEM_ERR_INVALID,
                          "context %u was created with MLEM_FLAG_EXACT (bit-exact kernels)", i);
+        if (c->mirrored)
+            return bfail(nullptr, MLEM_ERR_INVALID,
+                         "context %u was created with MLEM_FLAG_MIRROR_KERNELS (a batch runs the "
+                         "one-pass kernels over full matrices)", i);
         if (!c->B || !c->images_ready)
             return bfail(nullptr, MLEM_ERR_STATE, "context %u: sinograms and images not set", i);
     }

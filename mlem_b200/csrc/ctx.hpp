@@ -96,6 +96,16 @@ struct mlem_ctx {
     double* tmp_d = nullptr;
     float* inits_dev = nullptr;
 
+    // Mirrors applied in the kernels (MLEM_FLAG_MIRROR_KERNELS): the matrix
+    // arrays hold the stored elements only; norm holds the full matrix's
+    // column sums; f_mirror_d is the per-row sum buffer of mlem_fused_update_d.
+    bool mirrored = false;
+    mlem::MirrorView mirror;
+    uint32_t* mirror_lut = nullptr;
+    uint32_t* mirror_vox = nullptr;
+    float* f_mirror_d = nullptr;
+    size_t f_mirror_d_floats = 0;
+
     // region-blocked copy of the matrix (MLEM_BK_REGION), for one frame tile
     mlem::RegionBlocks rb;
     size_t rb_bytes = 0;

@@ -355,16 +355,20 @@ int mlem_create_from_file(mlem_ctx** out, const char* path, uint32_t flags, int 
         std::memcpy(aligned.data(), base + h.data_offset, 8ull * h.n_rows);
         row_end = aligned.data();
     }
-    if ((flags & MLEM_FLAG_EXPAND_SYMMETRY) && (h.flags & 7u)) {
-        // regenerate the elements the symmetries omitted (the reference's MLEM
-        // would use the stored ones only)
+    const uint32_t sym_flags = MLEM_FLAG_EXPAND_SYMMETRY | MLEM_FLAG_MIRROR_KERNELS;
+    if ((flags & MLEM_FLAG_EXPAND_SYMMETRY) && (flags & MLEM_FLAG_MIRROR_KERNELS)) {
+        s = err(MLEM_ERR_INVALID,
+                "MLEM_FLAG_EXPAND_SYMMETRY and MLEM_FLAG_MIRROR_KERNELS exclude each other");
+    } else if ((flags & sym_flags) && (h.flags & 7u)) {
+        // the elements the symmetries omitted: regenerated (expand) or applied
+        // in the kernels (the reference's MLEM would use the stored ones only)
         mlem_symmetry sym{h.flags & 7u, h.n_layers, h.n_blocks, h.block_size, h.n_rings,
                           {h.grid[0], h.grid[1], h.grid[2]}};
         s = mlem_create_symmetric(out, row_end, elems, h.n_rows, h.n_cols, h.nnz, &sym,
                                   flags & ~MLEM_FLAG_EXPAND_SYMMETRY, device);
     } else {
         s = mlem_create_grid(out, row_end, elems, h.n_rows, h.n_cols, h.nnz, h.grid,
-                             flags & ~MLEM_FLAG_EXPAND_SYMMETRY, device);
+                             flags & ~sym_flags, device);
     }
     if (map) ::munmap(map, h.file_size);
     return s;

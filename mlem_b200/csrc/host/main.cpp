@@ -23,7 +23,8 @@
 // openmpcsr4mlem built with -DMESSUNG, openmpcsr4mlem.cpp:217),
 // MLEM_B200_EXPAND_SYMMETRY=1 (reconstruct with the full matrix of a
 // symmetry-compressed file; by default its symmetry flags are ignored, as the
-// reference's drivers ignore them).
+// reference's drivers ignore them; =kernels: the same reconstruction with only
+// the stored elements on the GPU and the mirrors applied in the kernels).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -111,7 +112,9 @@ int run(int argc, char** argv) {
         if (o.has_checkpointing) std::cout << "Checkpointing: " << o.checkpointing << std::endl;
     }
     uint32_t flags = env_int("MLEM_B200_EXACT", 0) ? MLEM_FLAG_EXACT : 0u;
-    if (env_int("MLEM_B200_EXPAND_SYMMETRY", 0)) flags |= MLEM_FLAG_EXPAND_SYMMETRY;
+    const char* expand = std::getenv("MLEM_B200_EXPAND_SYMMETRY");
+    if (expand && std::strcmp(expand, "kernels") == 0) flags |= MLEM_FLAG_MIRROR_KERNELS;
+    else if (env_int("MLEM_B200_EXPAND_SYMMETRY", 0)) flags |= MLEM_FLAG_EXPAND_SYMMETRY;
     const int device = env_int("MLEM_B200_DEVICE", 0);
 
     auto t0 = std::chrono::steady_clock::now();
@@ -168,7 +171,9 @@ int run(int argc, char** argv) {
     const char* tune = std::getenv("MLEM_B200_AUTOTUNE");
     if (tune && *tune && std::strcmp(tune, "0") != 0) {
         mlem_tuning t;
-        check(mlem_autotune(ctx, std::strcmp(tune, "any") == 0 ? 0 : 1, &t), ctx);
+        // the mirrored kernels have atomics only: no deterministic choice to restrict to
+        const bool any = std::strcmp(tune, "any") == 0 || (info.flags & MLEM_FLAG_MIRROR_KERNELS);
+        check(mlem_autotune(ctx, any ? 0 : 1, &t), ctx);
         if (!csv)
             std::cout << "Autotuned: mode " << t.bk_mode << ", group " << t.group << ", frame tile "
                       << t.frame_tile << ", row visit " << t.visit << ", " << t.ms_per_iter

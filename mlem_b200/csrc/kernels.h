@@ -96,6 +96,35 @@ cudaError_t sym_count(const SymExpand& s, uint32_t mirror, unsigned long long* c
 cudaError_t sym_fill(const SymExpand& s, uint32_t mirror, unsigned long long* cursor, uint2* out,
                      cudaStream_t st);
 
+// ---- mirrors applied in the kernels (k_mirror.cu) --------------------------
+// A symmetry-compressed matrix kept as stored; mirror j (0 = the identity,
+// then the header's mirrors in generateSyms order) maps stored row r to full
+// row lor(r, j) through lut[j * n_crystals + detector], and device voxel v to
+// vox[j * C + v], or to v ^ xor_mask[j] when vox is null (power-of-two grid
+// in Morton order).
+struct MirrorView {
+    const uint32_t* lut = nullptr;
+    const uint32_t* vox = nullptr;
+    uint32_t xor_mask[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    uint32_t n_crystals = 0;
+    uint32_t C = 0;
+    uint32_t n = 1;  // mirrors including the identity, 1..8
+};
+// f[lor(r, j)][f0 .. f0+frame_tile) += the stored row's partial sums under
+// every mirror (f zeroed by the caller; float atomics).
+cudaError_t mirror_fwproj(const SparseView& csr, const MirrorView& mv, const float* x, uint32_t B,
+                          uint32_t f0, int frame_tile, float* f, int sm_count, int blocks_per_sm,
+                          cudaStream_t st);
+// u[vox(v, j)][...] += value * c for every stored element and mirror, with
+// c = calcCorrel(sino[t], y[t]) when sino is non-null, else y[t] (u zeroed
+// by the caller).
+cudaError_t mirror_bkproj(const SparseView& csr, const MirrorView& mv, const float* y,
+                          const int32_t* sino, uint32_t B, uint32_t f0, int frame_tile, float* u,
+                          int sm_count, int blocks_per_sm, cudaStream_t st);
+// Full column sums from the stored matrix's: sum over j of norm[vox(w, j)].
+cudaError_t mirror_norm(const float* norm_stored, const MirrorView& mv, float* norm_full,
+                        cudaStream_t st);
+
 // ---- rows too long for one warp (k_long.cu) ------------------------------
 // Rows longer than kLongRowElems are cut into segments of at most
 // kLongSegElems elements: elements [b, e) of row `row`, the slot-th long row.
