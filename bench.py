@@ -11,7 +11,10 @@ plus the per-iteration image-sum census the reference prints).  The matrix
 steps.  The batched line ("batched-b16") runs 16 sinograms over the same
 matrix in one pass per iteration; the "uneven" line batches three matrices
 of different geometry (12, 8 and 4 sinograms) in one kernel per iteration
-(mlem_b200.uneven).
+(mlem_b200.uneven); the "mirrored" line reconstructs the plain-full matrix
+read as a symmetry-compressed file (three mirrors, a 50 GB full matrix) once
+expanded on the device and once with the mirrors applied in the kernels
+(mlem_b200.mirrored).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -60,6 +63,8 @@ def parse_args():
     ap.add_argument("--no-differentiable", action="store_true")
     ap.add_argument("--no-uneven", action="store_true",
                     help="skip the uneven three-geometry batch (one GPU only)")
+    ap.add_argument("--no-mirrored", action="store_true",
+                    help="skip the symmetry-compressed matrix, expanded vs mirrored kernels (one GPU only)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=3)
     return ap.parse_args()
@@ -410,6 +415,12 @@ def run_ours(a, rank, world, local_rank):
         from mlem_b200 import uneven
         torch.cuda.synchronize()
         line["uneven"] = uneven.run(iters=max(10, min(a.steps, 20)), warmup=3, device=local_rank)
+
+    # --- a symmetry-compressed matrix: expanded on the device vs mirrors in the kernels ---
+    if world == 1 and not a.no_mirrored:
+        from mlem_b200 import mirrored
+        torch.cuda.synchronize()
+        line["mirrored"] = mirrored.run(iters=10, warmup=3, device=local_rank)
 
     if dist is not None:
         dist.destroy_process_group()
