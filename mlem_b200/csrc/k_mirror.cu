@@ -32,15 +32,44 @@ namespace mlem {
 namespace {
 
 constexpr int kMirrorThreads = 256;
+constexpr int kMirrorCtasPerSm = 3;
+// 3 blocks of 256 threads per SM (at most 85 registers): the mirror groups
+// below hold more loads in flight than 64 registers allow, and unbounded
+// they take 100-110 registers and too few warps (measured on the plain-full
+// matrix with three mirrors: 30.7 ms per iteration bounded, 33.3 unbounded,
+// 31.8 with one mirror at a time).
 constexpr int kMirrorBatch = 8;  // elements per lane held across the mirrors
 
-// Full row of stored row r under mirror j (symhandler.hpp transformLor: both
-// detectors mapped, the smaller first); mirror 0 is the row itself.
-__device__ __forceinline__ uint32_t mirror_row(uint32_t r, uint32_t j, const MirrorView& mv) {
-    if (j == 0) return r;
-    const uint32_t* lut = mv.lut + (size_t)j * mv.n_crystals;
-    const uint32_t d1 = lut[r / mv.n_crystals], d2 = lut[r % mv.n_crystals];
-    return d1 < d2 ? d1 * mv.n_crystals + d2 : d2 * mv.n_crystals + d1;
+// Mirrors worked on together, so that their loads go out back to back: the
+// forward pass gathers for FW mirrors at once (one at wide frame tiles, whose
+// gathers already fill the registers), the backward pass loads the row sums
+// and counts of BK mirrors at once.
+template <int BT>
+constexpr int fw_group() { return Lanes<BT>::VW == 1 ? 2 : 1; }
+template <int BT>
+constexpr int bk_group() { return Lanes<BT>::VW == 1 ? 8 : Lanes<BT>::VW == 2 ? 4 : 2; }
+
+// Full rows of stored row r = d1 * n_crystals + d2 under mirrors j0 .. j0+MG-1
+// (symhandler.hpp transformLor: both detectors mapped, the smaller first;
+// mirror 0 is the row itself).  Entries past the last mirror are left as r.
+template <int MG>
+__device__ __forceinline__ void mirror_rows(uint32_t r, uint32_t d1, uint32_t d2, uint32_t j0,
+                                            const MirrorView& mv, uint32_t (&t)[MG]) {
+    uint32_t a[MG], c[MG];
+#pragma unroll
+    for (int p = 0; p < MG; ++p) {
+        const uint32_t j = j0 + p;
+        const bool mapped = j != 0 && j < mv.n;
+        const uint32_t* lut = mv.lut + (size_t)(mapped ? j : 0) * mv.n_crystals;
+        a[p] = mapped ? __ldg(lut + d1) : 0u;
+        c[p] = mapped ? __ldg(lut + d2) : 0u;
+    }
+#pragma unroll
+    for (int p = 0; p < MG; ++p) {
+        const uint32_t j = j0 + p;
+        t[p] = (j == 0 || j >= mv.n) ? r
+               : a[p] < c[p] ? a[p] * mv.n_crystals + c[p] : c[p] * mv.n_crystals + a[p];
+    }
 }
 
 struct VoxMap {
@@ -51,36 +80,47 @@ struct VoxMap {
     }
 };
 
+// Mirror j's voxel map (j past the last mirror: the identity, never used).
 __device__ __forceinline__ VoxMap vox_map(uint32_t j, const MirrorView& mv) {
-    if (j == 0 || !mv.vox) return VoxMap{nullptr, j == 0 ? 0u : mv.xor_mask[j]};
+    if (j == 0 || j >= mv.n) return VoxMap{nullptr, 0u};
+    if (!mv.vox) return VoxMap{nullptr, mv.xor_mask[j]};
     return VoxMap{mv.vox + (size_t)j * mv.C, 0u};
 }
 
-// acc[0..VW) += sum over nb loaded elements q[] of value * vec[map(col) * B + off ...]
-template <int BT>
-__device__ __forceinline__ void mirrored_dot(const uint2 (&q)[kMirrorBatch], const bool (&live)[kMirrorBatch],
-                                             const VoxMap& map, const float* __restrict__ base,
-                                             uint32_t B, float (&acc)[Lanes<BT>::VW], uint64_t ph) {
+// acc[p][0..VW) += sum over the loaded elements q[] of value *
+// vec[map_p(col) * B + ...] for the MG mirrors of a group (nm of them real).
+template <int BT, int MG>
+__device__ __forceinline__ void mirrored_dot(const uint2 (&q)[kMirrorBatch],
+                                             const bool (&live)[kMirrorBatch],
+                                             const VoxMap (&map)[MG], int nm,
+                                             const float* __restrict__ base, uint32_t B,
+                                             float (&acc)[MG][Lanes<BT>::VW], uint64_t ph) {
     constexpr int VW = Lanes<BT>::VW;
-    uint32_t m[kMirrorBatch];
+    uint32_t m[MG][kMirrorBatch];
 #pragma unroll
-    for (int u = 0; u < kMirrorBatch; ++u) m[u] = live[u] ? map(q[u].x) : 0u;
-    float xv[kMirrorBatch][VW];
+    for (int p = 0; p < MG; ++p)
 #pragma unroll
-    for (int u = 0; u < kMirrorBatch; ++u) {
-        if (live[u]) {
-            ld_vec<VW>(base + (size_t)m[u] * B, xv[u], ph);
-        } else {
+        for (int u = 0; u < kMirrorBatch; ++u) m[p][u] = (p < nm && live[u]) ? map[p](q[u].x) : 0u;
+    float xv[MG][kMirrorBatch][VW];
 #pragma unroll
-            for (int i = 0; i < VW; ++i) xv[u][i] = 0.0f;
+    for (int p = 0; p < MG; ++p)
+#pragma unroll
+        for (int u = 0; u < kMirrorBatch; ++u) {
+            if (p < nm && live[u]) {
+                ld_vec<VW>(base + (size_t)m[p][u] * B, xv[p][u], ph);
+            } else {
+#pragma unroll
+                for (int i = 0; i < VW; ++i) xv[p][u][i] = 0.0f;
+            }
         }
-    }
 #pragma unroll
-    for (int u = 0; u < kMirrorBatch; ++u) {
-        const float v = __uint_as_float(q[u].y);
+    for (int p = 0; p < MG; ++p)
 #pragma unroll
-        for (int i = 0; i < VW; ++i) acc[i] = fmaf(v, xv[u][i], acc[i]);
-    }
+        for (int u = 0; u < kMirrorBatch; ++u) {
+            const float v = __uint_as_float(q[u].y);
+#pragma unroll
+            for (int i = 0; i < VW; ++i) acc[p][i] = fmaf(v, xv[p][u][i], acc[p][i]);
+        }
 }
 
 // Element range of the warp's row at visiting position v.
@@ -116,10 +156,10 @@ __device__ __forceinline__ void load_batch(const uint2* __restrict__ el, uint64_
 // Forward pass: f[lor(r, j) * B + f0 + ...] += the partial sum of stored row
 // r under mirror j, for frames [f0, f0 + BT).
 template <int BT, bool SORTED>
-__global__ void __launch_bounds__(kMirrorThreads) k_mirror_fw(SparseView csr, MirrorView mv,
+__global__ void __launch_bounds__(kMirrorThreads, kMirrorCtasPerSm) k_mirror_fw(SparseView csr, MirrorView mv,
                                                               const float* __restrict__ x, uint32_t B,
                                                               uint32_t f0, float* __restrict__ f) {
-    constexpr int VW = Lanes<BT>::VW, FL = Lanes<BT>::FL, EPS = 32 / FL;
+    constexpr int VW = Lanes<BT>::VW, FL = Lanes<BT>::FL, EPS = 32 / FL, MG = fw_group<BT>();
     constexpr uint64_t kSpan = (uint64_t)kMirrorBatch * EPS;
     const int lane = threadIdx.x & 31, sub = lane % FL;
     const uint64_t ps = l2_evict_first(), ph = l2_evict_last();
@@ -132,25 +172,33 @@ __global__ void __launch_bounds__(kMirrorThreads) k_mirror_fw(SparseView csr, Mi
         row_at<SORTED>(csr, v, r, b, e);
         const uint64_t n = e - b;
         if (n == 0) continue;  // warp-uniform
+        const uint32_t d1 = r / mv.n_crystals, d2 = r - d1 * mv.n_crystals;
         uint2 q0[kMirrorBatch];
         bool l0[kMirrorBatch];
         load_batch<BT>(el, b, n, 0, lane, q0, l0, ps);
-        for (uint32_t j = 0; j < mv.n; ++j) {
-            const VoxMap map = vox_map(j, mv);
-            float acc[VW];
+        for (uint32_t j0 = 0; j0 < mv.n; j0 += MG) {
+            const int nm = (int)min((uint32_t)MG, mv.n - j0);
+            uint32_t t[MG];
+            mirror_rows<MG>(r, d1, d2, j0, mv, t);  // off the gathers' path
+            VoxMap map[MG];
 #pragma unroll
-            for (int i = 0; i < VW; ++i) acc[i] = 0.0f;
-            mirrored_dot<BT>(q0, l0, map, xb, B, acc, ph);
+            for (int p = 0; p < MG; ++p) map[p] = vox_map(j0 + p, mv);
+            float acc[MG][VW];
+#pragma unroll
+            for (int p = 0; p < MG; ++p)
+#pragma unroll
+                for (int i = 0; i < VW; ++i) acc[p][i] = 0.0f;
+            mirrored_dot<BT, MG>(q0, l0, map, nm, xb, B, acc, ph);
             for (uint64_t k0 = kSpan; k0 < n; k0 += kSpan) {  // rows longer than one batch
                 uint2 q[kMirrorBatch];
                 bool l[kMirrorBatch];
                 load_batch<BT>(el, b, n, k0, lane, q, l, ps);
-                mirrored_dot<BT>(q, l, map, xb, B, acc, ph);
+                mirrored_dot<BT, MG>(q, l, map, nm, xb, B, acc, ph);
             }
-            slot_allreduce<32, BT>(acc);
-            if (lane < FL) {
-                const uint32_t t = mirror_row(r, j, mv);
-                red_vec<VW>(f + (size_t)t * B + f0 + sub * VW, 1.0f, acc);
+#pragma unroll
+            for (int p = 0; p < MG; ++p) {
+                slot_allreduce<32, BT>(acc[p]);
+                if (p < nm && lane < FL) red_vec<VW>(f + (size_t)t[p] * B + f0 + sub * VW, 1.0f, acc[p]);
             }
         }
     }
@@ -159,12 +207,12 @@ __global__ void __launch_bounds__(kMirrorThreads) k_mirror_fw(SparseView csr, Mi
 // Backward pass: u[vox(v, j) * B + f0 + ...] += value * c, with c =
 // calcCorrel(sino[t], y[t]) when sino is non-null, else y[t] (t = lor(r, j)).
 template <int BT, bool SORTED>
-__global__ void __launch_bounds__(kMirrorThreads) k_mirror_bk(SparseView csr, MirrorView mv,
+__global__ void __launch_bounds__(kMirrorThreads, kMirrorCtasPerSm) k_mirror_bk(SparseView csr, MirrorView mv,
                                                               const float* __restrict__ y,
                                                               const int32_t* __restrict__ sino,
                                                               uint32_t B, uint32_t f0,
                                                               float* __restrict__ u) {
-    constexpr int VW = Lanes<BT>::VW, FL = Lanes<BT>::FL, EPS = 32 / FL;
+    constexpr int VW = Lanes<BT>::VW, FL = Lanes<BT>::FL, EPS = 32 / FL, MG = bk_group<BT>();
     constexpr uint64_t kSpan = (uint64_t)kMirrorBatch * EPS;
     const int lane = threadIdx.x & 31, sub = lane % FL;
     const uint64_t ps = l2_evict_first();
@@ -177,31 +225,41 @@ __global__ void __launch_bounds__(kMirrorThreads) k_mirror_bk(SparseView csr, Mi
         row_at<SORTED>(csr, v, r, b, e);
         const uint64_t n = e - b;
         if (n == 0) continue;  // warp-uniform
+        const uint32_t d1 = r / mv.n_crystals, d2 = r - d1 * mv.n_crystals;
         uint2 q0[kMirrorBatch];
         bool l0[kMirrorBatch];
         load_batch<BT>(el, b, n, 0, lane, q0, l0, ps);
-        for (uint32_t j = 0; j < mv.n; ++j) {
-            const uint32_t t = mirror_row(r, j, mv);
-            const size_t idx = (size_t)t * B + f0 + sub * VW;
-            float cv[VW];
-            ld_plain<VW>(y + idx, cv);
-            if (sino) {
-                int32_t s[VW];
-                ld_counts<VW>(sino + idx, s);
+        for (uint32_t j0 = 0; j0 < mv.n; j0 += MG) {
+            uint32_t t[MG];
+            mirror_rows<MG>(r, d1, d2, j0, mv, t);
+            // the group's row sums and counts, all loads in flight together
+            float cv[MG][VW];
+            int32_t s[MG][VW];
 #pragma unroll
-                for (int i = 0; i < VW; ++i) cv[i] = correl_of(s[i], cv[i]);
+            for (int p = 0; p < MG; ++p) {
+                const size_t idx = (size_t)t[p] * B + f0 + sub * VW;
+                ld_plain<VW>(y + idx, cv[p]);
+                if (sino) ld_counts<VW>(sino + idx, s[p]);
             }
-            bool any = false;
 #pragma unroll
-            for (int i = 0; i < VW; ++i) any |= (cv[i] != 0.0f);
-            if (!__any_sync(MLEM_FULL_MASK, any)) continue;
-            const VoxMap map = vox_map(j, mv);
+            for (int p = 0; p < MG; ++p) {
+                if (j0 + p >= mv.n) break;  // warp-uniform
+                bool any = false;
 #pragma unroll
-            for (int w = 0; w < kMirrorBatch; ++w)
-                if (l0[w] && any) red_vec<VW>(ub + (size_t)map(q0[w].x) * B, __uint_as_float(q0[w].y), cv);
-            for (uint64_t k = kSpan + (uint64_t)(lane / FL); k < n; k += EPS) {
-                const uint2 qe = ld_keep2(el + b + k, ps);
-                if (any) red_vec<VW>(ub + (size_t)map(qe.x) * B, __uint_as_float(qe.y), cv);
+                for (int i = 0; i < VW; ++i) {
+                    if (sino) cv[p][i] = correl_of(s[p][i], cv[p][i]);
+                    any |= (cv[p][i] != 0.0f);
+                }
+                if (!__any_sync(MLEM_FULL_MASK, any)) continue;
+                const VoxMap map = vox_map(j0 + p, mv);
+#pragma unroll
+                for (int w = 0; w < kMirrorBatch; ++w)
+                    if (l0[w] && any)
+                        red_vec<VW>(ub + (size_t)map(q0[w].x) * B, __uint_as_float(q0[w].y), cv[p]);
+                for (uint64_t k = kSpan + (uint64_t)(lane / FL); k < n; k += EPS) {
+                    const uint2 qe = ld_keep2(el + b + k, ps);
+                    if (any) red_vec<VW>(ub + (size_t)map(qe.x) * B, __uint_as_float(qe.y), cv[p]);
+                }
             }
         }
     }
@@ -219,6 +277,10 @@ __global__ void k_mirror_norm(const float* __restrict__ norm, MirrorView mv, flo
     }
 }
 
+// blocks_per_sm x SMs blocks (at most one warp per row).  More blocks than
+// are resident (kMirrorCtasPerSm per SM) measured faster than one resident
+// wave: 30.7 against 33.2 ms per iteration on the plain-full matrix with
+// three mirrors at blocks_per_sm 8.
 int mirror_grid(const SparseView& csr, int sm_count, int blocks_per_sm) {
     const uint64_t warps = csr.n;
     const uint64_t want = (warps * 32 + kMirrorThreads - 1) / kMirrorThreads;
