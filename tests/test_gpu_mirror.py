@@ -167,3 +167,27 @@ def test_file_flag_and_cli(tmp_path):
         env = dict(os.environ, MLEM_B200_EXPAND_SYMMETRY="kernels", MLEM_B200_AUTOTUNE=tune)
         subprocess.run([CLI, path, sp, out, "5"], check=True, env=env, capture_output=True)
         assert ob.rel_l2(formats.read_vector(out, np.float32), want) <= TOL
+
+
+def test_torch_projector_and_unrolled_mlem():
+    """The torch extension over a mirrored context: forward and back projection
+    equal the full matrix's, and the unrolled MLEM's forward pass equals the
+    oracle's MLEM on the full matrix."""
+    from mlem_b200 import torch_ext
+
+    m = sym_matrix(7, seed=111, grid=(6, 8, 4))
+    full = ob.expand_symmetries(m)
+    A = _full_dense(full)
+    sino = _frames(m, 1, 13)[0]
+    with api.Context.symmetric(m, flags=MK) as ctx:
+        x = torch.rand(m.n_cols, device="cuda", dtype=torch.float32, requires_grad=True)
+        y = torch_ext.forward_project(x, ctx)
+        assert ob.rel_l2(y.detach().cpu().numpy(), A @ x.detach().cpu().numpy().astype(np.float64)) <= 1e-6
+        g = torch.rand(m.n_rows, device="cuda", dtype=torch.float32)
+        (y * g).sum().backward()
+        assert ob.rel_l2(x.grad.cpu().numpy(), A.T @ g.cpu().numpy().astype(np.float64)) <= 1e-6
+        norm = ob.column_sums(full)
+        x0 = torch.full((m.n_cols,), float(ob.init_value(norm, sino)), device="cuda")
+        xk = torch_ext.unrolled_mlem(x0, torch.ones(4), torch.from_numpy(sino), ctx)
+        want, _ = ob.mlem(full, sino, 4)
+        assert ob.rel_l2(xk.detach().cpu().numpy(), want) <= TOL

@@ -107,3 +107,16 @@ def test_no_symmetry_is_the_stored_matrix():
     full = ob.expand_symmetries(m)
     assert full.elems.tobytes() == np.ascontiguousarray(m.elems).tobytes()
     assert np.array_equal(full.row_end, m.row_end)
+
+
+def test_mirrored_workload_scanner():
+    """The bench's symmetry-compressed workload reads an n^2-LOR matrix as a
+    scanner of n crystals (n a multiple of 512)."""
+    from mlem_b200 import mirrored
+
+    assert mirrored.scanner_for(4194304) == (1, 32, 16, 4)
+    nl, nb, bs, nr = mirrored.scanner_for(1048576)
+    assert nl * nb * bs * nr == 1024
+    for bad in (1000, 512 * 512 + 1, 256 * 256):
+        with pytest.raises(ValueError):
+            mirrored.scanner_for(bad)
