@@ -66,7 +66,12 @@ extern "C" {
                                           file: keep only the stored elements on the device and
                                           apply the mirrors inside the projection kernels
                                           (MLEM_BK_MIRRORED): the full matrix's results with
-                                          about 1/|mirrors| of its device memory */
+                                          about 1/|mirrors| of its device memory.  mlem_info.nnz,
+                                          mlem_get_csr and mlem_get_csc give the stored elements;
+                                          the column sums are the full matrix's.  Not with
+                                          MLEM_FLAG_EXACT, ordered subsets, batches,
+                                          mlem_bkproj_update_d or mlem_project_f64 (they
+                                          return MLEM_ERR_INVALID / MLEM_ERR_STATE) */
 
 /* ---- back-projection strategies ---------------------------------------- */
 #define MLEM_BK_AUTO 0    /* the autotuner's choice (CSC when not tuned) */
