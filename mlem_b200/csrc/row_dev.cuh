@@ -120,13 +120,20 @@ __device__ __forceinline__ bool row_dot(const uint2* __restrict__ el, uint64_t b
 #pragma unroll
     for (int i = 0; i < VW; ++i) acc[i] = 0.0f;
     const bool one_batch = e - b <= (uint64_t)kBatch * EPS;
+    // Elements go through L1 when the fused kernel may re-read them for its
+    // scatter (rows longer than one batch).  A full warp at one frame holds 256
+    // elements per batch, so the rows of a typical matrix stay in registers
+    // and their elements skip L1, leaving its lines to the image gathers
+    // (plain-full, chunked walk: 2.450 vs 2.471 ms; at 16 frames, where rows
+    // span several batches, skipping L1 cost 13 %).
+    constexpr bool kL1 = KEEP && !(G == 32 && BT == 1);
     for (uint64_t k0 = b + lane / FL; k0 < e; k0 += (uint64_t)kBatch * EPS) {
         uint2 q[kBatch];
 #pragma unroll
         for (int u = 0; u < kBatch; ++u) {
             const uint64_t k = k0 + (uint64_t)u * EPS;
             q[u] = make_uint2(0u, 0u);  // value 0: contributes nothing
-            if (k < e) q[u] = KEEP ? ld_keep2(el + k, ps) : ld_stream2(el + k, ps);
+            if (k < e) q[u] = kL1 ? ld_keep2(el + k, ps) : ld_stream2(el + k, ps);
         }
         float xv[kBatch][VW];
 #pragma unroll
