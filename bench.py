@@ -604,7 +604,7 @@ def run_reference(a, rank, world):
         del m
         threads = host_threads()
         k = max(1, min(a.steps, 20))
-        wu = max(1, min(a.warmup, 2))
+        wu = max(3, min(a.warmup, 5))  # at least 3 warm-up iterations, at most 5 (bounded run)
         secs, wall = run_reference_binary(mp, sp, wu + k, threads)
         timed = secs[wu:]
         per = statistics.mean(timed)
