@@ -224,6 +224,7 @@ def run_ours(a, rank, world, local_rank):
     stream = torch.cuda.current_stream()
     ctx.set_stream(stream.cuda_stream)
     ctx.set_sinograms(frames.sinograms)
+    ctx._refresh()  # rows_with_counts of this sinogram
     ctx.init_images()
 
     mode_map = {"csc": api.BK_CSC, "atomic": api.BK_ATOMIC, "fused": api.BK_FUSED,
@@ -324,11 +325,16 @@ def run_ours(a, rank, world, local_rank):
                    "frame_tile": tuning["frame_tile"], "blocks_per_sm": tuning["blocks_per_sm"],
                    "row_visit": api.VISIT_NAMES[tuning["visit"]],
                    "l2": "inputs larger than L2 (6.2 GB matrix), no flush",
+                   # rows whose counts are zero add nothing to the update; the sorted
+                   # one-pass walks leave them out (the roofline counts the rest)
+                   "rows_with_counts": int(ctx.info.rows_with_counts),
+                   "nnz_with_counts": int(ctx.info.nnz_with_counts),
                    "parallelism": "replicas" if world > 1 else "single"},
         "hbm_gbs": round(total_bytes / (ms_per_step / 1e3) / 1e9, 1),
         # the same iteration against the two-pass byte count of the reference's
         # algorithm (CSR pass for calcFwProj + CSC pass for calcBkProj):
-        # 16 Z + 20 R + 24 C bytes, which the one-pass kernel does not move
+        # 16 Z + 20 R + 24 C bytes over every row, which the one-pass kernel does
+        # not move (one pass, and only the rows with counts)
         "two_pass_formula": {
             "bytes_per_iteration": two_pass_bytes(ctx.nnz, ctx.n_rows, ctx.n_cols),
             "achieved_gbs": round(two_pass_bytes(ctx.nnz, ctx.n_rows, ctx.n_cols)

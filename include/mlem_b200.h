@@ -95,6 +95,10 @@ typedef struct {
     uint32_t max_col_len;
     uint32_t max_row_len;
     uint64_t device_bytes; /* device memory held by the context */
+    uint64_t nnz_with_counts;  /* elements of the rows with a nonzero count in some frame of the
+                                  current sinograms (0 before mlem_set_sinograms) */
+    uint32_t rows_with_counts; /* those rows: the rest have calcCorrel 0 in every frame and are
+                                  not walked by the one-pass iteration with a sorted visit */
 } mlem_info;
 
 /* Launch configuration chosen by the autotuner (or set by the caller).

@@ -15,7 +15,8 @@ class MlemInfo(ctypes.Structure):
                 ("nnz", ctypes.c_uint64), ("n_frames", ctypes.c_uint32),
                 ("flags", ctypes.c_uint32), ("device", ctypes.c_int), ("has_csc", ctypes.c_int),
                 ("max_col_len", ctypes.c_uint32), ("max_row_len", ctypes.c_uint32),
-                ("device_bytes", ctypes.c_uint64)]
+                ("device_bytes", ctypes.c_uint64), ("nnz_with_counts", ctypes.c_uint64),
+                ("rows_with_counts", ctypes.c_uint32)]
 
 
 class MlemTuning(ctypes.Structure):

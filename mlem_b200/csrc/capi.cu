@@ -413,6 +413,7 @@ void free_frames(mlem_ctx* c) {
     c->stats_scratch = nullptr; c->inits_dev = nullptr; c->f_long = nullptr;
     c->B = c->Bp = 0;
     c->images_ready = false;
+    c->act_ready = false;
 }
 
 int alloc_frames(mlem_ctx* c, uint32_t B) {
@@ -469,6 +470,55 @@ int download_images(mlem_ctx* c, float* host) {
     CK(c, deinterleave_f32(c->x, st, c->C, c->B, c->Bp, c->bricked ? c->perm : nullptr, c->stream));
     CK(c, cudaMemcpyAsync(host, st, (size_t)c->C * c->B * 4, cudaMemcpyDeviceToHost, c->stream));
     return MLEM_OK;
+}
+
+// The one-pass iteration's sorted visiting list without the rows whose counts
+// are zero in every frame (active_rows_build), rebuilt whenever the
+// sinograms change.  Contexts without a row order and the bit-exact mode
+// keep every row; so does a context with no room for the list.  read_back:
+// wait for the list and record its size (mlem_info.rows_with_counts).
+int build_active_list(mlem_ctx* c, bool read_back) {
+    c->act_ready = false;
+    if (!c->row_order || (c->flags & MLEM_FLAG_EXACT) || c->R == 0 || c->R > 0x7fffffffu)
+        return MLEM_OK;
+    if (!c->act_tmp) {
+        const size_t tb = active_rows_tmp_bytes(c->R);
+        int s = MLEM_OK;
+        if (!c->act_order) s = dev_alloc(c, &c->act_order, c->R);
+        if (s == MLEM_OK && !c->act_ranges) s = dev_alloc(c, &c->act_ranges, c->R);
+        if (s == MLEM_OK && !c->act_flags) s = dev_alloc(c, &c->act_flags, c->R);
+        if (s == MLEM_OK && !c->act_n) s = dev_alloc(c, &c->act_n, 1);
+        if (s == MLEM_OK && !c->act_z) s = dev_alloc(c, &c->act_z, 1);
+        if (s == MLEM_OK) s = dev_alloc(c, &c->act_tmp, tb);
+        if (s != MLEM_OK) {  // no room: every row stays in the walk
+            c->err.clear();
+            return MLEM_OK;
+        }
+        c->act_tmp_bytes = tb;
+    }
+    CK(c, active_rows_build(csr_view(c), c->sino, c->Bp, c->act_flags, c->act_tmp,
+                            c->act_tmp_bytes, c->act_order, c->act_ranges, c->act_n, c->act_z,
+                            c->stream));
+    if (read_back) {
+        uint32_t n = 0;
+        unsigned long long z = 0;
+        CK(c, cudaMemcpyAsync(&n, c->act_n, 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(c, cudaMemcpyAsync(&z, c->act_z, 8, cudaMemcpyDeviceToHost, c->stream));
+        CK(c, cudaStreamSynchronize(c->stream));
+        c->act_rows = n;
+        c->act_nnz = z;
+    }
+    c->act_ready = true;
+    return MLEM_OK;
+}
+
+// A captured iteration holds the list or the full visiting order: capture
+// again when that changes (not when the list is only rebuilt in place).
+int build_active(mlem_ctx* c, bool read_back) {
+    const bool was = c->act_ready;
+    const int s = build_active_list(c, read_back);
+    if (c->act_ready != was) c->graph_dirty = true;
+    return s;
 }
 
 // ---------------------------------------------------------------------------
@@ -598,15 +648,22 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                     TRY(mark(c, pe, 2));
                     break;
                 }
-                if (c->n_long) {
-                    // the long rows are cut into segments for their own kernels
+                {
+                    // sorted visits walk only the rows with counts (their list is
+                    // rebuilt with every new sinogram); the long rows are cut into
+                    // segments for their own kernels
                     SparseView v = csr;
-                    v.long_len = kLongRowElems;
+                    if (c->act_ready && t.visit != MLEM_VISIT_FILE) {
+                        v.order = c->act_order;
+                        v.vrange = c->act_ranges;
+                        v.n_dev = c->act_n;
+                    }
+                    if (c->n_long) v.long_len = kLongRowElems;
                     TRY(fused_pass(c, t, v, st));
-                    CK(c, long_rows_pass(csr, c->long_segs, c->n_long_segs, c->n_long, c->x, Bp,
-                                         t.frame_tile, c->sino, c->f_long, c->update, c->n_sm, st));
-                } else {
-                    TRY(fused_pass(c, t, csr, st));
+                    if (c->n_long)
+                        CK(c, long_rows_pass(csr, c->long_segs, c->n_long_segs, c->n_long, c->x,
+                                             Bp, t.frame_tile, c->sino, c->f_long, c->update,
+                                             c->n_sm, st));
                 }
                 TRY(mark(c, pe, 1));
                 TRY(mark(c, pe, 2));
@@ -657,8 +714,13 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
 
 namespace mlem {
 void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* bytes,
-                     int* launches) {
-    const double R = c->R, C = c->C, Z = (double)c->Z, B = c->B;
+                     int* launches, bool active_rows) {
+    const double C = c->C, B = c->B;
+    // the one-pass sorted walk visits only the rows with counts
+    const bool act = active_rows && c->act_ready && bk_mode == MLEM_BK_FUSED &&
+                     c->n_subsets == 1 && !(c->flags & MLEM_FLAG_EXACT);
+    const double R = act ? (double)c->act_rows : (double)c->R;
+    const double Z = act ? (double)c->act_nnz : (double)c->Z;
     const bool exact = (c->flags & MLEM_FLAG_EXACT) != 0;
     const int mode = exact ? MLEM_BK_CSC : bk_mode;
     const double tiles = exact ? 1.0 : (double)(c->Bp / (uint32_t)frame_tile);
@@ -731,7 +793,8 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
 namespace {
 
 void phase_bytes(const mlem_ctx* c, double* bytes, int* launches) {
-    phase_bytes_for(c, c->tuning.bk_mode, c->tuning.frame_tile, bytes, launches);
+    phase_bytes_for(c, c->tuning.bk_mode, c->tuning.frame_tile, bytes, launches,
+                    c->tuning.visit != MLEM_VISIT_FILE);
 }
 
 }  // namespace
@@ -1145,7 +1208,8 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->sub_norm,
                     (void*)c->sub_file, (void*)c->sub_file_ranges, (void*)c->sub_sorted,
                     (void*)c->sub_sorted_ranges, (void*)c->mirror_lut, (void*)c->mirror_vox,
-                    (void*)c->f_mirror_d})
+                    (void*)c->f_mirror_d, (void*)c->act_order, (void*)c->act_ranges,
+                    (void*)c->act_flags, (void*)c->act_tmp, (void*)c->act_n, (void*)c->act_z})
         dev_free(p);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -1164,6 +1228,8 @@ int mlem_get_info(const mlem_ctx* c, mlem_info* out) {
     out->max_col_len = c->max_col_len;
     out->max_row_len = c->max_row_len;
     out->device_bytes = c->device_bytes;
+    out->nnz_with_counts = c->act_nnz;
+    out->rows_with_counts = c->act_rows;
     return MLEM_OK;
 }
 
@@ -1343,6 +1409,7 @@ int mlem_set_sinograms(mlem_ctx* c, const int32_t* sino, uint32_t B) {
         c->sumin[b] = s;
     }
     TRY(upload_frames<int32_t>(c, sino, c->sino, c->R));
+    TRY(build_active(c, true));
     CK(c, cudaStreamSynchronize(c->stream));
     c->images_ready = false;
     return MLEM_OK;
@@ -1421,6 +1488,7 @@ int mlem_step_host(mlem_ctx* c, const int32_t* sino, float* images, uint32_t B) 
     TRY(set_device(c));
     if (c->B != B) TRY(alloc_frames(c, B));
     TRY(upload_frames<int32_t>(c, sino, c->sino, c->R));
+    TRY(build_active(c, false));
     TRY(upload_frames<float>(c, images, c->x, c->C));
     c->images_ready = true;
     if (c->tuning.bk_mode == MLEM_BK_REGION && !(c->flags & MLEM_FLAG_EXACT))

@@ -47,6 +47,20 @@ struct mlem_ctx {
     // entry and exit voxels next to each other.  Null with MLEM_FLAG_NO_ROW_ORDER.
     uint32_t* row_order = nullptr;
     ulonglong2* row_ranges = nullptr;  // element range of each visited row (row_ranges_build)
+    // The sorted visiting list without the rows whose counts are zero in every
+    // frame, rebuilt on the device whenever the sinograms change
+    // (active_rows_build); the one-pass iteration walks it.  act_rows and
+    // act_nnz are read back by mlem_set_sinograms.
+    uint32_t* act_order = nullptr;
+    ulonglong2* act_ranges = nullptr;
+    uint8_t* act_flags = nullptr;
+    uint8_t* act_tmp = nullptr;
+    size_t act_tmp_bytes = 0;
+    uint32_t* act_n = nullptr;
+    unsigned long long* act_z = nullptr;
+    bool act_ready = false;
+    uint32_t act_rows = 0;
+    uint64_t act_nnz = 0;
     unsigned int* counter = nullptr;  // work counter of the dynamically scheduled kernels
 
     // Rows longer than kLongRowElems, cut into segments (k_long.cu) for the
@@ -136,8 +150,10 @@ struct PhaseEvents {
 SparseView csr_view(const mlem_ctx* c);
 void dev_free(void* p);
 // Algorithmic bytes and kernel launches of one iteration, per phase.
+// active_rows: the context's one-pass sorted walk, which visits only the
+// rows with counts (the batch kernels visit every row).
 void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* bytes,
-                     int* launches);
+                     int* launches, bool active_rows = false);
 // Room for the image statistics of n iterations.
 int ensure_history(mlem_ctx* c, int n);
 

@@ -132,14 +132,15 @@ __global__ void __launch_bounds__(1024, 1) k_fused_chunked(SparseView csr,
                                                                      unsigned int* __restrict__ counter) {
     __shared__ uint32_t s_chunk;
     const uint64_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const uint64_t nchunks = ((uint64_t)csr.n + chunk - 1) / chunk;
     for (;;) {
         if (threadIdx.x == 0) s_chunk = atomicAdd(counter, 1u);
         __syncthreads();
         const uint64_t ci = s_chunk;
         __syncthreads();  // s_chunk is rewritten by the next grab
-        if (ci >= nchunks) return;  // block-uniform
-        const uint64_t r0 = ci * chunk, r1 = r0 + chunk < csr.n ? r0 + chunk : csr.n;
+        // re-read per chunk (a cached load) rather than held in a register
+        const uint64_t n = visit_count(csr);
+        if (ci >= (n + chunk - 1) / chunk) return;  // block-uniform
+        const uint64_t r0 = ci * chunk, r1 = r0 + chunk < n ? r0 + chunk : n;
 #pragma unroll 1
         for (uint32_t f0 = 0; f0 < B; f0 += BT)
             fused_row_range<32, BT, true>(csr, x, B, f0, sino, u, r0, r1, warp, nwarps);

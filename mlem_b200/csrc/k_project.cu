@@ -152,7 +152,7 @@ __global__ void __launch_bounds__(256) k_fused_row(SparseView csr, const float* 
                                                    float* __restrict__ u) {
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
-    fused_row_range<G, BT, SORTED>(csr, x, B, f0, sino, u, 0, csr.n, warp, nwarps);
+    fused_row_range<G, BT, SORTED>(csr, x, B, f0, sino, u, 0, visit_count(csr), warp, nwarps);
 }
 
 

@@ -37,14 +37,15 @@ __global__ void __launch_bounds__(kStagedThreads, 4) k_fused_staged(SparseView c
     const uint32_t warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
     const uint2* stages = reinterpret_cast<const uint2*>(s_stage) + (size_t)warp * kStages * kStageCap;
     const uint32_t sa = (uint32_t)__cvta_generic_to_shared(stages);
-    const uint64_t nchunks = ((uint64_t)csr.n + chunk - 1) / chunk;
     for (;;) {
         if (threadIdx.x == 0) s_chunk = atomicAdd(counter, 1u);
         __syncthreads();
         const uint64_t ci = s_chunk;
         __syncthreads();  // s_chunk is rewritten by the next grab
-        if (ci >= nchunks) return;  // block-uniform
-        const uint64_t r0 = ci * chunk, r1 = r0 + chunk < csr.n ? r0 + chunk : csr.n;
+        // re-read per chunk (a cached load) rather than held in a register
+        const uint64_t n = visit_count(csr);
+        if (ci >= (n + chunk - 1) / chunk) return;  // block-uniform
+        const uint64_t r0 = ci * chunk, r1 = r0 + chunk < n ? r0 + chunk : n;
 #pragma unroll 1
         for (uint32_t f0 = 0; f0 < B; f0 += BT)
             staged_walk<BT, kStages>(csr, x, B, f0, sino, u, r0 + warp, r1, nwarps, stages, sa);

@@ -32,6 +32,10 @@ struct SparseView {
     // The one-pass row walks treat a row with more elements as empty: it is
     // left to the long-row kernels (k_long.cu).  Every other kernel ignores it.
     uint64_t long_len = ~0ull;
+    // When non-null, the one-pass walks (k_fused_row, k_fused_chunked,
+    // k_fused_staged) visit *n_dev positions of order/vrange instead of n: a
+    // visiting list built on the device (active_rows_build), n its capacity.
+    const uint32_t* n_dev = nullptr;
 };
 
 // Row index of visiting position v.
@@ -229,6 +233,17 @@ cudaError_t row_order_build(const SparseView& csr, uint32_t C, uint32_t* order, 
 // vrange[k] = {ptr[order[k]], ptr[order[k] + 1]} for k < csr.n.
 cudaError_t row_ranges_build(const SparseView& csr, const uint32_t* order, ulonglong2* vrange,
                              cudaStream_t st);
+// The sorted visiting list (csr.order, csr.vrange, csr.n < 2^31) without the
+// rows whose counts are zero in all Bp frames of sino ([R][Bp]): their
+// calcCorrel is 0 in every frame, so they add nothing to the update and their
+// forward sums are never used.  Writes act_order / act_ranges (csr.n
+// capacity), *act_n = rows kept, *act_z = their elements; flags: csr.n
+// bytes; tmp: active_rows_tmp_bytes(csr.n) bytes.
+size_t active_rows_tmp_bytes(uint32_t n);
+cudaError_t active_rows_build(const SparseView& csr, const int32_t* sino, uint32_t Bp,
+                              uint8_t* flags, void* tmp, size_t tmp_bytes, uint32_t* act_order,
+                              ulonglong2* act_ranges, uint32_t* act_n, unsigned long long* act_z,
+                              cudaStream_t st);
 
 // ---- matrix validation: every column < C and offsets non-decreasing ------
 cudaError_t validate_csr(const SparseView& csr, uint32_t C, unsigned int* bad_flag,

@@ -74,6 +74,12 @@ __device__ __forceinline__ void ld_counts(const int32_t* __restrict__ p, int32_t
     }
 }
 
+// Visiting positions of a one-pass walk: *csr.n_dev for a device-built list
+// (rows with counts), else csr.n.
+__device__ __forceinline__ uint64_t visit_count(const SparseView& csr) {
+    return csr.n_dev ? (uint64_t)__ldg(csr.n_dev) : (uint64_t)csr.n;
+}
+
 // L2 prefetch of the bytes [p, p + bytes) rounded out to 16-byte bounds (at
 // most 64 KiB): a hint -- nothing completes or waits on it.  The caller keeps
 // the rounded range inside the allocation (the element arrays carry a spare

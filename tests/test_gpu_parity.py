@@ -400,3 +400,52 @@ def test_fused_update_d_matches_two_step(golden, flags, frames, long_row):
         ctx.fused_update_d(x.data_ptr(), s.data_ptr(), u1.data_ptr(), frames, st)
         torch.cuda.synchronize()
         assert ob.rel_l2(u1.cpu().numpy(), u2.cpu().numpy()) <= 1e-5
+
+
+@pytest.mark.parametrize("visit,bps", [(api.VISIT_SORTED, 8), (api.VISIT_SORTED_CHUNKED, 4),
+                                       (api.VISIT_SORTED_STAGED, 4)])
+def test_rows_without_counts_are_skipped(golden, visit, bps):
+    """Rows whose counts are zero in every frame add nothing to the update: the
+    sorted one-pass walks leave them out, and the list follows new sinograms,
+    through the captured graph and through mlem_step_host."""
+    m, sino, _, _, _ = golden.case("plain_small_it10")
+    rng = np.random.default_rng(5)
+    B = 3
+    lens = np.diff(np.concatenate([[0], np.asarray(m.row_end, np.int64)]))
+    sinos = np.stack([rng.permutation(sino) for _ in range(B)]).astype(np.int32)
+    dead = rng.random(m.n_rows) < 0.5
+    sinos[:, dead] = 0
+    with api.Context.from_matrix(m) as ctx:
+        ctx.set_sinograms(sinos)
+        ctx._refresh()
+        live = (sinos != 0).any(axis=0)
+        assert ctx.info.rows_with_counts == int(live.sum())
+        assert ctx.info.nnz_with_counts == int(lens[live].sum())
+        ctx.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=4, blocks_per_sm=bps, visit=visit)
+        for it in range(2):
+            ctx.init_images()
+            ctx.iterate(6)
+            got = ctx.get_images()
+            for b in range(B):
+                want, _ = ob.mlem(m, sinos[b], 6)
+                assert ob.rel_l2(got[b], want) <= TOL_MLEM, (it, b)
+            # other rows with counts, same frame count: the list is rebuilt in place
+            sinos = sinos.copy()
+            sinos[:, ~dead] = 0
+            sinos[:, dead] = rng.poisson(30, (B, int(dead.sum())))
+            ctx.set_sinograms(sinos)
+        x0 = np.full((B, m.n_cols), 0.5, np.float32)
+        x = x0.copy()
+        ctx.step_host(sinos, x)
+        for b in range(B):
+            want, _ = ob.mlem(m, sinos[b], 1, start_image=x0[b])
+            assert ob.rel_l2(x[b], want) <= TOL_MLEM, b
+        zero = np.zeros_like(sinos)  # no row left: the walk visits nothing
+        ctx.set_sinograms(zero)
+        ctx._refresh()
+        assert ctx.info.rows_with_counts == 0
+        x = x0.copy()
+        ctx.step_host(zero, x)
+        for b in range(B):
+            want, _ = ob.mlem(m, zero[b], 1, start_image=x0[b])
+            assert x[b].tobytes() == want.tobytes()
