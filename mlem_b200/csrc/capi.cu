@@ -1410,6 +1410,7 @@ int mlem_set_sinograms(mlem_ctx* c, const int32_t* sino, uint32_t B) {
     }
     TRY(upload_frames<int32_t>(c, sino, c->sino, c->R));
     TRY(build_active(c, true));
+    ++c->sino_gen;
     CK(c, cudaStreamSynchronize(c->stream));
     c->images_ready = false;
     return MLEM_OK;
@@ -1489,6 +1490,7 @@ int mlem_step_host(mlem_ctx* c, const int32_t* sino, float* images, uint32_t B) 
     if (c->B != B) TRY(alloc_frames(c, B));
     TRY(upload_frames<int32_t>(c, sino, c->sino, c->R));
     TRY(build_active(c, false));
+    ++c->sino_gen;
     TRY(upload_frames<float>(c, images, c->x, c->C));
     c->images_ready = true;
     if (c->tuning.bk_mode == MLEM_BK_REGION && !(c->flags & MLEM_FLAG_EXACT))

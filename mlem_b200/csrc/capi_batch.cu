@@ -28,6 +28,13 @@ struct mlem_batch {
     // Element prefix of each matrix in file order and in sorted order (empty
     // without a row order), for cutting items of equal cost.
     std::vector<std::vector<uint64_t>> pre_file, pre_sorted;
+    // Per context, its sorted list of the rows with counts (ctx act_order,
+    // rebuilt with each sinogram): the element prefix over it, its length, and
+    // the sinogram upload it was read for.  The sorted visits walk it.
+    std::vector<std::vector<uint64_t>> pre_active;
+    std::vector<uint32_t> n_active;
+    std::vector<char> has_active;
+    std::vector<uint64_t> gen_seen;
     int policy = MLEM_BATCH_INTERLEAVED;
     int visit = MLEM_VISIT_FILE;
     int tile = 0;  // frames per pass of every context without a tile of its own
@@ -121,6 +128,15 @@ int batch_default_tile(const mlem_batch* b) {
 int eff_tile(const mlem_batch* b, size_t i) { return b->tiles[i] ? b->tiles[i] : b->tile; }
 int eff_visit(const mlem_batch* b, size_t i) { return b->visits[i] >= 0 ? b->visits[i] : b->visit; }
 
+// Context i's sorted visit walks only its rows with counts (as its own
+// one-pass iteration does); its visiting positions are then [0, n_active).
+bool uses_active(const mlem_batch* b, size_t i) {
+    return b->has_active[i] && eff_visit(b, i) != MLEM_VISIT_FILE;
+}
+uint32_t rows_of(const mlem_batch* b, size_t i) {
+    return uses_active(b, i) ? b->n_active[i] : b->ctx[i]->R;
+}
+
 // Per-group counters sit a cache sector apart.  Groups are distinct (tile,
 // visit) pairs: at most 5 tiles x 3 visits.
 constexpr uint32_t kCounterStride = 8;
@@ -133,7 +149,9 @@ static_assert(5 * 3 <= kMaxGroups, "one counter per (frame tile, row visit) grou
 double item_cost(const mlem_batch* b, size_t i, uint32_t r0, uint32_t r1) {
     const mlem_ctx* c = b->ctx[i];
     const std::vector<uint64_t>& pre =
-        (eff_visit(b, i) != MLEM_VISIT_FILE && !b->pre_sorted[i].empty()) ? b->pre_sorted[i] : b->pre_file[i];
+        uses_active(b, i) ? b->pre_active[i]
+        : (eff_visit(b, i) != MLEM_VISIT_FILE && !b->pre_sorted[i].empty()) ? b->pre_sorted[i]
+                                                                             : b->pre_file[i];
     const double nnz = (double)(pre[r1] - pre[r0]);
     const double passes = (double)(c->Bp / (uint32_t)eff_tile(b, i));
     return nnz * (8.0 * passes + 8.0 * c->Bp) + (double)(r1 - r0) * (16.0 + 8.0 * c->Bp);
@@ -159,10 +177,10 @@ bool build_groups(mlem_batch* b) {
         }
         BatchTable& t_ = it->table;
         t_.mats[t_.n] = b->table.mats[i];
-        t_.row_base[t_.n + 1] = t_.row_base[t_.n] + b->ctx[i]->R;
+        t_.row_base[t_.n + 1] = t_.row_base[t_.n] + rows_of(b, i);
         ++t_.n;
         it->ctx_of.push_back(i);
-        it->cost += item_cost(b, i, 0, b->ctx[i]->R);
+        it->cost += item_cost(b, i, 0, rows_of(b, i));
     }
     std::stable_sort(gs.begin(), gs.end(), [](const mlem_batch::Group& a, const mlem_batch::Group& c) {
         return a.cost > c.cost;
@@ -178,6 +196,32 @@ bool build_groups(mlem_batch* b) {
         }
     b->groups = std::move(gs);
     return !same;
+}
+
+// Context i's list of rows with counts, read from the device after a
+// sinogram upload, and the element prefix over it (for cutting items).
+int read_active(mlem_batch* b, size_t i) {
+    mlem_ctx* c = b->ctx[i];
+    b->has_active[i] = 0;
+    b->n_active[i] = 0;
+    b->pre_active[i].clear();
+    if (!c->act_ready || !c->row_order) return MLEM_OK;
+    uint32_t n = 0;
+    BCK(b, cudaMemcpyAsync(&n, c->act_n, 4, cudaMemcpyDeviceToHost, c->stream));
+    BCK(b, cudaStreamSynchronize(c->stream));
+    std::vector<uint32_t> ord(n);
+    if (n) BCK(b, cudaMemcpyAsync(ord.data(), c->act_order, (size_t)n * 4, cudaMemcpyDeviceToHost,
+                                  c->stream));
+    BCK(b, cudaStreamSynchronize(c->stream));
+    const std::vector<uint64_t>& pf = b->pre_file[i];
+    std::vector<uint64_t>& pa = b->pre_active[i];
+    pa.resize((size_t)n + 1);
+    pa[0] = 0;
+    for (uint32_t k = 0; k < n; ++k) pa[k + 1] = pa[k] + (pf[ord[k] + 1] - pf[ord[k]]);
+    c->act_rows = n;
+    b->n_active[i] = n;
+    b->has_active[i] = 1;
+    return MLEM_OK;
 }
 
 // Cut the rows of every group's matrices into items of about group total /
@@ -196,7 +240,7 @@ int batch_schedule(mlem_batch* b) {
     for (auto& g : b->groups) {
         const size_t n = g.ctx_of.size();
         std::vector<double> total(n, 0.0);
-        for (size_t j = 0; j < n; ++j) total[j] = item_cost(b, g.ctx_of[j], 0, b->ctx[g.ctx_of[j]]->R);
+        for (size_t j = 0; j < n; ++j) total[j] = item_cost(b, g.ctx_of[j], 0, rows_of(b, g.ctx_of[j]));
         const double target = std::max(g.cost / (resident * (double)b->items_per_block), 1.0);
         std::vector<size_t> order(n);
         for (size_t j = 0; j < n; ++j) order[j] = j;
@@ -206,7 +250,7 @@ int batch_schedule(mlem_batch* b) {
         std::vector<std::pair<double, BatchItem>> tail;
         for (size_t j : order) {
             const size_t i = g.ctx_of[j];
-            const uint32_t R = b->ctx[i]->R;
+            const uint32_t R = rows_of(b, i);
             uint32_t r0 = 0;
             while (r0 < R) {
                 uint32_t lo = r0 + 1, hi = R;  // smallest r1 whose cost reaches the target
@@ -264,15 +308,25 @@ int batch_refresh(mlem_batch* b, int chunk) {
             return bfail(b, MLEM_ERR_STATE, "context %zu: ordered subsets do not run in a batch", i);
         if (c->stream != b->stream) BCK(b, cudaStreamSynchronize(c->stream));
         TRY(bctx(b, c, ensure_history(c, chunk)));
+        if (c->sino_gen != b->gen_seen[i]) {  // new sinograms: another list of rows with counts
+            TRY(read_active(b, i));
+            b->gen_seen[i] = c->sino_gen;
+            reschedule = true;
+            b->graph_dirty = true;
+        }
         if (t.mats[i].Bp != c->Bp) reschedule = true;
         SparseView v = csr_view(c);
         if (c->n_long) v.long_len = kLongRowElems;  // long rows: segments in their own kernels
         if (eff_visit(b, i) == MLEM_VISIT_FILE) {
             v.order = nullptr;
             v.vrange = nullptr;
+        } else if (uses_active(b, i)) {
+            v.order = c->act_order;
+            v.vrange = c->act_ranges;
+            v.n = b->n_active[i];
         }
         t.mats[i] = BatchMat{v, c->x, c->sino, c->update, c->Bp, 0u};
-        t.row_base[i + 1] = t.row_base[i] + c->R;
+        t.row_base[i + 1] = t.row_base[i] + rows_of(b, i);
         for (const void* p : {(const void*)c->x, (const void*)c->sino, (const void*)c->update,
                               (const void*)c->norm, (const void*)c->stats_scratch,
                               (const void*)c->stats_slot, (const void*)c->hist_sums,
@@ -438,6 +492,10 @@ int mlem_batch_create(mlem_batch** out, mlem_ctx* const* ctxs, uint32_t n_ctx) {
         return bail(bfail(b, MLEM_ERR_CUDA, "cudaSetDevice(%d) failed", b->device));
     b->pre_file.resize(n_ctx);
     b->pre_sorted.resize(n_ctx);
+    b->pre_active.resize(n_ctx);
+    b->n_active.assign(n_ctx, 0);
+    b->has_active.assign(n_ctx, 0);
+    b->gen_seen.assign(n_ctx, ~0ull);  // read every context's list at the first refresh
     for (uint32_t i = 0; i < n_ctx; ++i) {
         mlem_ctx* c = ctxs[i];
         std::vector<uint64_t>& pre = b->pre_file[i];
@@ -663,7 +721,7 @@ int mlem_batch_autotune(mlem_batch* b, double* ms_per_iter) {
         std::vector<size_t> order(b->ctx.size());
         for (size_t i = 0; i < order.size(); ++i) order[i] = i;
         std::vector<double> cost(b->ctx.size());
-        for (size_t i = 0; i < cost.size(); ++i) cost[i] = item_cost(b, i, 0, b->ctx[i]->R);
+        for (size_t i = 0; i < cost.size(); ++i) cost[i] = item_cost(b, i, 0, rows_of(b, i));
         std::stable_sort(order.begin(), order.end(), [&](size_t a, size_t c) { return cost[a] > cost[c]; });
         for (size_t i : order)
             for (int t : {16, 8, 4, 2, 1}) {
@@ -775,7 +833,7 @@ int mlem_batch_profile(mlem_batch* b, int n, double* ms, double* bytes, int* lau
     for (size_t i = 0; i < b->ctx.size(); ++i) {
         double pb[MLEM_N_PHASES];
         int pl[MLEM_N_PHASES];
-        phase_bytes_for(b->ctx[i], MLEM_BK_FUSED, eff_tile(b, i), pb, pl);
+        phase_bytes_for(b->ctx[i], MLEM_BK_FUSED, eff_tile(b, i), pb, pl, uses_active(b, i));
         for (int p = 0; p < MLEM_N_PHASES; ++p) {
             tb[p] += pb[p];
             tl[p] += pl[p];

@@ -61,6 +61,7 @@ struct mlem_ctx {
     bool act_ready = false;
     uint32_t act_rows = 0;
     uint64_t act_nnz = 0;
+    uint64_t sino_gen = 0;  // counts sinogram uploads (a batch rebuilds its items on change)
     unsigned int* counter = nullptr;  // work counter of the dynamically scheduled kernels
 
     // Rows longer than kLongRowElems, cut into segments (k_long.cu) for the

@@ -273,3 +273,31 @@ def test_batch_rejects_bad_input(members):
     finally:
         for c in ctxs + [exact, bare, unsorted]:
             c.close()
+
+
+@pytest.mark.parametrize("policy,visit", [(IT, SORTED), (IT, STAGED), (IL, SORTED)])
+def test_batch_skips_rows_without_counts(members, policy, visit):
+    """Sorted visits walk each context's rows with counts only; new sinograms
+    with the same frame counts (the list rebuilt in place) are picked up."""
+    ctxs = _contexts(members)
+    rng = np.random.default_rng(21)
+    try:
+        with api.Batch(ctxs) as b:
+            b.set_schedule(policy, 4, 4, 0, visit)
+            for it in range(2):
+                sinos = []
+                for c, (m, s, _) in zip(ctxs, members):
+                    s = s.copy()
+                    s[:, rng.random(m.n_rows) < 0.5] = 0
+                    c.set_sinograms(s)
+                    c.init_images()
+                    sinos.append(s)
+                b.iterate(ITERS)
+                for c, (m, _, _), s in zip(ctxs, members, sinos):
+                    got = c.get_images()
+                    for f in range(s.shape[0]):
+                        want, _ = ob.mlem(m, s[f], ITERS)
+                        assert ob.rel_l2(got[f], want) <= TOL_MLEM, (it, m.n_rows, f)
+    finally:
+        for c in ctxs:
+            c.close()
