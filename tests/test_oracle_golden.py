@@ -68,3 +68,36 @@ def test_partition_matches_reference_rule(golden):
         assert np.all(s[1:] == e[:-1])
         nnz = [int(m.row_ptr()[b] - m.row_ptr()[a]) for a, b in zip(s, e)]
         assert sum(nnz) == m.nnz
+
+
+@pytest.mark.parametrize("name", ["plain_small_it10", "edge_it7"])
+def test_rows_without_counts_change_nothing(golden, name):
+    """The restated reference iteration gives the same image, bit for bit, when
+    the rows whose count is zero are emptied: their calcCorrel is 0, so they
+    only add +0 to the update (the fact the GPU walks rely on to leave them out)."""
+    from mlem_b200 import formats
+
+    m, sino, _, _, _ = golden.case(name)
+    rng = np.random.default_rng(3)
+    sino = sino.copy()
+    sino[rng.random(m.n_rows) < 0.4] = 0
+    keep = sino != 0
+    lens = np.diff(np.concatenate([[0], np.asarray(m.row_end, np.int64)]))
+    starts = np.concatenate([[0], np.asarray(m.row_end, np.int64)[:-1]])
+    idx = np.concatenate([np.arange(s, s + n) for s, n in zip(starts[keep], lens[keep])]) \
+        if keep.any() else np.zeros(0, np.int64)
+    kept_lens = np.where(keep, lens, 0)
+    m2 = formats.Csr4(m.n_rows, m.n_cols, np.cumsum(kept_lens).astype(np.uint64),
+                      np.ascontiguousarray(np.asarray(m.elems)[idx]))
+    # calcColumnSums stays the full matrix's (it does not depend on the counts);
+    # each iteration's update must match bit for bit
+    norm = ob.column_sums(m)
+    x = np.full(m.n_cols, ob.init_value(norm, sino), np.float32)
+    y = x.copy()
+    for _ in range(5):
+        ux = ob.bkproj(m, ob.correl(ob.fwproj(m, x), sino))
+        uy = ob.bkproj(m2, ob.correl(ob.fwproj(m2, y), sino))
+        assert ux.tobytes() == uy.tobytes()
+        x = ob.update(ux, norm, x)
+        y = ob.update(uy, norm, y)
+    assert x.tobytes() == y.tobytes()
