@@ -479,7 +479,9 @@ int download_images(mlem_ctx* c, float* host) {
 // wait for the list and record its size (mlem_info.rows_with_counts).
 int build_active_list(mlem_ctx* c, bool read_back) {
     c->act_ready = false;
-    if (!c->row_order || (c->flags & MLEM_FLAG_EXACT) || c->R == 0 || c->R > 0x7fffffffu)
+    // the mirrored kernels walk stored rows, whose counts are the mirrored rows'
+    if (!c->row_order || (c->flags & MLEM_FLAG_EXACT) || c->mirrored || c->R == 0 ||
+        c->R > 0x7fffffffu)
         return MLEM_OK;
     if (!c->act_tmp) {
         const size_t tb = active_rows_tmp_bytes(c->R);
