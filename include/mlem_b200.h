@@ -98,7 +98,9 @@ typedef struct {
     uint64_t nnz_with_counts;  /* elements of the rows with a nonzero count in some frame of the
                                   current sinograms (0 before mlem_set_sinograms) */
     uint32_t rows_with_counts; /* those rows: the rest have calcCorrel 0 in every frame and are
-                                  not walked by the one-pass iteration with a sorted visit */
+                                  not walked by the one-pass iteration with a sorted visit
+                                  (0 without a row order, in the bit-exact mode and with
+                                  MLEM_FLAG_MIRROR_KERNELS, which walk every row) */
 } mlem_info;
 
 /* Launch configuration chosen by the autotuner (or set by the caller).
