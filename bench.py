@@ -5,22 +5,38 @@ Workload ("plain-full"): a synthetic Siddon system matrix of 4,194,304 LORs
 x 1,048,576 voxels (128x128x64 grid, 150-250 elements per row, ~0.78e9
 elements, 6.2 GB CSR4 plus a 6.2 GB device CSC copy), one int32 Poisson
 sinogram of an 8-ellipsoid phantom at 1e9 counts, float32.  A step is one
-MLEM iteration (forward projection + correlation + back projection + update,
-plus the per-iteration image-sum census the reference prints).  The matrix
-(6.2 GB) is larger than the 126 MB L2, so no L2 flush is needed between
-steps.  The batched line ("batched-b16") runs 16 sinograms over the same
-matrix in one pass per iteration; the "uneven" line batches three matrices
-of different geometry (12, 8 and 4 sinograms) in one kernel per iteration
-(mlem_b200.uneven); the "mirrored" line reconstructs the plain-full matrix
-read as a symmetry-compressed file (three mirrors, a 50 GB full matrix) once
-expanded on the device and once with the mirrors applied in the kernels
-(mlem_b200.mirrored).
+MLEM iteration: forward projection + correlation + back projection + update,
+plus the per-iteration image-sum / zero / subnormal census the reference
+prints (seqcsr4mlem.cpp:172-185), whose sums are copied to the host.  The
+matrix (6.2 GB) is larger than the 126 MB L2, so no L2 flush is needed
+between steps.
+
+Besides the headline line, at one GPU:
+* batched: 16 sinograms over the same matrix in one pass per iteration;
+* parity_full: the full-size images after 60 iterations (the workload's
+  iteration count) against the reference's own seqcsr4mlem and against the
+  FP64 oracle -- the autotuned one-pass path, the command-line drop-in with a
+  checkpoint every 10 iterations (deterministic CSC method), and one frame of
+  the 16-frame batch; every batched frame against its own single-frame run.
+  The reference binary and the oracle run as background processes on the
+  host cores while the GPU lines are measured;
+* osem, differentiable, skewed, uneven (three matrices of different
+  geometry batched), mirrored (a symmetry-compressed matrix).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--parallelism single|shards|replicas]
+
+With N > 1 (torchrun, one process per GPU) the default is --parallelism
+shards: the rows are split into nnz-balanced blocks, one per rank, and each
+iteration computes every block's partial update in one pass and all-reduces
+the C floats once over NCCL (strong scaling: value = iterations/s of the one
+reconstruction).  --parallelism replicas gives each rank its own full-size
+LOR set instead (weak scaling, no data-path collective).
 
 Prints ONE JSON line (rank 0).  --impl reference times the reference's own
 OpenMP implementation (openmpcsr4mlem, compiled from its sources into
-oracle/_ref) on this host's cores on the same workload.
+oracle/_ref) on this host's cores on the same workload; its inputs are made
+by oracle/_bin/oracle_tool in a child process.
 """
 from __future__ import annotations
 
@@ -41,8 +57,13 @@ sys.path.insert(0, ROOT)
 
 METRIC = "MLEM iterations/s and HBM GB/s, plain vs batched B=16, at rel L2 err <=1e-4"
 UNIT = "iterations/s"
-REF_MESSUNG = os.path.join(ROOT, "oracle", "_ref", "openmpcsr4mlem_messung")
+REF_DIR = os.path.join(ROOT, "oracle", "_ref")
+REF_MESSUNG = os.path.join(REF_DIR, "openmpcsr4mlem_messung")
+REF_SEQ = os.path.join(REF_DIR, "seqcsr4mlem")
+ORACLE_TOOL = os.path.join(ROOT, "oracle", "_bin", "oracle_tool")
+CLI = os.path.join(ROOT, "mlem_b200", "bin", "mlem_b200")
 PHASES = ("project", "backproject", "update", "stats")
+TOL = 1e-4
 
 
 def parse_args():
@@ -51,6 +72,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--parallelism", choices=["auto", "single", "shards", "replicas"],
+                    default="auto", help="auto: single at N=1, shards at N>1")
     ap.add_argument("--mode", choices=["auto", "csc", "atomic", "fused", "region"], default="auto",
                     help="back-projection method; auto = autotuned")
     ap.add_argument("--visit", choices=["file", "sorted", "chunked", "staged"], default="file",
@@ -65,8 +88,11 @@ def parse_args():
                     help="skip the uneven three-geometry batch (one GPU only)")
     ap.add_argument("--no-mirrored", action="store_true",
                     help="skip the symmetry-compressed matrix, expanded vs mirrored kernels (one GPU only)")
-    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true",
+                    help="skip the host-core legs (openmpcsr4mlem timing and the full-size parity)")
+    ap.add_argument("--no-parity-full", action="store_true")
     ap.add_argument("--cpu-iters", type=int, default=3)
+    ap.add_argument("--parity-iters", type=int, default=60)
     return ap.parse_args()
 
 
@@ -128,6 +154,9 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# ---------------------------------------------------------------------------
+# shared helpers
+# ---------------------------------------------------------------------------
 def two_pass_bytes(nnz, rows, cols):
     """Algorithmic bytes of one plain iteration as two passes over the matrix:
     CSR (8R offsets + 8Z + 4C image + 4R sinogram + 4R correlation) and CSC
@@ -154,16 +183,13 @@ def committed_traffic():
     return {}
 
 
-# ---------------------------------------------------------------------------
-# CPU baseline: the reference's openmpcsr4mlem on this host
-# ---------------------------------------------------------------------------
-def write_inputs(tmpdir, row_end, elems, n_rows, n_cols, grid, sino):
-    from mlem_b200 import formats
-    mp = os.path.join(tmpdir, "matrix.csr4")
-    sp = os.path.join(tmpdir, "sino.bin")
-    formats.write_csr4(mp, n_rows, n_cols, row_end, elems, grid=grid)
-    formats.write_vector(sp, sino, "int32")
-    return mp, sp
+def workload_config(g, nnz, parallelism="single", frames=1):
+    """The workload's identity, the same in both arms (tuning lives elsewhere)."""
+    return {"workload": "plain-full", "grid": f"{g.nx}x{g.ny}x{g.nz}", "n_rows": int(g.n_rows),
+            "n_cols": int(g.n_cols), "nnz": int(nnz), "frames": frames,
+            "iterations_per_step": 1,
+            "l2": "inputs larger than L2 (6.2 GB matrix), no flush",
+            "parallelism": parallelism}
 
 
 def scratch_dir(need_bytes):
@@ -176,9 +202,38 @@ def scratch_dir(need_bytes):
     return None
 
 
+def host_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+def rel_l2(a, b):
+    import numpy as np
+    a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def sig(x):
+    return None if x is None else float(f"{x:.3g}")
+
+
+def write_csr4_and_sinos(d, row_end, elems, n_rows, n_cols, grid, sinos: dict):
+    """The CSR4 file and raw int32 sinograms of the run, for the reference's binaries."""
+    from mlem_b200 import formats
+    mp = os.path.join(d, "matrix.csr4")
+    formats.write_csr4(mp, n_rows, n_cols, row_end, elems, grid=grid)
+    paths = {}
+    for name, s in sinos.items():
+        paths[name] = os.path.join(d, f"{name}.sino")
+        formats.write_vector(paths[name], s, "int32")
+    return mp, paths
+
+
 def run_reference_binary(matrix_path, sino_path, iters, threads, timeout=900):
     """Per-iteration seconds printed by openmpcsr4mlem -DMESSUNG (iter,elapsed)."""
-    out = os.path.join(os.path.dirname(matrix_path), "image.out")
+    out = os.path.join(os.path.dirname(matrix_path), "image_omp.out")
     env = dict(os.environ, OMP_NUM_THREADS=str(threads))
     t0 = time.time()
     p = subprocess.run([REF_MESSUNG, matrix_path, sino_path, out, str(iters)], env=env,
@@ -187,20 +242,82 @@ def run_reference_binary(matrix_path, sino_path, iters, threads, timeout=900):
     if p.returncode != 0:
         raise RuntimeError(f"openmpcsr4mlem failed: {p.stderr[-500:]}")
     secs = [float(m.group(2)) for m in re.finditer(r"^(\d+),([0-9.eE+-]+)$", p.stdout, re.M)]
-    return secs, time.time() - t0
-
-
-def host_threads():
-    try:
-        return len(os.sched_getaffinity(0))
-    except AttributeError:
-        return os.cpu_count() or 1
+    return secs, time.time() - t0, out
 
 
 # ---------------------------------------------------------------------------
-# our implementation
+# full-size parity: the reference's seqcsr4mlem and the FP64 oracle on the
+# host cores, in the background while the GPU lines run
 # ---------------------------------------------------------------------------
-def run_ours(a, rank, world, local_rank):
+class ParityJobs:
+    """For each named sinogram: seqcsr4mlem (single core, the reference's
+    sequential float path) and oracle_tool f64-mlem (FP64 oracle, threads),
+    both for `iters` iterations on the same CSR4 file."""
+
+    def __init__(self, d, matrix, sinos: dict, iters, threads):
+        self.d, self.iters = d, iters
+        self.procs = {}
+        self.t0 = time.time()
+        self.error = None
+        if not (os.path.exists(REF_SEQ) and os.path.exists(ORACLE_TOOL)):
+            self.error = "oracle/_ref/seqcsr4mlem or oracle/_bin/oracle_tool is not built"
+            return
+        n = max(1, len(sinos))
+        f64_threads = max(1, (threads - n) // n)
+        self.f64_threads = f64_threads
+        for name, sp in sinos.items():
+            seq_out = os.path.join(d, f"{name}.seq.img")
+            f64_out = os.path.join(d, f"{name}.f64.img")
+            logs = [open(os.path.join(d, f"{name}.{k}.log"), "w") for k in ("seq", "f64")]
+            ps = subprocess.Popen([REF_SEQ, matrix, sp, seq_out, str(iters)], cwd=d,
+                                  stdout=logs[0], stderr=subprocess.STDOUT)
+            pf = subprocess.Popen([ORACLE_TOOL, "f64-mlem", matrix, sp, str(iters),
+                                   str(f64_threads), f64_out], cwd=d,
+                                  stdout=logs[1], stderr=subprocess.STDOUT)
+            self.procs[name] = (ps, pf, seq_out, f64_out, logs)
+
+    def collect(self, timeout=1200):
+        """{name: (seq image f32, f64 image f64)}; seconds until the last ended."""
+        import numpy as np
+        out = {}
+        deadline = time.time() + timeout
+        for name, (ps, pf, so, fo, logs) in self.procs.items():
+            for p in (ps, pf):
+                try:
+                    p.wait(timeout=max(1.0, deadline - time.time()))
+                except subprocess.TimeoutExpired:
+                    p.kill()
+                    p.wait()
+            for f in logs:
+                f.close()
+            if ps.returncode != 0 or pf.returncode != 0:
+                raise RuntimeError(f"{name}: seqcsr4mlem rc={ps.returncode}, "
+                                   f"oracle_tool rc={pf.returncode}")
+            out[name] = (np.fromfile(so, np.float32), np.fromfile(fo, np.float64))
+        return out, time.time() - self.t0
+
+
+def run_cli(d, matrix, sino, iters, chk):
+    """The command-line drop-in, as the reference's drivers are called:
+    matrix input output iterations checkpointing (default method: the
+    deterministic CSC back projection).  Returns the image and whether the
+    checkpoint pair was removed after the run, as mpicsr4mlem does."""
+    import numpy as np
+    out = os.path.join(d, "cli.img")
+    t0 = time.time()
+    p = subprocess.run([CLI, matrix, sino, out, str(iters), str(chk)], cwd=d,
+                       capture_output=True, text=True, timeout=900)
+    if p.returncode != 0:
+        raise RuntimeError(f"mlem_b200 CLI failed: {p.stderr[-300:]}")
+    clean = not (os.path.exists(os.path.join(d, "img.chkpt"))
+                 or os.path.exists(os.path.join(d, "iter.chkpt")))
+    return np.fromfile(out, np.float32), clean, time.time() - t0
+
+
+# ---------------------------------------------------------------------------
+# our implementation, one context per GPU (single, or weak-scaling replicas)
+# ---------------------------------------------------------------------------
+def run_ours(a, rank, world, local_rank, parallelism):
     import numpy as np
     import torch
 
@@ -215,7 +332,7 @@ def run_ours(a, rank, world, local_rank):
 
     w = synth.WORKLOADS["plain-full"]
     g = w.geometry
-    if world > 1:  # weak scaling: every rank reconstructs its own full-size LOR set
+    if world > 1:  # replicas: every rank reconstructs its own full-size LOR set
         g = synth.Geometry(g.nx, g.ny, g.nz, g.n_rows, g.min_count, g.max_count, seed=g.seed + 100 * rank)
     t_setup = time.time()
     ctx = api.Context.siddon(g, device=local_rank)
@@ -238,7 +355,7 @@ def run_ours(a, rank, world, local_rank):
                        blocks_per_sm=a.blocks_per_sm, visit=visit)
         tuning = ctx.tuning()
     ctx.init_images()
-    ctx.iterate(a.warmup, stats=False)
+    ctx.iterate(a.warmup)
     kernels_per_iter = ctx.kernels_per_iteration()
 
     def barrier():
@@ -246,7 +363,8 @@ def run_ours(a, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
 
-    # --- timed region: K iterations, device events on the context's stream ---
+    # --- timed region: K iterations (census sums copied to the host), device
+    # events on the context's stream ---
     clocks = ClockSampler(local_rank) if rank == 0 else None
     barrier()
     if clocks:
@@ -254,7 +372,7 @@ def run_ours(a, rank, world, local_rank):
         time.sleep(0.3)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    ctx.iterate(a.steps, stats=False)
+    sums, _, _ = ctx.iterate(a.steps)
     e1.record(stream)
     barrier()
     ms = e0.elapsed_time(e1)
@@ -267,11 +385,7 @@ def run_ours(a, rank, world, local_rank):
         ms = float(t.item())
     ms_per_step = ms / a.steps
     value = world * a.steps / (ms / 1e3)
-
-    # parity of this run's image against the FP64 projection of its phantom is
-    # covered by the tests; report the image sum as a sanity figure
     img = ctx.get_images()[0]
-    image_sum = float(img.astype(np.float64).sum())
 
     # --- end to end through the C ABI: pinned host sinogram + image in, image out ---
     sino_h = torch.from_numpy(frames.sinograms[0].copy()).pin_memory()
@@ -286,7 +400,7 @@ def run_ours(a, rank, world, local_rank):
     f1.record(stream)
     barrier()
     e2e_ms = f0.elapsed_time(f1) / k_e2e
-    e2e = {"value": world * 1e3 / e2e_ms, "unit": UNIT,
+    e2e = {"value": round(world * 1e3 / e2e_ms, 3), "unit": UNIT,
            "h2d_bytes_per_step": int(4 * ctx.n_rows + 4 * ctx.n_cols),
            "d2h_bytes_per_step": int(4 * ctx.n_cols),
            "call": "mlem_step_host (pinned host sinogram + image)"}
@@ -308,129 +422,280 @@ def run_ours(a, rank, world, local_rank):
                 "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
                 "traffic": traffic, "peak_kind": peak_kind,
                 "algorithmic_bytes_per_launch": ph_bytes[dom] / max(1, ph_launch[dom]),
-                "ms_per_launch": ph_ms[dom] / max(1, ph_launch[dom])}
+                "ms_per_launch": round(ph_ms[dom] / max(1, ph_launch[dom]), 4)}
     phases = {PHASES[p]: {"ms": round(float(ph_ms[p]), 4), "GB": round(ph_bytes[p] / 1e9, 4),
                           "GB/s": round(ph_bytes[p] / (ph_ms[p] / 1e3) / 1e9, 1) if ph_ms[p] > 0 else None,
                           "kernel": kernel_names[p], "launches": int(ph_launch[p])}
               for p in range(4)}
+    tp = two_pass_bytes(ctx.nnz, ctx.n_rows, ctx.n_cols)
 
-    line = {
+    head = {
         "metric": METRIC, "value": round(value, 3), "unit": UNIT, "n_gpus": world,
         "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(ms_per_step, 4),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded Siddon matrix, ellipsoid phantom, Poisson sinogram)",
-        "config": {"workload": "plain-full", "grid": [g.nx, g.ny, g.nz], "n_rows": ctx.n_rows,
-                   "n_cols": ctx.n_cols, "nnz": int(ctx.nnz), "frames": 1,
-                   "bk_mode": api.BK_NAMES[tuning["bk_mode"]], "group": tuning["group"],
+        "config": workload_config(g, ctx.nnz, parallelism),
+        "roofline": roofline, "e2e": e2e,
+        "gpu_launches": int(kernels_per_iter * a.steps),
+        "clocks": clk,
+    }
+    detail = {
+        "tuning": {"bk_mode": api.BK_NAMES[tuning["bk_mode"]], "group": tuning["group"],
                    "frame_tile": tuning["frame_tile"], "blocks_per_sm": tuning["blocks_per_sm"],
                    "row_visit": api.VISIT_NAMES[tuning["visit"]],
-                   "l2": "inputs larger than L2 (6.2 GB matrix), no flush",
                    # rows whose counts are zero add nothing to the update; the sorted
                    # one-pass walks leave them out (the roofline counts the rest)
                    "rows_with_counts": int(ctx.info.rows_with_counts),
-                   "nnz_with_counts": int(ctx.info.nnz_with_counts),
-                   "parallelism": "replicas" if world > 1 else "single"},
+                   "nnz_with_counts": int(ctx.info.nnz_with_counts)},
         "hbm_gbs": round(total_bytes / (ms_per_step / 1e3) / 1e9, 1),
         # the same iteration against the two-pass byte count of the reference's
         # algorithm (CSR pass for calcFwProj + CSC pass for calcBkProj):
         # 16 Z + 20 R + 24 C bytes over every row, which the one-pass kernel does
         # not move (one pass, and only the rows with counts)
-        "two_pass_formula": {
-            "bytes_per_iteration": two_pass_bytes(ctx.nnz, ctx.n_rows, ctx.n_cols),
-            "achieved_gbs": round(two_pass_bytes(ctx.nnz, ctx.n_rows, ctx.n_cols)
-                                  / (ms_per_step / 1e3) / 1e9, 1),
-            "frac": round(two_pass_bytes(ctx.nnz, ctx.n_rows, ctx.n_cols)
-                          / (ms_per_step / 1e3) / 1e9 / peak, 4)},
+        "two_pass_formula": {"bytes_per_iteration": tp,
+                             "achieved_gbs": round(tp / (ms_per_step / 1e3) / 1e9, 1),
+                             "frac": round(tp / (ms_per_step / 1e3) / 1e9 / peak, 4)},
         "iteration_roofline_frac": round(total_bytes / (ms_per_step / 1e3) / 1e9 / peak, 4),
-        "bytes_per_iteration": total_bytes,
-        "roofline": roofline, "phases": phases, "e2e": e2e,
-        "gpu_launches": int(kernels_per_iter * a.steps),
-        "clocks": clk, "image_sum": image_sum, "setup_s": {"matrix": round(t_matrix, 2)},
+        "bytes_per_iteration": total_bytes, "phases": phases,
+        "last_image_sum": float(sums[-1, 0]), "setup_s": {"matrix": round(t_matrix, 2)},
     }
+    tail = {}
 
-    # --- batched: 16 sinograms in one pass over the matrix per iteration ---
-    if not a.no_batched:
-        wb = synth.WORKLOADS["batched-b16"]
-        fb = synth.make_frames(wb, ctx.project_f64)
-        ctx.set_sinograms(fb.sinograms)
-        ctx.init_images()
-        tb = ctx.autotune()
-        ctx.init_images()
-        ctx.iterate(a.warmup, stats=False)
-        kb = max(10, a.steps // 4)
-        barrier()
-        e0.record(stream)
-        ctx.iterate(kb, stats=False)
-        e1.record(stream)
-        barrier()
-        bms = e0.elapsed_time(e1) / kb
-        bph_ms, bph_bytes, _ = ctx.profile_phases(10)
-        line["batched"] = {
-            "workload": "batched-b16", "frames": 16, "ms_per_iteration": round(bms, 4),
-            "frame_iterations_per_s": round(16 * 1e3 / bms, 2),
-            "per_frame_speedup_vs_plain": round((16 / bms) / (1 / ms_per_step), 3),
-            "hbm_gbs": round(float(bph_bytes.sum()) / (bms / 1e3) / 1e9, 1),
-            "bk_mode": api.BK_NAMES[tb["bk_mode"]], "group": tb["group"],
-            "frame_tile": tb["frame_tile"], "row_visit": api.VISIT_NAMES[tb["visit"]],
-            "phases_ms": [round(float(x), 4) for x in bph_ms],
-            "parity": batched_parity(ctx, fb.sinograms, tb, 10),
-        }
+    host_legs = rank == 0 and world == 1 and not a.no_cpu_baseline
+    wb = synth.WORKLOADS["batched-b16"]
+    fb = synth.make_frames(wb, ctx.project_f64) if not a.no_batched else None
+    # the batched frame checked against the reference binary: the one with the
+    # fewest counts (the noisiest reconstruction)
+    kf = int(np.argmin(fb.totals)) if fb is not None else None
 
-    # --- ordered subsets: 8 interleaved row subsets, the plain sinogram ---
-    if not a.no_osem:
-        n_sub = 8
-        ctx.set_sinograms(frames.sinograms)
-        ctx.init_images()
-        ctx.set_subsets(n_sub)
-        to = ctx.autotune()
-        ctx.init_images()
-        ctx.iterate(a.warmup, stats=False)
-        ko = max(10, a.steps // 2)
-        barrier()
-        e0.record(stream)
-        ctx.iterate(ko, stats=False)
-        e1.record(stream)
-        barrier()
-        oms = e0.elapsed_time(e1) / ko
-        line["osem"] = {
-            "workload": "plain-full", "subsets": n_sub, "ms_per_iteration": round(oms, 4),
-            "sub_iterations_per_s": round(n_sub * 1e3 / oms, 2),
-            "iteration_time_vs_plain": round(oms / ms_per_step, 3),
-            "frame_tile": to["frame_tile"], "group": to["group"],
-            "row_visit": api.VISIT_NAMES[to["visit"]],
-            "gpu_launches_per_iteration": int(ctx.kernels_per_iteration()),
-        }
-        ctx.set_subsets(1)
+    # --- host legs: the reference's openmpcsr4mlem timed on this host, then the
+    # full-size parity jobs started in the background ---
+    d = jobs = mpath = spaths = None
+    if host_legs:
+        need = 8 * ctx.nnz + 8 * ctx.n_rows + 12 * ctx.n_rows
+        d = scratch_dir(need)
+    try:
+        if host_legs and d is None:
+            head["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                    "sample": "unavailable: no scratch space for the CSR4 file"}
+        elif host_legs:
+            row_end, elems = ctx.csr()
+            sinos = {"plain": frames.sinograms[0]}
+            if fb is not None:
+                sinos["batched_frame"] = fb.sinograms[kf]
+            mpath, spaths = write_csr4_and_sinos(d, row_end, elems, ctx.n_rows, ctx.n_cols,
+                                                 (g.nx, g.ny, g.nz), sinos)
+            del row_end, elems
+            head["cpu_baseline"] = cpu_baseline(ctx, mpath, spaths["plain"], frames.sinograms[0],
+                                                a.cpu_iters)
+            if not a.no_parity_full:
+                jobs = ParityJobs(d, mpath, spaths, a.parity_iters, host_threads())
 
-    # --- differentiable MLEM: 10 unrolled iterations, gradient of an MSE loss ---
-    if not a.no_differentiable:
-        line["differentiable"] = differentiable_line(ctx, a, stream, barrier)
+        # --- batched: 16 sinograms in one pass over the matrix per iteration ---
+        if fb is not None:
+            ctx.set_sinograms(fb.sinograms)
+            ctx.init_images()
+            tb = ctx.autotune()
+            ctx.init_images()
+            ctx.iterate(a.warmup, stats=False)
+            kb = max(10, a.steps // 4)
+            barrier()
+            e0.record(stream)
+            ctx.iterate(kb)
+            e1.record(stream)
+            barrier()
+            bms = e0.elapsed_time(e1) / kb
+            bph_ms, bph_bytes, _ = ctx.profile_phases(10)
+            tail["batched"] = {
+                "frames": 16, "ms_per_iteration": round(bms, 4),
+                "per_frame_speedup_vs_plain": round((16 / bms) / (1 / ms_per_step), 3),
+                "frame_iterations_per_s": round(16 * 1e3 / bms, 1),
+                "hbm_gbs": round(float(bph_bytes.sum()) / (bms / 1e3) / 1e9, 1),
+                "method": f"{api.BK_NAMES[tb['bk_mode']]}/{api.VISIT_NAMES[tb['visit']]}"
+                          f"/tile{tb['frame_tile']}",
+            }
+            detail["batched_phases_ms"] = [round(float(x), 4) for x in bph_ms]
 
-    # --- a skewed matrix: the long rows run as segments (k_long.cu) ---
-    if not a.no_skewed:
-        line["skewed"] = skewed_line(a, stream, barrier)
+        # --- full-size parity, GPU side (the host jobs run meanwhile) ---
+        if jobs is not None and jobs.error is None:
+            pf = parity_gpu_side(ctx, a, tuning, frames.sinograms, fb, tb if fb is not None else None,
+                                 kf, d, mpath, spaths["plain"])
+        else:
+            pf = None
 
-    # --- CPU baseline: the reference's openmpcsr4mlem on this host (rank 0, N=1) ---
-    if rank == 0 and world == 1 and not a.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline_from_ctx(ctx, frames.sinograms[0], g, a.cpu_iters)
+        # --- ordered subsets: 8 interleaved row subsets, the plain sinogram ---
+        if not a.no_osem:
+            detail["osem"] = osem_line(ctx, a, frames.sinograms, stream, barrier, ms_per_step)
 
-    ctx.close()
+        # --- differentiable MLEM: 10 unrolled iterations, gradient of an MSE loss ---
+        if not a.no_differentiable:
+            detail["differentiable"] = differentiable_line(ctx, a, stream, barrier)
+        ctx.close()
 
-    # --- uneven batch over three geometries (12 + 8 + 4 frames), one GPU ---
-    if world == 1 and not a.no_uneven:
-        from mlem_b200 import uneven
-        torch.cuda.synchronize()
-        line["uneven"] = uneven.run(iters=max(10, min(a.steps, 20)), warmup=3, device=local_rank)
+        # --- a skewed matrix: the long rows run as segments (k_long.cu) ---
+        if not a.no_skewed:
+            detail["skewed"] = skewed_line(a, stream, barrier)
 
-    # --- a symmetry-compressed matrix: expanded on the device vs mirrors in the kernels ---
-    if world == 1 and not a.no_mirrored:
-        from mlem_b200 import mirrored
-        torch.cuda.synchronize()
-        line["mirrored"] = mirrored.run(iters=10, warmup=3, device=local_rank)
+        # --- uneven batch over three geometries (12 + 8 + 4 frames), one GPU ---
+        if world == 1 and not a.no_uneven:
+            from mlem_b200 import uneven
+            torch.cuda.synchronize()
+            u = uneven.run(iters=max(10, min(a.steps, 20)), warmup=3, device=local_rank)
+            detail["uneven"] = u
 
+        # --- a symmetry-compressed matrix: expanded on the device vs mirrors in the kernels ---
+        if world == 1 and not a.no_mirrored:
+            from mlem_b200 import mirrored
+            torch.cuda.synchronize()
+            detail["mirrored"] = mirrored.run(iters=10, warmup=3, device=local_rank)
+
+        # --- full-size parity, host side: wait for the reference binary and the oracle ---
+        if jobs is not None:
+            tail["parity_full"] = parity_finish(jobs, pf, a.parity_iters)
+    finally:
+        if d is not None:
+            shutil.rmtree(d, ignore_errors=True)
+
+    if "uneven" in detail:
+        u = detail["uneven"]
+        tail["uneven"] = {"ms_per_iteration": u["batch_ms_per_iteration"],
+                          "speedup_vs_separate": u["speedup_vs_separate"],
+                          "hbm_gbs": u["hbm_gbs"],
+                          "max_rel_l2_vs_separate": sig(u["max_rel_l2_batch_vs_separate"])}
     if dist is not None:
         dist.destroy_process_group()
-    return line
+    return detail, head, tail
+
+
+def cpu_baseline(ctx, mpath, spath, sino, iters):
+    """openmpcsr4mlem on all host cores, on the bench's CSR4 file."""
+    from mlem_b200 import api
+    if not os.path.exists(REF_MESSUNG):
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "unavailable: oracle/_ref/openmpcsr4mlem_messung not built"}
+    import numpy as np
+    threads = host_threads()
+    secs, wall, out = run_reference_binary(mpath, spath, iters, threads)
+    per = statistics.mean(secs[1:]) if len(secs) > 1 else secs[0]
+    ref_img = np.fromfile(out, dtype=np.float32)
+    ctx.set_sinograms(sino)
+    ctx.init_images()
+    ctx.iterate(iters, stats=False)
+    return {"value": round(1.0 / per, 4), "unit": UNIT, "cores": threads, "kind": "reference",
+            "sample": f"{iters} full iterations of openmpcsr4mlem (reference source, -O3 -fopenmp "
+                      f"-DMESSUNG) on the same plain-full CSR4 file; mean of iterations 2..{iters}; "
+                      f"wall {wall:.1f} s incl. load and serial column sums",
+            "iteration_seconds": secs,
+            "parity": {"iterations": iters,
+                       "rel_l2_vs_reference_image": rel_l2(ctx.get_images()[0], ref_img),
+                       "tolerance": TOL, "method": api.BK_NAMES[ctx.tuning()["bk_mode"]]}}
+
+
+def parity_gpu_side(ctx, a, tuning, sinograms, fb, tb, kf, d, mpath, spath):
+    """The GPU images of the full-size parity check (60 iterations):
+    * fast: the autotuned one-pass path on the bench's context;
+    * cli: the command-line drop-in with a checkpoint every 10 iterations
+      (the deterministic CSC method, its default);
+    * batch: the 16-frame batch, and every frame run on its own with the same
+      method and visit (frame tile 1)."""
+    import numpy as np
+
+    from mlem_b200 import api
+    n = a.parity_iters
+    out = {}
+    ctx.set_sinograms(sinograms)
+    ctx.set_tuning(**{k: tuning[k] for k in ("bk_mode", "group", "frame_tile", "blocks_per_sm",
+                                              "visit")})
+    ctx.init_images()
+    ctx.iterate(n, stats=False)
+    out["fast"] = ctx.get_images()[0]
+    out["fast_method"] = f"{api.BK_NAMES[tuning['bk_mode']]}/{api.VISIT_NAMES[tuning['visit']]}"
+    try:
+        out["cli"], out["cli_clean"], out["cli_wall"] = run_cli(d, mpath, spath, n, 10)
+    except Exception as e:  # reported, not fatal
+        out["cli_error"] = str(e)[:200]
+    if fb is not None:
+        ctx.set_sinograms(fb.sinograms)
+        ctx.set_tuning(**{k: tb[k] for k in ("bk_mode", "group", "frame_tile", "blocks_per_sm",
+                                              "visit")})
+        ctx.init_images()
+        ctx.iterate(n, stats=False)
+        batch = ctx.get_images()
+        worst = 0.0
+        for b in range(fb.sinograms.shape[0]):
+            ctx.set_sinograms(fb.sinograms[b:b + 1])
+            ctx.set_tuning(bk_mode=tb["bk_mode"], group=tb["group"], frame_tile=1,
+                           blocks_per_sm=tb["blocks_per_sm"], visit=tb["visit"])
+            ctx.init_images()
+            ctx.iterate(n, stats=False)
+            worst = max(worst, rel_l2(batch[b], ctx.get_images()[0]))
+        out["batch_frame"] = batch[kf]
+        out["batch_vs_single_max"] = worst
+        out["kf"] = kf
+        ctx.set_sinograms(sinograms)
+    return out
+
+
+def parity_finish(jobs, pf, n):
+    """Relative L2 errors of the 60-iteration images: ours against the
+    reference's seqcsr4mlem, and ours and the reference's against the FP64
+    oracle of the same iterations."""
+    try:
+        ref, wait_s = jobs.collect()
+    except Exception as e:
+        return {"iterations": n, "error": str(e)[:300]}
+    res = {"iterations": n, "tolerance": TOL, "reference": "seqcsr4mlem (1 core)",
+           "fp64_oracle_threads": jobs.f64_threads, "host_wall_s": round(wait_s, 1)}
+    seq, f64 = ref["plain"]
+    p = {"fast_vs_seq": sig(rel_l2(pf["fast"], seq)), "fast_vs_f64": sig(rel_l2(pf["fast"], f64)),
+         "seq_vs_f64": sig(rel_l2(seq, f64)), "fast_method": pf["fast_method"]}
+    if "cli" in pf:
+        p.update({"cli_chk10_vs_seq": sig(rel_l2(pf["cli"], seq)),
+                  "cli_chk10_vs_f64": sig(rel_l2(pf["cli"], f64)),
+                  "cli_checkpoints_removed": pf["cli_clean"]})
+    else:
+        p["cli_error"] = pf.get("cli_error")
+    res["plain"] = p
+    if "batched_frame" in ref and "batch_frame" in pf:
+        bseq, bf64 = ref["batched_frame"]
+        res["batched"] = {"frame": pf["kf"],
+                          "batch_vs_seq": sig(rel_l2(pf["batch_frame"], bseq)),
+                          "batch_vs_f64": sig(rel_l2(pf["batch_frame"], bf64)),
+                          "seq_vs_f64": sig(rel_l2(bseq, bf64)),
+                          "max_frame_vs_single_run": sig(pf["batch_vs_single_max"])}
+    worst = [v for blk in (res.get("plain", {}), res.get("batched", {}))
+             for k, v in blk.items() if k.endswith("_vs_seq") or k == "max_frame_vs_single_run"]
+    res["ok"] = bool(worst) and all(v is not None and v <= TOL for v in worst)
+    return res
+
+
+def osem_line(ctx, a, sinograms, stream, barrier, ms_per_step):
+    import torch
+
+    from mlem_b200 import api
+    n_sub = 8
+    ctx.set_sinograms(sinograms)
+    ctx.init_images()
+    ctx.set_subsets(n_sub)
+    to = ctx.autotune()
+    ctx.init_images()
+    ctx.iterate(a.warmup, stats=False)
+    ko = max(10, a.steps // 2)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    e0.record(stream)
+    ctx.iterate(ko, stats=False)
+    e1.record(stream)
+    barrier()
+    oms = e0.elapsed_time(e1) / ko
+    out = {"workload": "plain-full", "subsets": n_sub, "ms_per_iteration": round(oms, 4),
+           "sub_iterations_per_s": round(n_sub * 1e3 / oms, 2),
+           "iteration_time_vs_plain": round(oms / ms_per_step, 3),
+           "frame_tile": to["frame_tile"], "group": to["group"],
+           "row_visit": api.VISIT_NAMES[to["visit"]],
+           "gpu_launches_per_iteration": int(ctx.kernels_per_iteration())}
+    ctx.set_subsets(1)
+    return out
 
 
 def differentiable_line(ctx, a, stream, barrier):
@@ -522,106 +787,171 @@ def skewed_line(a, stream, barrier):
                 "gpu_launches_per_iteration": int(ctx.kernels_per_iteration())}
 
 
-def rel_l2(a, b):
+# ---------------------------------------------------------------------------
+# our implementation, row shards over N GPUs (strong scaling)
+# ---------------------------------------------------------------------------
+def run_shards(a, rank, world, local_rank):
+    """The plain-full matrix split into nnz-balanced row blocks (the
+    reference's partition, mpicsr4mlem.cpp:202-234), one per rank; each
+    iteration is the block's one-pass partial update and ONE NCCL all-reduce
+    of the C floats (fusedmpimlem.cpp:195-236).  Timed: K iterations on the
+    device, max over ranks.  Rank 0 checks the image against a single-context
+    run of the whole matrix."""
+    import datetime
+
     import numpy as np
-    a, b = np.asarray(a, np.float64).ravel(), np.asarray(b, np.float64).ravel()
-    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+    import torch
+    import torch.distributed as dist
 
+    from mlem_b200 import api, distributed, synth
 
-def batched_parity(ctx, sinograms, tuning, iters):
-    """Every frame of a batched reconstruction against its own single-frame
-    run (same tuning method and visit), after `iters` iterations."""
-    from mlem_b200 import api
-
-    ctx.set_sinograms(sinograms)
-    ctx.init_images()
-    ctx.iterate(iters, stats=False)
-    batch = ctx.get_images()
-    worst = 0.0
-    for b in range(sinograms.shape[0]):
-        ctx.set_sinograms(sinograms[b:b + 1])
-        ctx.set_tuning(bk_mode=tuning["bk_mode"], group=tuning["group"], frame_tile=1,
-                       blocks_per_sm=tuning["blocks_per_sm"], visit=tuning["visit"])
-        ctx.init_images()
-        ctx.iterate(iters, stats=False)
-        worst = max(worst, rel_l2(batch[b], ctx.get_images()[0]))
-    return {"iterations": iters, "max_rel_l2_frame_vs_single_run": worst, "tolerance": 1e-4,
-            "single_run_visit": api.VISIT_NAMES[tuning["visit"]]}
-
-
-def cpu_baseline_from_ctx(ctx, sino, g, iters):
-    if not os.path.exists(REF_MESSUNG):
-        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                "sample": "unavailable: oracle/_ref/openmpcsr4mlem_messung not built"}
-    need = 8 * ctx.nnz + 8 * ctx.n_rows + 4 * ctx.n_rows
-    d = scratch_dir(need)
-    if d is None:
-        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
-                "sample": "unavailable: no scratch space for the CSR4 file"}
-    try:
-        row_end, elems = ctx.csr()
-        mp, sp = write_inputs(d, row_end, elems, ctx.n_rows, ctx.n_cols, (g.nx, g.ny, g.nz), sino)
-        del row_end, elems
-        threads = host_threads()
-        secs, wall = run_reference_binary(mp, sp, iters, threads)
-        per = statistics.mean(secs[1:]) if len(secs) > 1 else secs[0]
-        # the reference's image after these iterations against ours from the same inputs
-        import numpy as np
-
-        from mlem_b200 import api
-        ref_img = np.fromfile(os.path.join(d, "image.out"), dtype=np.float32)
-        ctx.set_sinograms(sino)
-        ctx.init_images()
-        ctx.iterate(iters, stats=False)
-        parity = {"iterations": iters, "rel_l2_vs_reference_image": rel_l2(ctx.get_images()[0], ref_img),
-                  "tolerance": 1e-4, "method": api.BK_NAMES[ctx.tuning()["bk_mode"]]}
-        return {"value": round(1.0 / per, 4), "unit": UNIT, "cores": threads, "kind": "reference",
-                "sample": f"{iters} full iterations of openmpcsr4mlem (reference source, -O3 -fopenmp "
-                          f"-DMESSUNG) on the same plain-full CSR4 file; mean of iterations 2..{iters}; "
-                          f"wall {wall:.1f} s incl. load and serial column sums",
-                "iteration_seconds": secs, "parity": parity}
-    finally:
-        shutil.rmtree(d, ignore_errors=True)
+    torch.cuda.set_device(local_rank)
+    if "MASTER_ADDR" not in os.environ:  # one rank without torchrun
+        import socket
+        with socket.socket() as s:
+            s.bind(("127.0.0.1", 0))
+            port = s.getsockname()[1]
+        os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK="0",
+                          WORLD_SIZE="1")
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                            device_id=torch.device("cuda", local_rank))
+    w = synth.WORKLOADS["plain-full"]
+    g = w.geometry
+    stream = torch.cuda.current_stream()
+    t0 = time.time()
+    full = api.Context.siddon(g, flags=api.FLAG_NO_CSC, device=local_rank)
+    frames = synth.make_frames(w, full.project_f64)
+    row_end, elems = full.csr()
+    nnz = int(full.nnz)
+    starts, ends = distributed.partition(row_end, world)
+    blk = distributed.row_block(row_end, elems, int(starts[rank]), int(ends[rank]))
+    del row_end, elems
+    if rank != 0:
+        full.close()
+        full = None
+    shard = distributed.CudaShard(blk, g.n_cols, frames.sinograms[0][blk.start:blk.end], local_rank)
+    setup_s = time.time() - t0
+    x = distributed.init_image(shard, dist)
+    distributed.iterate(shard, x, a.warmup, dist)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local_rank) if rank == 0 else None
+    if clocks:
+        clocks.start()
+        time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    distributed.iterate(shard, x, a.steps, dist)
+    e1.record(stream)
+    dist.barrier()
+    torch.cuda.synchronize()
+    clk = clocks.stop() if clocks else None
+    # end to end: every step uploads the rank's sinogram block from pinned host
+    # memory and reads the image back into pinned host memory
+    sino_h = torch.from_numpy(frames.sinograms[0][blk.start:blk.end].copy()).pin_memory()
+    img_h = torch.empty(g.n_cols, dtype=torch.float32).pin_memory()
+    k_e2e = max(5, min(a.steps, 50))
+    dist.barrier()
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record(stream)
+    for _ in range(k_e2e):
+        shard.sino.copy_(sino_h, non_blocking=True)
+        distributed.iterate(shard, x, 1, dist)
+        img_h.copy_(x, non_blocking=True)
+    f1.record(stream)
+    dist.barrier()
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1), f0.elapsed_time(f1)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms, e2e_ms = float(t[0].item()), float(t[1].item()) / k_e2e
+    img = shard.to_host(x)
+    n_total = a.warmup + a.steps + k_e2e
+    line = None
+    if rank == 0:
+        full.set_stream(stream.cuda_stream)
+        full.set_sinograms(frames.sinograms)
+        full.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=1, blocks_per_sm=4,
+                        visit=api.VISIT_SORTED_CHUNKED)
+        full.init_images()
+        full.iterate(n_total, stats=False)
+        ref = full.get_images()[0]
+        full.close()
+        line = ({"shard_rows": [int(s) for s in (starts[0], ends[0])], "setup_s": round(setup_s, 1)},
+                {"metric": METRIC, "value": round(a.steps / (ms / 1e3), 3), "unit": UNIT,
+                 "n_gpus": world, "steps": a.steps, "warmup": a.warmup,
+                 "ms_per_step": round(ms / a.steps, 4), "higher_is_better": True,
+                 "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+                 "data": "synthetic (seeded Siddon matrix, ellipsoid phantom, Poisson sinogram)",
+                 "config": workload_config(g, nnz, "shards"),
+                 "e2e": {"value": round(1e3 / e2e_ms, 3), "unit": UNIT,
+                         "h2d_bytes_per_step": int(4 * (blk.end - blk.start)),
+                         "d2h_bytes_per_step": int(4 * g.n_cols),
+                         "call": "distributed.iterate (pinned sinogram block in, image out)"},
+                 # per iteration and rank: the one-pass kernel and the update apply
+                 "gpu_launches": int(2 * a.steps * world),
+                 "clocks": clk},
+                {"shards": {"ranks": world, "allreduce_floats_per_iteration": int(g.n_cols),
+                            "iterations": n_total,
+                            "rel_l2_vs_single_context": sig(rel_l2(img, ref)),
+                            "tolerance": TOL}})
+    shard.close()
+    dist.destroy_process_group()
+    return line
 
 
 # ---------------------------------------------------------------------------
 # reference arm
 # ---------------------------------------------------------------------------
-def run_reference(a, rank, world):
+def run_reference(a, rank, world, parallelism):
+    """The reference's openmpcsr4mlem on this host's cores, on the plain-full
+    workload.  The inputs are written by oracle_tool in a child process (the
+    seeded generator and the FP64 projection, byte-identical to the GPU
+    arm's), so this process maps no library of the package under test."""
     if rank != 0:
         return None
     import numpy as np
 
-    from mlem_b200 import synth
+    from mlem_b200 import synth  # numpy-only parts: phantom, Poisson draw
 
     if not os.path.exists(REF_MESSUNG):
         return {"impl": "reference", "unavailable": "oracle/_ref/openmpcsr4mlem_messung is not built"}
+    if not os.path.exists(ORACLE_TOOL):
+        return {"impl": "reference", "unavailable": "oracle/_bin/oracle_tool is not built"}
     w = synth.WORKLOADS["plain-full"]
     g = w.geometry
-    m = synth.host_matrix(g)  # host generator (CPU); bit-identical to the GPU arm's matrix
-    frames = synth.make_frames(w, lambda x: synth.project_f64(m, x))
-    need = 8 * m.nnz + 8 * m.n_rows
-    d = scratch_dir(need)
+    d = scratch_dir(8 * 9e8)
     if d is None:
         return {"impl": "reference", "unavailable": "no scratch space for the 6 GB CSR4 file"}
     try:
-        mp, sp = write_inputs(d, m.row_end, m.elems, m.n_rows, m.n_cols, (g.nx, g.ny, g.nz),
-                              frames.sinograms[0])
-        del m
+        mp = os.path.join(d, "matrix.csr4")
+        subprocess.run([ORACLE_TOOL, "synth-matrix", str(g.nx), str(g.ny), str(g.nz),
+                        str(g.n_rows), str(g.min_count), str(g.max_count), str(g.seed),
+                        repr(g.radius_scale), repr(g.min_len), mp], check=True, timeout=1200)
+        with open(mp, "rb") as f:
+            nnz = int(np.frombuffer(f.read(24)[16:24], np.uint64)[0])
+        n_ell, counts = synth.frame_spec(w, 0)
+        x = synth.phantom(g.nx, g.ny, g.nz, n_ell, w.frame_seed(0))
+        xp, mp_out = os.path.join(d, "phantom.f32"), os.path.join(d, "means.f64")
+        x.astype(np.float32).tofile(xp)
+        subprocess.run([ORACLE_TOOL, "project-f64", mp, xp, mp_out], check=True, timeout=600)
+        sino = synth.poisson_sinogram(np.fromfile(mp_out, np.float64), counts, w.frame_seed(0) + 500)
+        sp = os.path.join(d, "plain.sino")
+        sino.astype(np.int32).tofile(sp)
         threads = host_threads()
         k = max(1, min(a.steps, 20))
         wu = max(3, min(a.warmup, 5))  # at least 3 warm-up iterations, at most 5 (bounded run)
-        secs, wall = run_reference_binary(mp, sp, wu + k, threads)
+        secs, wall, _ = run_reference_binary(mp, sp, wu + k, threads)
         timed = secs[wu:]
         per = statistics.mean(timed)
         value = 1.0 / per
         return {
             "impl": "reference", "metric": METRIC, "value": round(value, 4), "unit": UNIT,
             "n_gpus": world, "steps": len(timed), "warmup": wu, "ms_per_step": round(per * 1e3, 2),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "higher_is_better": True, "scaling": "strong" if parallelism == "shards" else "weak",
+            "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded Siddon matrix, ellipsoid phantom, Poisson sinogram)",
-            "config": {"workload": "plain-full", "grid": [g.nx, g.ny, g.nz], "n_rows": g.n_rows,
-                       "n_cols": g.n_cols, "frames": 1},
+            "config": workload_config(g, nnz, parallelism),
             "cpu_baseline": {"value": round(value, 4), "unit": UNIT, "cores": threads,
                              "kind": "reference",
                              "sample": f"{len(timed)} timed iterations (of the {a.steps} requested; "
@@ -639,11 +969,25 @@ def main():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    parallelism = a.parallelism
+    if parallelism == "auto":
+        parallelism = "shards" if world > 1 else "single"
     if a.impl == "reference":
-        line = run_reference(a, rank, world)
+        line = run_reference(a, rank, world, parallelism)
+        if rank == 0 and line is not None:
+            print(json.dumps(line), flush=True)
+        return
+    if parallelism == "shards":
+        parts = run_shards(a, rank, world, local_rank)
     else:
-        line = run_ours(a, rank, world, local_rank)
-    if rank == 0 and line is not None:
+        parts = run_ours(a, rank, world, local_rank, parallelism)
+    if rank == 0 and parts is not None:
+        detail, head, tail = parts
+        # one line: details first, then the contract's keys, then the short
+        # summaries (batched, parity_full) last, where a tail of the output keeps them
+        line = dict(detail)
+        line.update(head)
+        line.update(tail)
         print(json.dumps(line), flush=True)
 
 

@@ -314,30 +314,34 @@ int mlem_project_f64(mlem_ctx* ctx, const float* x, double* out);
 /* No counterpart in the reference.  Every other entry point keeps working
  * vectors in device memory the library allocates.  This one is for callers
  * that cannot let a library call cudaMalloc: programs that run inside a fixed
- * device-memory budget handed out by a framework or scheduler, or that must
- * keep allocations out of a latency-critical section.  It runs one MLEM
+ * device-memory budget handed out by a framework or scheduler, or that run
+ * while another component owns the device allocator.  It runs one MLEM
  * iteration (calcFwProj, calcCorrel, calcBkProj, calcUpdate,
  * mlem_seq/seqcsr4mlem.cpp:164-167) on caller-owned DEVICE buffers and calls
  * no cudaMalloc, cudaFree or allocating library routine:
  *   row_ptr  uint64[R+1]: row offsets WITH a leading 0 (the CSR4 row END
- *            offsets shifted by one), elems: R rows of 8-byte {uint32
- *            column, float32 value} elements, sino int32[R], norm float32[C]
- *            (the column sums), image float32[C], updated in place.
+ *            offsets shifted by one); elems: n_elems 8-byte {uint32 column,
+ *            float32 value} elements; sino int32[R]; norm float32[C] (the
+ *            column sums); image float32[C], updated in place.
  * Its only working vector, the back-projection update, is a fixed
  * MLEM_NOALLOC_MAX_VOXELS-float array in the library's static device memory:
  * every GPU that loads the library holds those 4 MiB until exit.  Images with
  * more voxels are rejected (MLEM_ERR_INVALID).  All calls on a device share the
  * array and each call clears it first, so calls that overlap on the GPU
  * (several streams or host threads) race and must be serialised by the
- * caller.  The first call on a device looks up the array's device address
- * (cudaGetSymbolAddress, with that device current); make that first call
- * before any stream capture.  The call enqueues on `stream` and waits for it,
- * then returns MLEM_ERR_MATRIX if any column index was >= n_cols (those
- * elements are skipped).  Natural voxel order; one frame. */
+ * caller.  The first call on a device (and the first after its context is
+ * created again) does a one-time set-up: it looks up the array's device
+ * address (cudaGetSymbolAddress, with that device current); make that first
+ * call before any stream capture begins.  The call enqueues on `stream`, then
+ * waits for the stream to finish and reads the kernels' error word back.  It
+ * checks the matrix as it goes: a row whose offsets decrease or pass n_elems
+ * is skipped, and so is an element whose column is >= n_cols; either gives
+ * MLEM_ERR_MATRIX after the iteration (the other rows are applied).  Natural
+ * voxel order; one frame. */
 #define MLEM_NOALLOC_MAX_VOXELS 1048576
-int mlem_iterate_noalloc_d(const uint64_t* row_ptr, const void* elems, uint32_t n_rows,
-                           uint32_t n_cols, const int32_t* sino, const float* norm, float* image,
-                           void* stream);
+int mlem_iterate_noalloc_d(const uint64_t* row_ptr, const void* elems, uint64_t n_elems,
+                           uint32_t n_rows, uint32_t n_cols, const int32_t* sino,
+                           const float* norm, float* image, void* stream);
 
 /* ---- uneven multi-matrix batches ----------------------------------------
  * No counterpart in the reference, which reconstructs one matrix per process

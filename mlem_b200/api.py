@@ -568,15 +568,17 @@ def mlem(matrix: Context, lmsino, image: Optional[np.ndarray] = None, nIteration
 NOALLOC_MAX_VOXELS = 1048576
 
 
-def iterate_noalloc_d(row_ptr: int, elems: int, n_rows: int, n_cols: int, sino: int, norm: int,
-                      image: int, stream: int = 0) -> None:
+def iterate_noalloc_d(row_ptr: int, elems: int, n_elems: int, n_rows: int, n_cols: int,
+                      sino: int, norm: int, image: int, stream: int = 0) -> None:
     """mlem_iterate_noalloc_d: one MLEM iteration on caller-owned device
     buffers (integer device addresses) for callers that cannot let the
     library allocate device memory; its update vector lives in a fixed
     4 MiB static device array (at most NOALLOC_MAX_VOXELS voxels), shared by
-    all calls on a device, so overlapping calls race."""
-    _raise(core_lib().mlem_iterate_noalloc_d(row_ptr, elems, n_rows, n_cols, sino, norm, image,
-                                             stream or None))
+    all calls on a device, so overlapping calls race.  Rows whose offsets
+    decrease or pass n_elems, and columns >= n_cols, are skipped and raise
+    MlemError(MLEM_ERR_MATRIX) after the iteration."""
+    _raise(core_lib().mlem_iterate_noalloc_d(row_ptr, elems, n_elems, n_rows, n_cols, sino, norm,
+                                             image, stream or None))
 
 
 # ---------------------------------------------------------------------------

@@ -63,10 +63,19 @@ class Shard(Protocol):
     def to_host(self, x) -> np.ndarray: ...
 
 
-def reconstruct(shard: Shard, n_iter: int, dist, group=None, start_image=None):
-    """Run initImage + n_iter iterations; returns the (replicated) image on
-    the host.  `dist` is torch.distributed (or any module with all_reduce
-    and ReduceOp); every rank takes the same collective steps."""
+def sequential_sum(v: np.ndarray) -> float:
+    """Double sum of v in array order (the loop of initImage,
+    seqcsr4mlem.cpp:55-56): np.cumsum accumulates left to right, unlike
+    np.sum's pairwise summation."""
+    v = np.asarray(v).ravel()
+    return float(np.cumsum(v, dtype=np.float64)[-1]) if v.size else 0.0
+
+
+def init_image(shard: Shard, dist, group=None, start_image=None):
+    """Install the global column sums on the shard (one all-reduce,
+    mpicsr4mlem.cpp:266) and return the starting image: initImage's value
+    from the global sums (seqcsr4mlem.cpp:52-66), or `start_image` (restart).
+    Every rank takes the same collective steps."""
     import torch
 
     norm = shard.local_norm()
@@ -76,14 +85,17 @@ def reconstruct(shard: Shard, n_iter: int, dist, group=None, start_image=None):
         sumin = torch.tensor([shard.local_count_sum()], dtype=torch.float64,
                              device=norm.device)
         dist.all_reduce(sumin, op=dist.ReduceOp.SUM, group=group)
-        host_norm = shard.to_host(norm)
-        sumnorm = 0.0
-        for v in host_norm.tolist():  # sequential double sum, seqcsr4mlem.cpp:55-56
-            sumnorm += v
-        x = shard.fill(float(np.float32(float(sumin.item()) / sumnorm)))
-    else:
-        x = shard.fill(0.0)
-        x.copy_(torch.as_tensor(np.asarray(start_image, np.float32)).to(x.device))
+        sumnorm = sequential_sum(shard.to_host(norm))
+        return shard.fill(float(np.float32(float(sumin.item()) / sumnorm)))
+    x = shard.fill(0.0)
+    x.copy_(torch.as_tensor(np.asarray(start_image, np.float32)).to(x.device))
+    return x
+
+
+def iterate(shard: Shard, x, n_iter: int, dist, group=None):
+    """n_iter iterations on the replicated image x (updated in place): the
+    shard's partial update, ONE sum all-reduce of the C floats
+    (fusedmpimlem.cpp:227), the identical update on every rank."""
     one_step = getattr(shard, "partial_update", None)
     for _ in range(n_iter):
         if one_step is not None:
@@ -92,20 +104,40 @@ def reconstruct(shard: Shard, n_iter: int, dist, group=None, start_image=None):
             update = shard.backproject(shard.project_correl(x))
         dist.all_reduce(update, op=dist.ReduceOp.SUM, group=group)  # fusedmpimlem.cpp:227
         shard.apply(update, x)
+    return x
+
+
+def reconstruct(shard: Shard, n_iter: int, dist, group=None, start_image=None):
+    """Run initImage + n_iter iterations; returns the (replicated) image on
+    the host.  `dist` is torch.distributed (or any module with all_reduce
+    and ReduceOp); every rank takes the same collective steps."""
+    x = init_image(shard, dist, group, start_image)
+    iterate(shard, x, n_iter, dist, group)
     return shard.to_host(x)
 
 
 class CudaShard:
-    """A row block on this rank's GPU, driven through the C ABI."""
+    """A row block on this rank's GPU, driven through the C ABI.
+
+    With one_pass (the default) every iteration computes the block's partial
+    update in one pass over its rows (partial_update), which reads no CSC, so
+    the context is built without one (MLEM_FLAG_NO_CSC: half the device
+    memory, and the block's column sums by atomics).  With one_pass=False
+    the shard offers only the two passes (project_correl, then backproject
+    over the CSC)."""
 
     def __init__(self, block: RowBlock, n_cols: int, sino_block: np.ndarray, device: int,
-                 flags: int = 0):
+                 flags: int = 0, one_pass: bool = True):
         import torch
 
         self.torch = torch
         self.device = torch.device("cuda", device)
         self.n_cols = n_cols
         self.n_rows = block.end - block.start
+        if one_pass:
+            flags |= api.FLAG_NO_CSC
+        else:
+            self.partial_update = None  # iterate() then takes the two passes
         self.ctx = api.Context(block.row_end, block.elems, self.n_rows, n_cols, flags, device)
         self.stream = torch.cuda.current_stream(self.device)
         self.ctx.set_stream(self.stream.cuda_stream)

@@ -303,6 +303,89 @@ int oracle_mlem_f64(uint32_t R, uint32_t C, const uint64_t* row_end, const oracl
     return 0;
 }
 
+/*
+ * The FP64 oracle above on several host threads, for matrices where the serial
+ * loop takes minutes.  Rows are cut into n_threads contiguous blocks of about
+ * equal element counts; each thread sums its rows' column sums and back
+ * projection into a private double vector, and the vectors are added in
+ * thread order.  The forward projection of a row is the same sequential
+ * double sum as oracle_mlem_f64's; the column sums and back projection differ
+ * from it only by the order of double additions (a few units in the last
+ * place), and a fixed thread count gives the same image on every run.
+ */
+int oracle_mlem_f64_threads(uint32_t R, uint32_t C, const uint64_t* row_end,
+                            const oracle_elem* e, const int32_t* sino, uint64_t S, int n_iter,
+                            int n_threads, double* image) {
+    if (S != R) return -1;
+    if (n_threads < 1) n_threads = 1;
+    if ((uint32_t)n_threads > R && R > 0) n_threads = (int)R;
+    const int T = n_threads;
+    double* fw = (double*)malloc((size_t)R * sizeof(double) + 1);
+    double* norm = (double*)calloc((size_t)C + 1, sizeof(double));
+    double* priv = (double*)malloc((size_t)T * (C + 1) * sizeof(double));
+    uint32_t* cut = (uint32_t*)malloc((size_t)(T + 1) * sizeof(uint32_t));
+    if (!fw || !norm || !priv || !cut) {
+        free(fw); free(norm); free(priv); free(cut);
+        return -2;
+    }
+    /* block t holds rows [cut[t], cut[t+1]): the first row whose END offset
+     * reaches t/T of the elements starts block t */
+    const uint64_t Z = R ? row_end[R - 1] : 0;
+    cut[0] = 0;
+    cut[T] = R;
+    for (int t = 1; t < T; ++t) {
+        const uint64_t want = Z / (uint64_t)T * (uint64_t)t;
+        uint32_t lo = cut[t - 1], hi = R;
+        while (lo < hi) {
+            uint32_t mid = lo + (hi - lo) / 2;
+            if (row_end[mid] < want) lo = mid + 1; else hi = mid;
+        }
+        cut[t] = lo;
+    }
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+    for (int t = 0; t < T; ++t) {
+        double* p = priv + (size_t)t * (C + 1);
+        memset(p, 0, (size_t)C * sizeof(double));
+        for (uint32_t r = cut[t]; r < cut[t + 1]; ++r)
+            for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+                p[e[k].index] += (double)e[k].value;
+    }
+#pragma omp parallel for num_threads(T) schedule(static)
+    for (int64_t i = 0; i < (int64_t)C; ++i) {
+        double s = 0.0;
+        for (int t = 0; t < T; ++t) s += priv[(size_t)t * (C + 1) + i];
+        norm[i] = s;
+    }
+    double sumnorm = 0.0, sumin = 0.0;
+    for (uint32_t i = 0; i < C; ++i) sumnorm += norm[i];
+    for (uint64_t i = 0; i < S; ++i) sumin += sino[i];
+    for (uint32_t i = 0; i < C; ++i) image[i] = sumin / sumnorm;
+    for (int it = 0; it < n_iter; ++it) {
+#pragma omp parallel for num_threads(T) schedule(static, 1)
+        for (int t = 0; t < T; ++t) {
+            for (uint32_t r = cut[t]; r < cut[t + 1]; ++r) {
+                double res = 0.0;
+                for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+                    res += (double)e[k].value * image[e[k].index];
+                fw[r] = (res != 0.0) ? (double)sino[r] / res : 0.0;
+            }
+            double* p = priv + (size_t)t * (C + 1);
+            memset(p, 0, (size_t)C * sizeof(double));
+            for (uint32_t r = cut[t]; r < cut[t + 1]; ++r)
+                for (uint64_t k = row_begin(row_end, r); k < row_end[r]; ++k)
+                    p[e[k].index] += (double)e[k].value * fw[r];
+        }
+#pragma omp parallel for num_threads(T) schedule(static)
+        for (int64_t i = 0; i < (int64_t)C; ++i) {
+            double u = 0.0;
+            for (int t = 0; t < T; ++t) u += priv[(size_t)t * (C + 1) + i];
+            image[i] *= (norm[i] != 0.0) ? (u / norm[i]) : u;
+        }
+    }
+    free(fw); free(norm); free(priv); free(cut);
+    return 0;
+}
+
 void oracle_mlem_relaxed_f64(uint32_t R, uint32_t C, const uint64_t* row_end,
                              const oracle_elem* e, const int32_t* sino, const double* x0,
                              const double* omega, int K, double* xK) {

@@ -109,6 +109,14 @@ uint64_t oracle_expand_symmetries(uint32_t R, const uint64_t* row_end, const ora
 int oracle_mlem_f64(uint32_t R, uint32_t C, const uint64_t* row_end, const oracle_elem* e,
                     const int32_t* sino, uint64_t S, int n_iter, double* image);
 
+/* oracle_mlem_f64 on n_threads host threads (OpenMP): row blocks of about
+ * equal element counts, private double column sums and update vectors added in
+ * thread order.  Equal to oracle_mlem_f64 up to the order of double additions
+ * in the column sums and the back projection. */
+int oracle_mlem_f64_threads(uint32_t R, uint32_t C, const uint64_t* row_end,
+                            const oracle_elem* e, const int32_t* sino, uint64_t S, int n_iter,
+                            int n_threads, double* image);
+
 /*
  * Relaxed FP64 MLEM used by the gradient checks:
  *   x_{k+1} = x_k * ratio_k ^ omega_k,  ratio_k = calcUpdate's factor

@@ -80,7 +80,17 @@ def _worker(rank, world, port, out_dir, mode):
     try:
         if mode == "die" and rank == 1:
             os._exit(3)  # a rank that never joins the first collective
-        img = distributed.reconstruct(shard, iters, dist)
+        if mode == "pieces":
+            # the benchmark's order: start image, warm-up, timed iterations,
+            # then single steps
+            x = distributed.init_image(shard, dist)
+            distributed.iterate(shard, x, 2, dist)
+            distributed.iterate(shard, x, iters - 5, dist)
+            for _ in range(3):
+                distributed.iterate(shard, x, 1, dist)
+            img = shard.to_host(x)
+        else:
+            img = distributed.reconstruct(shard, iters, dist)
         np.save(os.path.join(out_dir, f"img{rank}.npy"), img)
         dist.barrier()
     except Exception as e:  # the surviving rank must see an error, not hang
@@ -137,3 +147,24 @@ def test_dead_rank_is_detected_not_hung(tmp_path):
     err = tmp_path / "err0.txt"
     assert err.exists(), "rank 0 should have failed its collective"
     assert not (tmp_path / "img0.npy").exists()
+
+
+def test_iterations_in_pieces_equal_one_reconstruction(tmp_path, golden):
+    import oracle_bind as ob
+    _launch(2, "pieces", tmp_path)
+    m, sino, iters, gold, _ = golden.case("tiny_it10")
+    a = np.load(tmp_path / "img0.npy")
+    b = np.load(tmp_path / "img1.npy")
+    assert a.tobytes() == b.tobytes()
+    want, _ = ob.mlem(m, sino, iters, ftz=False)
+    assert ob.rel_l2(a, want) <= 1e-5
+
+
+def test_sequential_sum_is_the_reference_order():
+    from mlem_b200 import distributed
+    rng = np.random.default_rng(2)
+    v = rng.uniform(0, 1e4, 100_001).astype(np.float32)
+    acc = 0.0
+    for t in v.tolist():
+        acc += t
+    assert distributed.sequential_sum(v) == acc
