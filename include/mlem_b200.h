@@ -105,7 +105,13 @@ typedef struct {
 
 /* Launch configuration chosen by the autotuner (or set by the caller).
  * MLEM_BK_REGION builds its region-blocked copy of the matrix (about the
- * size of the CSR) when it is first selected for a frame tile. */
+ * size of the CSR) when it is first selected for a frame tile.  MLEM_BK_CSC
+ * with MLEM_VISIT_SORTED builds, when first selected, a second CSC in which
+ * each column lists its rays by their position in the sorted row order
+ * (another Z x 8 bytes + R x 4): the forward pass stores the correlations
+ * by that position and the back projection gathers neighbouring rays.  It
+ * stays deterministic (each column summed in ascending position); with
+ * MLEM_VISIT_FILE the CSC lists rows ascending, as calcBkProj adds them. */
 typedef struct {
     int bk_mode;        /* MLEM_BK_CSC, MLEM_BK_ATOMIC, MLEM_BK_FUSED or MLEM_BK_REGION */
     int group;          /* lanes per row/column: 4, 8, 16 or 32 */
@@ -119,7 +125,7 @@ typedef struct {
 
 /* Row visiting orders (mlem_tuning.visit).  The sorted orders need the row
  * order built at creation (not MLEM_FLAG_NO_ROW_ORDER); results change only
- * by the order of the scatter atomics. */
+ * by the order of the scatter atomics (MLEM_BK_CSC: of the column sums). */
 #define MLEM_VISIT_FILE 0           /* file order, grid stride */
 #define MLEM_VISIT_SORTED 1         /* rows sorted by entry/exit voxel, grid stride */
 #define MLEM_VISIT_SORTED_CHUNKED 2 /* sorted; CTAs take chunks of neighbouring rows from a counter

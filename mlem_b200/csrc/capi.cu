@@ -223,6 +223,53 @@ int ensure_region(mlem_ctx* c, int frame_tile) {
     return MLEM_OK;
 }
 
+// The CSC in visiting order (mlem_ctx::celems_vis), built once on first use:
+// the transpose keyed by every row's visiting position.  Deterministic like
+// the CSC: a column's entries are summed in ascending visiting position.
+int ensure_csc_vis(mlem_ctx* c) {
+    if (c->celems_vis) return MLEM_OK;
+    if (!c->has_csc || !c->row_order)
+        return fail(c, MLEM_ERR_STATE, "the CSC in visiting order needs the CSC and the row order");
+    uint64_t* col_ptr = nullptr;
+    void* scratch = nullptr;
+    const size_t sb = transpose_scratch_bytes(c->C);
+    int s = dev_alloc(c, &c->row_pos, std::max<uint32_t>(c->R, 1));
+    if (s == MLEM_OK) s = dev_alloc(c, &c->celems_vis, c->Z + 2);
+    if (s == MLEM_OK) s = dev_alloc(c, &col_ptr, (size_t)c->C + 1);
+    if (s == MLEM_OK) s = dev_alloc(c, &scratch, sb);
+    if (s == MLEM_OK) {
+        cudaError_t e = cudaMemsetAsync(c->celems_vis + c->Z, 0, 2 * sizeof(uint2), c->stream);
+        if (e == cudaSuccess) e = invert_permutation(c->row_order, c->row_pos, c->R, c->stream);
+        if (e == cudaSuccess)
+            e = transpose(SparseView{c->row_ptr, reinterpret_cast<const uint4*>(c->elems), c->R,
+                                     c->Z},
+                          c->C, col_ptr, c->celems_vis, scratch, nullptr, c->stream, c->row_pos,
+                          c->row_order);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            s = fail(c, e == cudaErrorMemoryAllocation ? MLEM_ERR_NOMEM : MLEM_ERR_CUDA,
+                     "CSC in visiting order: %s", cudaGetErrorString(e));
+        }
+    }
+    if (col_ptr) { dev_free(col_ptr); c->device_bytes -= ((size_t)c->C + 1) * 8; }
+    if (scratch) { dev_free(scratch); c->device_bytes -= sb; }
+    if (s != MLEM_OK) {
+        if (c->celems_vis) { dev_free(c->celems_vis); c->device_bytes -= (c->Z + 2) * 8; }
+        if (c->row_pos) { dev_free(c->row_pos); c->device_bytes -= (size_t)std::max<uint32_t>(c->R, 1) * 4; }
+        c->celems_vis = nullptr;
+        c->row_pos = nullptr;
+        return s;
+    }
+    c->graph_dirty = true;
+    return MLEM_OK;
+}
+
+// The CSC method walks the CSC in visiting order with the sorted row visit.
+bool csc_by_visit(const mlem_ctx* c, const mlem_tuning& t) {
+    return t.bk_mode == MLEM_BK_CSC && t.visit != MLEM_VISIT_FILE && c->row_order && c->has_csc;
+}
+
 bool region_ready(const mlem_ctx* c, int frame_tile) {
     int rlog = 0, sblog = 0;
     uint32_t gpw = 0;
@@ -620,15 +667,27 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                             ? "a context made with MLEM_FLAG_MIRROR_KERNELS runs MLEM_BK_MIRRORED only"
                             : "MLEM_BK_MIRRORED needs a context made with MLEM_FLAG_MIRROR_KERNELS");
         switch (t.bk_mode) {
-            case MLEM_BK_CSC:
+            case MLEM_BK_CSC: {
                 if (!c->has_csc) return fail(c, MLEM_ERR_STATE, "no CSC copy (MLEM_FLAG_NO_CSC)");
+                // with a sorted visit: correlations by visiting position, and the
+                // CSC that lists each column's rays in that order
+                const bool by_visit = csc_by_visit(c, t);
+                if (by_visit && !c->celems_vis)
+                    return fail(c, MLEM_ERR_STATE, "the CSC in visiting order is not built");
+                SparseView fw = csr;
+                SparseView bk = csc_view(c);
+                if (by_visit) {
+                    fw.out_by_visit = true;
+                    bk.pairs = reinterpret_cast<const uint4*>(c->celems_vis);
+                }
                 for (uint32_t f0 = 0; f0 < Bp; f0 += T)
-                    CK(c, fwproj(csr, c->x, Bp, f0, c->sino, c->correl, nullptr, cfg, st));
+                    CK(c, fwproj(fw, c->x, Bp, f0, c->sino, c->correl, nullptr, cfg, st));
                 TRY(mark(c, pe, 1));
                 for (uint32_t f0 = 0; f0 < Bp; f0 += T)
-                    CK(c, bkproj_csc(csc_view(c), c->correl, Bp, f0, c->norm, c->x, nullptr, cfg, st));
+                    CK(c, bkproj_csc(bk, c->correl, Bp, f0, c->norm, c->x, nullptr, cfg, st));
                 TRY(mark(c, pe, 2));
                 break;
+            }
             case MLEM_BK_ATOMIC:
                 for (uint32_t f0 = 0; f0 < Bp; f0 += T)
                     CK(c, fwproj(csr, c->x, Bp, f0, c->sino, c->correl, nullptr, cfg, st));
@@ -1211,7 +1270,8 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->sub_file, (void*)c->sub_file_ranges, (void*)c->sub_sorted,
                     (void*)c->sub_sorted_ranges, (void*)c->mirror_lut, (void*)c->mirror_vox,
                     (void*)c->f_mirror_d, (void*)c->act_order, (void*)c->act_ranges,
-                    (void*)c->act_flags, (void*)c->act_tmp, (void*)c->act_n, (void*)c->act_z})
+                    (void*)c->act_flags, (void*)c->act_tmp, (void*)c->act_n, (void*)c->act_z,
+                    (void*)c->celems_vis, (void*)c->row_pos})
         dev_free(p);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
@@ -1596,6 +1656,10 @@ int mlem_set_tuning(mlem_ctx* c, const mlem_tuning* t) {
         TRY(set_device(c));
         TRY(ensure_region(c, n.frame_tile));
     }
+    if (csc_by_visit(c, n)) {
+        TRY(set_device(c));
+        TRY(ensure_csc_vis(c));
+    }
     c->tuning = n;
     c->graph_dirty = true;
     return MLEM_OK;
@@ -1662,6 +1726,9 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
                     // chunked: warp-wide rows; CTAs per SM 4 (bps 4) or 1 (bps 8 -> 1 below);
                     // staged: 4 or 3 CTAs of 256 threads
                     if (chunk_visit(visit) && group != 32) continue;
+                    if (mode == MLEM_BK_CSC && visit != MLEM_VISIT_FILE &&
+                        ensure_csc_vis(c) != MLEM_OK)
+                        continue;  // e.g. no memory for the second CSC: skip
                     const int ctas = visit == MLEM_VISIT_SORTED_CHUNKED ? (bps == 8 ? 1 : bps)
                                      : visit == MLEM_VISIT_SORTED_STAGED ? (bps == 8 ? 3 : bps)
                                                                          : bps;
@@ -1688,6 +1755,13 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
     cudaFree(saved);
     c->device_bytes -= xb;
     if (best.bk_mode == MLEM_BK_REGION) TRY(ensure_region(c, best.frame_tile));
+    if (!csc_by_visit(c, best) && c->celems_vis) {  // tried, not chosen: give the memory back
+        dev_free(c->celems_vis);
+        dev_free(c->row_pos);
+        c->device_bytes -= (c->Z + 2) * 8 + (size_t)std::max<uint32_t>(c->R, 1) * 4;
+        c->celems_vis = nullptr;
+        c->row_pos = nullptr;
+    }
     c->tuning = best;
     c->graph_dirty = true;
     if (best_out) *best_out = best;

@@ -27,6 +27,13 @@ struct mlem_ctx {
     uint64_t* col_ptr = nullptr;
     uint2* celems = nullptr;
     bool has_csc = false;
+    // The CSC in visiting order (ensure_csc_vis; built when MLEM_BK_CSC runs
+    // with a sorted visit): each column lists the visiting positions of its
+    // rays (positions in row_order) ascending, with the same col_ptr.  The
+    // forward pass then writes the correlations by visiting position, so a
+    // column's gathers fall on neighbouring, nearly coincident rays.
+    uint2* celems_vis = nullptr;
+    uint32_t* row_pos = nullptr;  // visiting position of every row
     uint32_t max_col_len = 0, max_row_len = 0;
     float* norm = nullptr;       // column sums, device voxel order
     float* norm_nat = nullptr;   // column sums, natural voxel order

@@ -169,7 +169,23 @@ int run(int argc, char** argv) {
             }
     }
     const char* tune = std::getenv("MLEM_B200_AUTOTUNE");
-    if (tune && *tune && std::strcmp(tune, "0") != 0) {
+    const bool autotune = tune && *tune && std::strcmp(tune, "0") != 0;
+    if (!autotune && info.has_csc && !(info.flags & (MLEM_FLAG_EXACT | MLEM_FLAG_MIRROR_KERNELS))) {
+        // The default method stays the deterministic CSC back projection; with
+        // the row order it walks the CSC in visiting order (a second CSC,
+        // built here), whose gathers fall on neighbouring rays.  Without the
+        // row order or the memory for it, the file-order CSC runs.
+        mlem_tuning t;
+        check(mlem_get_tuning(ctx, &t), ctx);
+        t.bk_mode = MLEM_BK_CSC;
+        t.group = 32;
+        t.blocks_per_sm = 4;
+        t.visit = MLEM_VISIT_SORTED;
+        if (mlem_set_tuning(ctx, &t) != MLEM_OK && !csv)
+            std::cout << "CSC in visiting order unavailable (" << mlem_last_error(ctx)
+                      << "); file-order CSC\n";
+    }
+    if (autotune) {
         mlem_tuning t;
         // the mirrored kernels have atomics only: no deterministic choice to restrict to
         const bool any = std::strcmp(tune, "any") == 0 || (info.flags & MLEM_FLAG_MIRROR_KERNELS);

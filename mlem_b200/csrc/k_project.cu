@@ -60,14 +60,15 @@ __global__ void __launch_bounds__(256) k_fwproj(SparseView csr, const float* __r
         slot_allreduce<G, BT>(acc);
         if (active && lane < FL) {
             const uint64_t idx = r * B + f0 + sub * VW;
-            if (y) st_vec<VW>(y + idx, acc);
+            const uint64_t oidx = (csr.out_by_visit ? v : r) * B + f0 + sub * VW;
+            if (y) st_vec<VW>(y + oidx, acc);
             if (c) {
                 int32_t s[VW];
                 ld_counts<VW>(sino + idx, s);
                 float o[VW];
 #pragma unroll
                 for (int i = 0; i < VW; ++i) o[i] = correl_of(s[i], acc[i]);
-                st_vec<VW>(c + idx, o);
+                st_vec<VW>(c + oidx, o);
             }
         }
     }

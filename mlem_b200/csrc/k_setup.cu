@@ -72,9 +72,11 @@ __global__ void k_count_cols(SparseView csr, unsigned long long* __restrict__ cn
 }
 
 // Warp per row: every element gets a slot in its column through an atomic
-// cursor; the slot holds {row, position in row} until the columns are sorted.
+// cursor; the slot holds {row (or its key), position in row} until the
+// columns are sorted.
 __global__ void k_fill_csc(SparseView csr, const uint64_t* __restrict__ col_ptr,
-                           unsigned long long* __restrict__ cursor, uint2* __restrict__ ce) {
+                           unsigned long long* __restrict__ cursor, uint2* __restrict__ ce,
+                           const uint32_t* __restrict__ row_key) {
     const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
     const int lane = threadIdx.x & 31;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -84,7 +86,7 @@ __global__ void k_fill_csc(SparseView csr, const uint64_t* __restrict__ col_ptr,
         for (uint64_t k = b + lane; k < e; k += 32) {
             const uint32_t col = el[k].x;
             const uint64_t slot = col_ptr[col] + atomicAdd(cursor + col, 1ull);
-            ce[slot] = make_uint2((uint32_t)r, (uint32_t)(k - b));
+            ce[slot] = make_uint2(row_key ? row_key[r] : (uint32_t)r, (uint32_t)(k - b));
         }
     }
 }
@@ -169,14 +171,22 @@ __global__ void k_list_long(const uint64_t* __restrict__ col_ptr, uint32_t C,
         if (col_ptr[c + 1] - col_ptr[c] > (uint64_t)kSortCap) list[atomicAdd(count, 1u)] = (uint32_t)c;
 }
 
-// {row, position} -> {row, value}.
-__global__ void k_materialize(SparseView csr, uint2* __restrict__ ce) {
+// {row (or key), position} -> {row (or key), value}.
+__global__ void k_materialize(SparseView csr, uint2* __restrict__ ce,
+                              const uint32_t* __restrict__ key_row) {
     const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
     for (uint64_t s = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; s < csr.nnz;
          s += (uint64_t)gridDim.x * blockDim.x) {
         const uint2 q = ce[s];
-        ce[s] = make_uint2(q.x, el[csr.ptr[q.x] + q.y].y);
+        const uint32_t r = key_row ? key_row[q.x] : q.x;
+        ce[s] = make_uint2(q.x, el[csr.ptr[r] + q.y].y);
     }
+}
+
+__global__ void k_invert(const uint32_t* __restrict__ order, uint32_t* __restrict__ pos, uint64_t n) {
+    for (uint64_t v = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; v < n;
+         v += (uint64_t)gridDim.x * blockDim.x)
+        pos[order[v]] = (uint32_t)v;
 }
 
 __global__ void k_validate(SparseView csr, uint32_t C, unsigned int* __restrict__ bad) {
@@ -424,8 +434,15 @@ size_t transpose_scratch_bytes(uint32_t C) {
            + scan_scratch_bytes((uint64_t)C);
 }
 
+cudaError_t invert_permutation(const uint32_t* order, uint32_t* pos, uint64_t n, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_invert<<<kB200SMs * 8, 256, 0, st>>>(order, pos, n);
+    return cudaGetLastError();
+}
+
 cudaError_t transpose(const SparseView& csr, uint32_t C, uint64_t* col_ptr, uint2* ce,
-                      void* scratch, uint32_t* max_col_len, cudaStream_t st) {
+                      void* scratch, uint32_t* max_col_len, cudaStream_t st,
+                      const uint32_t* row_key, const uint32_t* key_row) {
     char* p = static_cast<char*>(scratch);
     unsigned long long* cnt = reinterpret_cast<unsigned long long*>(p);
     p += align256(((size_t)C + 1) * 8);
@@ -451,7 +468,7 @@ cudaError_t transpose(const SparseView& csr, uint32_t C, uint64_t* col_ptr, uint
         return cudaStreamSynchronize(st);
     }
     MLEM_TRY(cudaMemsetAsync(cnt, 0, ((size_t)C + 1) * 8, st));
-    k_fill_csc<<<grid, 256, 0, st>>>(csr, col_ptr, cnt, ce);
+    k_fill_csc<<<grid, 256, 0, st>>>(csr, col_ptr, cnt, ce, row_key);
     MLEM_TRY(cudaGetLastError());
     k_col_len_max<<<kB200SMs * 2, 256, 0, st>>>(col_ptr, C, counters);
     MLEM_TRY(cudaGetLastError());
@@ -491,7 +508,7 @@ cudaError_t transpose(const SparseView& csr, uint32_t C, uint64_t* col_ptr, uint
         MLEM_TRY(cudaStreamSynchronize(st));
         cudaFree(tmp);
     }
-    k_materialize<<<grid, 256, 0, st>>>(csr, ce);
+    k_materialize<<<grid, 256, 0, st>>>(csr, ce, key_row);
     MLEM_TRY(cudaGetLastError());
     return cudaStreamSynchronize(st);
 #undef MLEM_TRY

@@ -36,6 +36,10 @@ struct SparseView {
     // k_fused_staged) visit *n_dev positions of order/vrange instead of n: a
     // visiting list built on the device (active_rows_build), n its capacity.
     const uint32_t* n_dev = nullptr;
+    // k_fwproj only: write the row's outputs (correlation, projection) at its
+    // visiting position instead of its row index -- the layout the CSC in
+    // visiting order (mlem_ctx::celems_vis) gathers from.
+    bool out_by_visit = false;
 };
 
 // Row index of visiting position v.
@@ -220,8 +224,15 @@ cudaError_t exclusive_scan_u64(const uint64_t* in, uint64_t* out, uint64_t n, vo
 // transpose_scratch_bytes(C) bytes.  Result is identical to a stable
 // counting-sort transpose (ascending row, then in-row position).
 size_t transpose_scratch_bytes(uint32_t C);
+// CSR -> CSC.  Each column lists its rows ascending.  With row_key (and its
+// inverse key_row), row r is stored as row_key[r] and the columns list those
+// keys ascending: with the visiting positions of the row order as keys, a
+// column lists its rays in visiting order.
 cudaError_t transpose(const SparseView& csr, uint32_t C, uint64_t* col_ptr, uint2* celems,
-                      void* scratch, uint32_t* max_col_len, cudaStream_t st);
+                      void* scratch, uint32_t* max_col_len, cudaStream_t st,
+                      const uint32_t* row_key = nullptr, const uint32_t* key_row = nullptr);
+// pos[order[v]] = v for a permutation order of [0, n).
+cudaError_t invert_permutation(const uint32_t* order, uint32_t* pos, uint64_t n, cudaStream_t st);
 
 // ---- row visiting order (k_order.cu) -------------------------------------------
 // order[k]: rows sorted by a key that interleaves the bits of the device

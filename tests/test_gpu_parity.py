@@ -121,6 +121,51 @@ def test_csc_mode_is_deterministic(ctxs):
     assert a.tobytes() == b.tobytes()
 
 
+def test_csc_in_visiting_order_is_deterministic(golden):
+    """The CSC method with the sorted visit gathers the correlations by
+    visiting position from a CSC in that order: reproducible to the bit, in
+    one context or another, whole or step by step."""
+    m, sino, iters, gold, _ = golden.case("plain_small_it10")
+    imgs = []
+    for _ in range(2):
+        with api.Context.from_matrix(m) as ctx:
+            ctx.set_sinograms(sino)
+            ctx.set_tuning(bk_mode=api.BK_CSC, group=16, frame_tile=1, blocks_per_sm=4,
+                           visit=api.VISIT_SORTED)
+            ctx.init_images()
+            ctx.iterate(iters)
+            imgs.append(ctx.get_images())
+            ctx.init_images()
+            for _ in range(iters):
+                ctx.iterate(1)
+            imgs.append(ctx.get_images())
+    assert all(x.tobytes() == imgs[0].tobytes() for x in imgs)
+    assert ob.rel_l2(imgs[0][0], gold) <= TOL_MLEM
+
+
+@pytest.mark.parametrize("group,tile", [(32, 1), (16, 4), (8, 16)])
+def test_csc_in_visiting_order_with_frames(golden, group, tile):
+    m, sino, iters, gold, _ = golden.case("tiny_it10")
+    rng = np.random.default_rng(7 * tile)
+    B = 16
+    sinos = np.stack([rng.permutation(sino) if b else sino for b in range(B)]).astype(np.int32)
+    with api.Context.from_matrix(m) as ctx:
+        ctx.set_sinograms(sinos)
+        ctx.set_tuning(bk_mode=api.BK_CSC, group=group, frame_tile=tile, blocks_per_sm=8,
+                       visit=api.VISIT_SORTED)
+        ctx.init_images()
+        ctx.iterate(iters)
+        imgs = ctx.get_images()
+        # the device-pointer and host-buffer projections stay in row order
+        x = np.full(m.n_cols, 1.25, np.float32)
+        assert ob.rel_l2(ctx.fwproj(x), ob.fwproj(m, x)) <= TOL_PROJ
+        c = ob.correl(ob.fwproj(m, x), sino)
+        assert ob.rel_l2(ctx.bkproj(c), ob.bkproj(m, c)) <= TOL_PROJ
+    for b in range(B):
+        want, _ = ob.mlem(m, sinos[b], iters)
+        assert ob.rel_l2(imgs[b], want) <= TOL_MLEM, b
+
+
 @pytest.mark.parametrize("group,tile", [(8, 1), (16, 4), (32, 8), (32, 16), (16, 16), (4, 16)])
 @pytest.mark.parametrize("mode", MODES)
 def test_batched_frames_match_separate_runs(golden, group, tile, mode):
