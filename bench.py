@@ -21,7 +21,8 @@ Besides the headline line, at one GPU:
   The reference binary and the oracle run as background processes on the
   host cores while the GPU lines are measured;
 * osem, differentiable, skewed, uneven (three matrices of different
-  geometry batched), mirrored (a symmetry-compressed matrix).
+  geometry batched), mirrored (a symmetry-compressed matrix), matrix_free
+  (the rays traced in every pass instead of a stored matrix).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--parallelism single|shards|replicas]
@@ -88,6 +89,7 @@ def parse_args():
                     help="skip the uneven three-geometry batch (one GPU only)")
     ap.add_argument("--no-mirrored", action="store_true",
                     help="skip the symmetry-compressed matrix, expanded vs mirrored kernels (one GPU only)")
+    ap.add_argument("--no-matrix-free", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true",
                     help="skip the host-core legs (openmpcsr4mlem timing and the full-size parity)")
     ap.add_argument("--no-parity-full", action="store_true")
@@ -549,6 +551,15 @@ def run_ours(a, rank, world, local_rank, parallelism):
             torch.cuda.synchronize()
             detail["mirrored"] = mirrored.run(iters=10, warmup=3, device=local_rank)
 
+        # --- matrix-free: the rays traced in every pass instead of the stored matrix ---
+        if world == 1 and not a.no_matrix_free:
+            torch.cuda.synchronize()
+            mfl, mf_img = matrix_free_line(a, frames.sinograms[0], stream, barrier, ms_per_step,
+                                           pf["fast"] if pf else None)
+            detail["matrix_free"] = mfl
+            if pf is not None:
+                pf["matrix_free"] = mf_img
+
         # --- full-size parity, host side: wait for the reference binary and the oracle ---
         if jobs is not None:
             tail["parity_full"] = parity_finish(jobs, pf, a.parity_iters)
@@ -656,6 +667,9 @@ def parity_finish(jobs, pf, n):
     else:
         p["cli_error"] = pf.get("cli_error")
     res["plain"] = p
+    if "matrix_free" in pf:
+        p["matrix_free_vs_seq"] = sig(rel_l2(pf["matrix_free"], seq))
+        p["matrix_free_vs_f64"] = sig(rel_l2(pf["matrix_free"], f64))
     if "batched_frame" in ref and "batch_frame" in pf:
         bseq, bf64 = ref["batched_frame"]
         res["batched"] = {"frame": pf["kf"],
@@ -667,6 +681,52 @@ def parity_finish(jobs, pf, n):
              for k, v in blk.items() if k.endswith("_vs_seq") or k == "max_frame_vs_single_run"]
     res["ok"] = bool(worst) and all(v is not None and v <= TOL for v in worst)
     return res
+
+
+def matrix_free_line(a, sino, stream, barrier, ms_stored, fast_img):
+    """The matrix-free prototype (mlem_mf_*): the plain-full rays kept as
+    104-byte descriptors and traced again in every pass.  Device-timed
+    iterations, its device memory, and its image after the parity iteration
+    count against the stored path's (the same iterations); the 256x256x96
+    geometry (16.8M rays, whose stored matrix is 41 GB) timed alone."""
+    import numpy as np
+    import torch
+
+    from mlem_b200 import api, synth
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    out = {}
+    img = None
+    for name in ("plain-full", "uneven-large"):
+        g = synth.WORKLOADS[name].geometry
+        with api.MatrixFree(g) as mf:
+            mf.set_stream(stream.cuda_stream)
+            if name == "plain-full":
+                s = sino
+            else:  # a uniform-count stand-in: every ray walked, nothing skipped
+                s = np.full(g.n_rows, 50, np.int32)
+            mf.set_sinogram(s)
+            mf.init_image()
+            mf.iterate(3)
+            k = max(5, min(a.steps, 20))
+            barrier()
+            e0.record(stream)
+            mf.iterate(k)
+            e1.record(stream)
+            barrier()
+            ms = e0.elapsed_time(e1) / k
+            info = mf.info()
+            entry = {"ms_per_iteration": round(ms, 4), "device_bytes": info["device_bytes"],
+                     "rays": g.n_rows}
+            if name == "plain-full":
+                entry["stored_ms_per_iteration"] = round(ms_stored, 4)
+                mf.init_image()
+                mf.iterate(a.parity_iters)
+                img = mf.get_image()
+                if fast_img is not None:
+                    entry["rel_l2_vs_stored_path"] = sig(rel_l2(img, fast_img))
+                    entry["iterations"] = a.parity_iters
+            out[name] = entry
+    return out, img
 
 
 def osem_line(ctx, a, sinograms, stream, barrier, ms_per_step):

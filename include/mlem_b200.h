@@ -316,6 +316,38 @@ int mlem_set_norm_d(mlem_ctx* ctx, const float* norm, void* stream);
  * generator's; used for synthetic sinogram means).  Host buffers. */
 int mlem_project_f64(mlem_ctx* ctx, const float* x, double* out);
 
+/* ---- matrix-free iteration (prototype) ------------------------------------
+ * No counterpart in the reference, which reads a stored CSR4 matrix from an
+ * external generator (README.md:35-36).  For the synthetic Siddon geometry
+ * (mlem_create_siddon's parameters) the matrix is never stored: every ray is
+ * kept as a small descriptor of the generator's accepted line (entry point,
+ * direction, alpha range inside the grid: 104 bytes instead of about 8 bytes
+ * per element) and traced again, in double, in every pass.  One iteration is
+ * one pass per ray: forward projection, calcCorrel and the scatter of the
+ * traced elements, then calcUpdate.  The traced lengths equal the generator's
+ * up to rounding (a voxel cut by a lane's interval boundary is traced as two
+ * pieces), so results agree with a stored-matrix context of the same
+ * geometry within the float tolerance, not bit for bit.  Rays whose count is
+ * zero are skipped.  One frame; images in natural voxel order.  A walk whose
+ * interval held more elements than its bound returns MLEM_ERR_CUDA (the bound
+ * follows from the grid's diagonal, so this does not happen). */
+typedef struct mlem_mf mlem_mf;
+int mlem_mf_create_siddon(mlem_mf** out, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t n_rows,
+                          uint32_t min_count, uint32_t max_count, double radius_scale,
+                          double min_len, uint64_t seed, int device);
+void mlem_mf_destroy(mlem_mf* mf);
+int mlem_mf_set_stream(mlem_mf* mf, void* stream);
+/* Column sums (traced once at creation), natural voxel order, float[C]. */
+int mlem_mf_column_sums(mlem_mf* mf, float* norm);
+/* Upload the int32[R] sinogram (host buffer). */
+int mlem_mf_set_sinogram(mlem_mf* mf, const int32_t* sino);
+/* initImage (seqcsr4mlem.cpp:52-66); init_value (may be NULL) receives the value. */
+int mlem_mf_init_image(mlem_mf* mf, float* init_value);
+int mlem_mf_iterate(mlem_mf* mf, int n_iter);
+int mlem_mf_get_image(mlem_mf* mf, float* image);
+/* Device bytes held (descriptors, vectors, voxel order) and the per-lane element bound. */
+int mlem_mf_info(const mlem_mf* mf, uint64_t* device_bytes, uint32_t* lane_capacity);
+
 /* ---- allocation-free iteration ------------------------------------------- */
 /* No counterpart in the reference.  Every other entry point keeps working
  * vectors in device memory the library allocates.  This one is for callers

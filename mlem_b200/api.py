@@ -565,6 +565,67 @@ def mlem(matrix: Context, lmsino, image: Optional[np.ndarray] = None, nIteration
     return out, sums
 
 
+class MatrixFree:
+    """Matrix-free MLEM on the synthetic Siddon geometry (mlem_mf_*): the rays
+    are traced again in every pass instead of streaming a stored matrix.
+    One frame; natural voxel order."""
+
+    def __init__(self, g, device: int = 0):
+        h = ctypes.c_void_p()
+        _raise(core_lib().mlem_mf_create_siddon(ctypes.byref(h), g.nx, g.ny, g.nz, g.n_rows,
+                                                g.min_count, g.max_count, g.radius_scale,
+                                                g.min_len, g.seed, device))
+        self._h = h
+        self.n_rows, self.n_cols = g.n_rows, g.n_cols
+
+    def close(self):
+        if self._h:
+            core_lib().mlem_mf_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream: int = 0) -> None:
+        _raise(core_lib().mlem_mf_set_stream(self._h, stream or None))
+
+    def column_sums(self) -> np.ndarray:
+        out = np.zeros(self.n_cols, np.float32)
+        _raise(core_lib().mlem_mf_column_sums(self._h, _p(out)))
+        return out
+
+    def set_sinogram(self, sino) -> None:
+        s = _i32(sino, self.n_rows, "sinogram")
+        _raise(core_lib().mlem_mf_set_sinogram(self._h, _p(s)))
+
+    def init_image(self) -> float:
+        v = ctypes.c_float()
+        _raise(core_lib().mlem_mf_init_image(self._h, ctypes.byref(v)))
+        return float(v.value)
+
+    def iterate(self, n: int) -> None:
+        _raise(core_lib().mlem_mf_iterate(self._h, n))
+
+    def get_image(self) -> np.ndarray:
+        out = np.zeros(self.n_cols, np.float32)
+        _raise(core_lib().mlem_mf_get_image(self._h, _p(out)))
+        return out
+
+    def info(self) -> dict:
+        b, cap = ctypes.c_uint64(), ctypes.c_uint32()
+        _raise(core_lib().mlem_mf_info(self._h, ctypes.byref(b), ctypes.byref(cap)))
+        return {"device_bytes": int(b.value), "lane_capacity": int(cap.value)}
+
+
 NOALLOC_MAX_VOXELS = 1048576
 
 

@@ -849,6 +849,10 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
     bytes[3] = 4.0 * C * B;
     launches[3] = 2;
 }
+
+void voxel_permutation(uint32_t nx, uint32_t ny, uint32_t nz, std::vector<uint32_t>& perm) {
+    brick_order(nx, ny, nz, perm);
+}
 }  // namespace mlem
 
 namespace {

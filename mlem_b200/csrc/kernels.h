@@ -267,6 +267,10 @@ struct SiddonSpec {
     uint64_t seed;
 };
 cudaError_t siddon_counts(const SiddonSpec& s, uint64_t* counts, cudaStream_t st);
+// The device voxel order of a grid (capi.cu): perm[natural index] = device
+// index, the Morton code of (ix, iy, iz) with x lowest (ranked when a
+// dimension is not a power of two).
+void voxel_permutation(uint32_t nx, uint32_t ny, uint32_t nz, std::vector<uint32_t>& perm);
 cudaError_t siddon_fill(const SiddonSpec& s, const uint64_t* row_ptr, uint2* elems,
                         cudaStream_t st);
 // out[r] = sequential double sum of v_k * x[col_k] (bit-identical to the host).
