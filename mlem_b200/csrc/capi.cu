@@ -793,10 +793,9 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
         // one region-major element copy and the segment rows per pass; per
         // segment one partial (forward) or one correlation (backward) of B
         // floats; x once, fw zeroing + correl pass over R x B
-        const double S = (double)c->rb.nseg, ZR = (double)c->rb.nel;
-        const double pass = 8.0 * ZR + 4.0 * S;
-        bytes[0] = tiles * pass + B * (4.0 * C + 4.0 * S) + B * 16.0 * R;
-        bytes[1] = tiles * pass + B * (4.0 * S + 8.0 * C) + 4.0 * C;  // c per segment, x r/w, norm
+        const double S = (double)c->rb.nseg, ZR = (double)c->rb.nel, ZB = (double)c->rb.nel_bk;
+        bytes[0] = tiles * (8.0 * ZR + 4.0 * S) + B * (4.0 * C + 4.0 * S) + B * 16.0 * R;
+        bytes[1] = tiles * (8.0 * ZB + 4.0 * S) + B * (4.0 * S + 8.0 * C) + 4.0 * C;  // c per segment, x r/w, norm
         launches[0] = nt + 1;
         launches[1] = nt;
         bytes[3] = 4.0 * C * B;

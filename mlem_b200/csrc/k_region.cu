@@ -218,51 +218,75 @@ __global__ void k_pad(uint32_t nblk, uint32_t gpw, const uint64_t* __restrict__ 
 }
 
 // Voxel-major copy of every block: CTA per block, counting sort of its
-// elements by voxel (shared-memory histogram, scan, scatter).  The order
-// inside one voxel's run is whatever the scatter atomics give.
-__global__ void __launch_bounds__(512) k_fill_bk(int rlog, uint32_t gpw,
-                                                 const uint64_t* __restrict__ blk_raw,
-                                                 const uint64_t* __restrict__ blk_el_ptr,
-                                                 const uint2* __restrict__ el_fw,
-                                                 uint2* __restrict__ el_bk) {
-    extern __shared__ uint32_t hist[];  // RS counters, then blockDim.x partial sums
+// elements by voxel (shared-memory histogram, run placement, scatter).  The
+// order inside one voxel's run is whatever the scatter atomics give.  The
+// spans of the copy hold whole runs: a run of at most kSpan elements that
+// would cross a span boundary starts the next span instead (the gap is
+// padded with value-0 elements of the run before it), and a longer run
+// starts a span of its own and pads its last one, so a span holds either
+// whole runs or one piece of a single run.  The back projection then adds a
+// run into the shared update tile with a plain read-modify-write, and uses
+// atomics only for a span of one voxel (which may be such a piece).  A pad
+// element's word carries segment 0 of its block (it adds 0 x that segment's
+// correlation).  COUNT: the padded length of every block, whole tiles;
+// otherwise the copy.
+template <bool COUNT>
+__global__ void __launch_bounds__(512) k_bk_layout(int rlog, uint32_t gpw,
+                                                   const uint64_t* __restrict__ blk_raw,
+                                                   const uint64_t* __restrict__ blk_el_ptr,
+                                                   const uint2* __restrict__ el_fw,
+                                                   uint64_t* __restrict__ bk_plen,
+                                                   const uint64_t* __restrict__ bk_el_ptr,
+                                                   uint2* __restrict__ el_bk) {
+    extern __shared__ uint32_t hist[];  // RS counters, then the run starts
     const uint32_t RS = 1u << rlog, mask = RS - 1u;
-    uint32_t* partial = hist + RS;
+    const uint64_t tile = (uint64_t)gpw * kSpan;
     const uint64_t len = blk_raw[blockIdx.x + 1] - blk_raw[blockIdx.x];
     const uint2* src = el_fw + blk_el_ptr[blockIdx.x];
-    uint2* dst = el_bk + blk_el_ptr[blockIdx.x];
+    uint2* dst = COUNT ? nullptr : el_bk + bk_el_ptr[blockIdx.x];
     for (uint32_t i = threadIdx.x; i < RS; i += blockDim.x) hist[i] = 0;
     __syncthreads();
     for (uint64_t i = threadIdx.x; i < len; i += blockDim.x)
         atomicAdd(hist + (src[span_pos(i, gpw)].x & mask), 1u);
     __syncthreads();
-    const uint32_t per = (RS + blockDim.x - 1) / blockDim.x;
-    const uint32_t lo = min(RS, threadIdx.x * per), hi = min(RS, lo + per);
-    uint32_t sum = 0;
-    for (uint32_t i = lo; i < hi; ++i) sum += hist[i];
-    partial[threadIdx.x] = sum;
-    __syncthreads();
     if (threadIdx.x == 0) {
-        uint32_t run = 0;
-        for (uint32_t t = 0; t < blockDim.x; ++t) {
-            const uint32_t v = partial[t];
-            partial[t] = run;
-            run += v;
+        uint64_t pos = 0;
+        uint32_t last = 0;
+        auto pad_to = [&](uint64_t end, uint32_t word) {
+            if (!COUNT)
+                for (uint64_t p = pos; p < end; ++p) dst[span_pos(p, gpw)] = make_uint2(word, 0u);
+            pos = end;
+        };
+        for (uint32_t v = 0; v < RS; ++v) {
+            const uint32_t c = hist[v];
+            if (c == 0) continue;
+            const uint64_t up = cdiv(pos, kSpan) * kSpan;  // the next span boundary
+            if (c <= kSpan) {
+                if ((pos % kSpan) + c > kSpan) pad_to(up, last);
+            } else if (pos % kSpan) {
+                pad_to(up, last);
+            }
+            if (!COUNT) hist[v] = (uint32_t)pos;  // the run's first position
+            pos += c;
+            if (c > kSpan) {  // the long run's last span holds nothing else
+                const uint64_t end = cdiv(pos, kSpan) * kSpan;
+                if (!COUNT)
+                    for (uint64_t p = pos; p < end; ++p) dst[span_pos(p, gpw)] = make_uint2(v, 0u);
+                pos = end;
+            }
+            last = v;
         }
+        const uint64_t plen = cdiv(pos, tile) * tile;
+        pad_to(plen, last);
+        if (COUNT) bk_plen[blockIdx.x] = plen;
     }
     __syncthreads();
-    uint32_t run = partial[threadIdx.x];
-    for (uint32_t i = lo; i < hi; ++i) {
-        const uint32_t v = hist[i];
-        hist[i] = run;
-        run += v;
-    }
-    __syncthreads();
-    for (uint64_t i = threadIdx.x; i < len; i += blockDim.x) {
-        const uint2 q = src[span_pos(i, gpw)];
-        const uint32_t pos = atomicAdd(hist + (q.x & mask), 1u);
-        dst[span_pos(pos, gpw)] = q;
-    }
+    if (!COUNT)
+        for (uint64_t i = threadIdx.x; i < len; i += blockDim.x) {
+            const uint2 q = src[span_pos(i, gpw)];
+            const uint32_t p = atomicAdd(hist + (q.x & mask), 1u);
+            dst[span_pos(p, gpw)] = q;
+        }
 }
 
 // --- iteration kernels ---------------------------------------------------------
@@ -317,6 +341,7 @@ __global__ void __launch_bounds__(kRbThreads) k_rb_fwproj(RegionView rv, const f
     for (uint64_t t0 = E0 + (uint64_t)warp * TILE; t0 < E1; t0 += (uint64_t)nwarps * TILE) {
         const uint2* __restrict__ sp = rv.el_fw + t0 + grp;  // element k of the span: sp[k * GPW]
         uint32_t cur = 0xffffffffu;
+        uint32_t row = 0;  // srow[cur], loaded when the segment starts (used at its flush)
         float acc[VW];
 #pragma unroll
         for (int i = 0; i < VW; ++i) acc[i] = 0.0f;
@@ -330,8 +355,9 @@ __global__ void __launch_bounds__(kRbThreads) k_rb_fwproj(RegionView rv, const f
                 const uint32_t seg = q[j].x >> rv.rlog;
                 if (seg != cur) {
                     if (cur != 0xffffffffu)
-                        red_vec<VW>(fw + (uint64_t)srow[cur] * B + f0 + sub * VW, 1.0f, acc);
+                        red_vec<VW>(fw + (uint64_t)row * B + f0 + sub * VW, 1.0f, acc);
                     cur = seg;
+                    row = srow[seg];
 #pragma unroll
                     for (int i = 0; i < VW; ++i) acc[i] = 0.0f;
                 }
@@ -342,7 +368,7 @@ __global__ void __launch_bounds__(kRbThreads) k_rb_fwproj(RegionView rv, const f
                 for (int i = 0; i < VW; ++i) acc[i] += w * t[i];
             }
         }
-        red_vec<VW>(fw + (uint64_t)srow[cur] * B + f0 + sub * VW, 1.0f, acc);
+        red_vec<VW>(fw + (uint64_t)row * B + f0 + sub * VW, 1.0f, acc);
     }
 }
 
@@ -387,7 +413,7 @@ __global__ void __launch_bounds__(kRbThreads, 2) k_rb_bkproj(RegionView rv, cons
             }
         }
         __syncthreads();
-        const uint64_t E0 = rv.blk_el_ptr[b], E1 = rv.blk_el_ptr[b + 1];  // whole tiles
+        const uint64_t E0 = rv.bk_el_ptr[b], E1 = rv.bk_el_ptr[b + 1];  // whole tiles
         for (uint64_t t0 = E0 + (uint64_t)warp * TILE; t0 < E1; t0 += (uint64_t)nwarps * TILE) {
             const uint2* __restrict__ sp = rv.el_bk + t0 + grp;
             uint32_t cur = 0xffffffffu;
@@ -405,22 +431,15 @@ __global__ void __launch_bounds__(kRbThreads, 2) k_rb_bkproj(RegionView rv, cons
                     const uint32_t vox = q[j].x & mask;
                     if (vox != cur) {
                         if (cur != 0xffffffffu) {
-                            // A run that started after the span's first element and
-                            // ended before its last is in no other span: this lane
-                            // group owns the voxel, a plain read-modify-write does.
-                            // The first (and last) run may be shared with the
-                            // neighbouring span: atomics.
+                            // The spans hold whole runs (k_bk_layout): a run that
+                            // ends inside the span is in no other span, and this
+                            // lane group adds it with a plain read-modify-write.
                             float* dst = ut + cur * BT + sub * VW;
-                            if (first) {
+                            float t[VW];
+                            lds_vec<VW>(dst, t);
 #pragma unroll
-                                for (int i = 0; i < VW; ++i) atomicAdd(dst + i, acc[i]);
-                            } else {
-                                float t[VW];
-                                lds_vec<VW>(dst, t);
-#pragma unroll
-                                for (int i = 0; i < VW; ++i) t[i] += acc[i];
-                                sts_vec<VW>(dst, t);
-                            }
+                            for (int i = 0; i < VW; ++i) t[i] += acc[i];
+                            sts_vec<VW>(dst, t);
                             first = false;
                         }
                         cur = vox;
@@ -434,8 +453,19 @@ __global__ void __launch_bounds__(kRbThreads, 2) k_rb_bkproj(RegionView rv, cons
                     for (int i = 0; i < VW; ++i) acc[i] += w * cv[i];
                 }
             }
+            // the span's last run: whole (plain), unless the span holds one voxel
+            // only, which may be a piece of a run longer than a span (atomics)
+            float* dst = ut + cur * BT + sub * VW;
+            if (first) {
 #pragma unroll
-            for (int i = 0; i < VW; ++i) atomicAdd(ut + cur * BT + sub * VW + i, acc[i]);
+                for (int i = 0; i < VW; ++i) atomicAdd(dst + i, acc[i]);
+            } else {
+                float t[VW];
+                lds_vec<VW>(dst, t);
+#pragma unroll
+                for (int i = 0; i < VW; ++i) t[i] += acc[i];
+                sts_vec<VW>(dst, t);
+            }
         }
     }
     __syncthreads();
@@ -645,21 +675,35 @@ cudaError_t region_build(const SparseView& csr, uint32_t C, int rlog, int sblog,
     const uint64_t Z = h_el_ptr[nreg];
     MLEM_TRY(keep((void**)&out->seg_row, S * 4));
     MLEM_TRY(keep((void**)&out->el_fw, Z * 8));
-    MLEM_TRY(keep((void**)&out->el_bk, Z * 8));
     if (S) {
         k_fill_fw<<<grid, 256, 0, st>>>(csr, rlog, sblog, gpw, S, order, region_sorted, seg_start,
                                         seg_row, seg_len, el_off, out->reg_seg_ptr, out->reg_blk_ptr,
                                         blk_raw, out->blk_el_ptr, out->seg_row, out->el_fw);
         MLEM_TRY(cudaGetLastError());
     }
+    // the voxel-major copy: its block lengths (run-aligned spans), offsets, then the copy
+    MLEM_TRY(keep((void**)&out->bk_el_ptr, ((uint64_t)nblk + 1) * 8));
+    uint64_t Zb = 0;
     if (nblk) {
         k_pad<<<grid, 256, 0, st>>>(nblk, gpw, blk_raw, out->blk_el_ptr, out->el_fw);
         MLEM_TRY(cudaGetLastError());
-        MLEM_TRY(set_smem_all(k_fill_bk, fill_smem(14)));  // the largest region any build uses
-        k_fill_bk<<<nblk, 512, fill_smem(rlog), st>>>(rlog, gpw, blk_raw, out->blk_el_ptr,
-                                                      out->el_fw, out->el_bk);
+        // the largest region any build uses
+        MLEM_TRY(set_smem_all(k_bk_layout<true>, fill_smem(14)));
+        MLEM_TRY(set_smem_all(k_bk_layout<false>, fill_smem(14)));
+        k_bk_layout<true><<<nblk, 512, fill_smem(rlog), st>>>(rlog, gpw, blk_raw, out->blk_el_ptr,
+                                                            out->el_fw, blk_plen, nullptr, nullptr);
         MLEM_TRY(cudaGetLastError());
-        k_pad<<<grid, 256, 0, st>>>(nblk, gpw, blk_raw, out->blk_el_ptr, out->el_bk);
+        MLEM_TRY(exclusive_scan_u64(blk_plen, out->bk_el_ptr, nblk, scan_tmp_b, scan_bytes_b, st));
+        MLEM_TRY(cudaMemcpyAsync(&Zb, out->bk_el_ptr + nblk, 8, cudaMemcpyDeviceToHost, st));
+        MLEM_TRY(cudaStreamSynchronize(st));
+    } else {
+        MLEM_TRY(cudaMemsetAsync(out->bk_el_ptr, 0, 8, st));
+    }
+    MLEM_TRY(keep((void**)&out->el_bk, Zb * 8));
+    if (nblk) {
+        k_bk_layout<false><<<nblk, 512, fill_smem(rlog), st>>>(rlog, gpw, blk_raw, out->blk_el_ptr,
+                                                             out->el_fw, nullptr, out->bk_el_ptr,
+                                                             out->el_bk);
         MLEM_TRY(cudaGetLastError());
     }
     MLEM_TRY(cudaStreamSynchronize(st));
@@ -668,13 +712,15 @@ cudaError_t region_build(const SparseView& csr, uint32_t C, int rlog, int sblog,
 #undef MLEM_TRY
     out->nseg = S;
     out->nel = Z;
+    out->nel_bk = Zb;
     *bytes_out = bytes;
     return cudaSuccess;
 }
 
 void region_free(RegionBlocks* rb) {
     for (void* p : {(void*)rb->reg_order, (void*)rb->reg_seg_ptr, (void*)rb->reg_el_ptr,
-                    (void*)rb->reg_blk_ptr, (void*)rb->blk_el_ptr, (void*)rb->seg_row,
+                    (void*)rb->reg_blk_ptr, (void*)rb->blk_el_ptr, (void*)rb->bk_el_ptr,
+                    (void*)rb->seg_row,
                     (void*)rb->el_fw, (void*)rb->el_bk})
         if (p) cudaFree(p);
     *rb = RegionBlocks{};

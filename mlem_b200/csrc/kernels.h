@@ -293,7 +293,8 @@ struct RegionView {
     const uint64_t* reg_seg_ptr;  // nreg+1 segment ranges
     const uint64_t* reg_el_ptr;   // nreg+1 element ranges
     const uint32_t* reg_blk_ptr;  // nreg+1 block ranges
-    const uint64_t* blk_el_ptr;   // nblk+1 element ranges
+    const uint64_t* blk_el_ptr;   // nblk+1 element ranges of the segment-major copy
+    const uint64_t* bk_el_ptr;    // nblk+1 element ranges of the voxel-major copy
     const uint32_t* seg_row;
     const uint2* el_fw;
     const uint2* el_bk;
@@ -307,15 +308,17 @@ struct RegionBlocks {
     uint64_t* reg_el_ptr = nullptr;
     uint32_t* reg_blk_ptr = nullptr;
     uint64_t* blk_el_ptr = nullptr;
+    uint64_t* bk_el_ptr = nullptr;
     uint32_t* seg_row = nullptr;
     uint2* el_fw = nullptr;
     uint2* el_bk = nullptr;
     uint32_t nreg = 0, nblk = 0;
-    uint64_t nseg = 0, nel = 0;  // nel: elements of one copy, padding included
+    uint64_t nseg = 0, nel = 0;  // nel: elements of the segment-major copy, padding included
+    uint64_t nel_bk = 0;         // the same for the voxel-major copy (run-aligned spans)
     int rlog = 0, sblog = 0;
     uint32_t gpw = 0;            // lane groups per warp the copies are interleaved for
     RegionView view() const {
-        return RegionView{reg_order, reg_seg_ptr, reg_el_ptr, reg_blk_ptr, blk_el_ptr,
+        return RegionView{reg_order, reg_seg_ptr, reg_el_ptr, reg_blk_ptr, blk_el_ptr, bk_el_ptr,
                           seg_row,   el_fw,       el_bk,      nreg,        rlog,       sblog};
     }
 };
