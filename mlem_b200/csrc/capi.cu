@@ -1276,6 +1276,7 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->act_flags, (void*)c->act_tmp, (void*)c->act_n, (void*)c->act_z,
                     (void*)c->celems_vis, (void*)c->row_pos})
         dev_free(p);
+    if (c->act_host) cudaFreeHost(c->act_host);
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
@@ -1556,6 +1557,18 @@ int mlem_step_host(mlem_ctx* c, const int32_t* sino, float* images, uint32_t B) 
     TRY(upload_frames<int32_t>(c, sino, c->sino, c->R));
     TRY(build_active(c, false));
     ++c->sino_gen;
+    // the list's row and element counts for mlem_get_info: copied with the
+    // step, read after its final synchronisation
+    if (c->act_ready && !c->act_host &&
+        cudaHostAlloc(reinterpret_cast<void**>(&c->act_host), 16, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        c->act_host = nullptr;
+    }
+    const bool counts = c->act_ready && c->act_host;
+    if (counts) {
+        CK(c, cudaMemcpyAsync(c->act_host, c->act_n, 4, cudaMemcpyDeviceToHost, c->stream));
+        CK(c, cudaMemcpyAsync(c->act_host + 1, c->act_z, 8, cudaMemcpyDeviceToHost, c->stream));
+    }
     TRY(upload_frames<float>(c, images, c->x, c->C));
     c->images_ready = true;
     if (c->tuning.bk_mode == MLEM_BK_REGION && !(c->flags & MLEM_FLAG_EXACT))
@@ -1567,6 +1580,13 @@ int mlem_step_host(mlem_ctx* c, const int32_t* sino, float* images, uint32_t B) 
     CK(c, cudaGraphLaunch(c->graph, c->stream));
     TRY(download_images(c, images));
     CK(c, cudaStreamSynchronize(c->stream));
+    if (counts) {
+        c->act_rows = static_cast<uint32_t>(c->act_host[0] & 0xffffffffull);
+        c->act_nnz = c->act_host[1];
+    } else if (!c->act_ready) {
+        c->act_rows = 0;
+        c->act_nnz = 0;
+    }
     return MLEM_OK;
 }
 

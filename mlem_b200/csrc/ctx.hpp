@@ -68,6 +68,9 @@ struct mlem_ctx {
     bool act_ready = false;
     uint32_t act_rows = 0;
     uint64_t act_nnz = 0;
+    // pinned host copy of act_n / act_z, read after mlem_step_host's final
+    // synchronisation (that call does not wait for the list on its own)
+    unsigned long long* act_host = nullptr;
     uint64_t sino_gen = 0;  // counts sinogram uploads (a batch rebuilds its items on change)
     unsigned int* counter = nullptr;  // work counter of the dynamically scheduled kernels
 

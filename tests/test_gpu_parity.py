@@ -485,6 +485,15 @@ def test_rows_without_counts_are_skipped(golden, visit, bps):
         for b in range(B):
             want, _ = ob.mlem(m, sinos[b], 1, start_image=x0[b])
             assert ob.rel_l2(x[b], want) <= TOL_MLEM, b
+        # a step with another sinogram reports that sinogram's rows with counts
+        half = sinos.copy()
+        half[:, ::2] = 0
+        x = x0.copy()
+        ctx.step_host(half, x)
+        ctx._refresh()
+        live = (half != 0).any(axis=0)
+        assert ctx.info.rows_with_counts == int(live.sum())
+        assert ctx.info.nnz_with_counts == int(lens[live].sum())
         zero = np.zeros_like(sinos)  # no row left: the walk visits nothing
         ctx.set_sinograms(zero)
         ctx._refresh()
