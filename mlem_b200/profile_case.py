@@ -20,7 +20,8 @@ def main(argv=None):
     ap.add_argument("--rows", type=int, default=1 << 20)
     ap.add_argument("--count", type=int, nargs=2, default=[150, 250])
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--mode", choices=["csc", "atomic", "fused", "region", "exact"], default="csc")
+    ap.add_argument("--mode", choices=["csc", "atomic", "fused", "region", "exact", "matrix-free"],
+                    default="csc")
     ap.add_argument("--group", type=int, default=32)
     ap.add_argument("--frame-tile", type=int, default=1)
     ap.add_argument("--blocks-per-sm", type=int, default=8)
@@ -33,6 +34,8 @@ def main(argv=None):
     a = ap.parse_args(argv)
     nx, ny, nz = a.grid
     g = synth.Geometry(nx, ny, nz, a.rows, a.count[0], a.count[1], seed=a.seed)
+    if a.mode == "matrix-free":
+        return matrix_free(a, g)
     flags = api.FLAG_EXACT if a.mode == "exact" else 0
     if a.natural:
         flags |= api.FLAG_NATURAL_LAYOUT
@@ -56,6 +59,27 @@ def main(argv=None):
                           "phase_ms": [round(float(x), 4) for x in ms],
                           "phase_GBps": [round(float(b / (t / 1e3) / 1e9), 1) if t > 0 else 0
                                          for b, t in zip(by, ms)]}))
+
+
+
+
+def matrix_free(a, g):
+    """The matrix-free pass (mlem_mf_*) on the same geometry and frames: the
+    sinogram comes from a stored context's double projection, which is then
+    freed; one frame."""
+    import time
+
+    with api.Context.siddon(g, flags=api.FLAG_NO_CSC) as ctx:
+        w = synth.Workload("profile", g, 1, a.iters, 0, (3, 12), (1e6, 1e9), 9000)
+        fr = synth.make_frames(w, ctx.project_f64)
+    with api.MatrixFree(g) as mf:
+        mf.set_sinogram(fr.sinograms[0])
+        mf.init_image()
+        t0 = time.time()
+        mf.iterate(a.iters)
+        mf.get_image()
+        print(json.dumps({"mode": "matrix-free", "rays": g.n_rows, "iters": a.iters,
+                          "wall_s": round(time.time() - t0, 3), **mf.info()}))
 
 
 if __name__ == "__main__":
