@@ -716,7 +716,9 @@ def matrix_free_line(a, sino, stream, barrier, ms_stored, fast_img):
             ms = e0.elapsed_time(e1) / k
             info = mf.info()
             entry = {"ms_per_iteration": round(ms, 4), "device_bytes": info["device_bytes"],
-                     "rays": g.n_rows}
+                     "rays": g.n_rows,
+                     "sinogram": "plain-full" if name == "plain-full"
+                                 else "50 counts on every ray (every ray walked)"}
             if name == "plain-full":
                 entry["stored_ms_per_iteration"] = round(ms_stored, 4)
                 mf.init_image()
@@ -889,7 +891,8 @@ def run_shards(a, rank, world, local_rank):
     if rank != 0:
         full.close()
         full = None
-    shard = distributed.CudaShard(blk, g.n_cols, frames.sinograms[0][blk.start:blk.end], local_rank)
+    shard = distributed.CudaShard(blk, g.n_cols, frames.sinograms[0][blk.start:blk.end], local_rank,
+                                  grid=(g.nx, g.ny, g.nz))
     setup_s = time.time() - t0
     x = distributed.init_image(shard, dist)
     distributed.iterate(shard, x, a.warmup, dist)

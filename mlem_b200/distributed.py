@@ -124,10 +124,11 @@ class CudaShard:
     the context is built without one (MLEM_FLAG_NO_CSC: half the device
     memory, and the block's column sums by atomics).  With one_pass=False
     the shard offers only the two passes (project_correl, then backproject
-    over the CSC)."""
+    over the CSC).  The one-pass update takes the caller's sinogram block, so
+    it walks every row of the block, those without counts included."""
 
     def __init__(self, block: RowBlock, n_cols: int, sino_block: np.ndarray, device: int,
-                 flags: int = 0, one_pass: bool = True):
+                 flags: int = 0, one_pass: bool = True, grid=None):
         import torch
 
         self.torch = torch
@@ -138,7 +139,9 @@ class CudaShard:
             flags |= api.FLAG_NO_CSC
         else:
             self.partial_update = None  # iterate() then takes the two passes
-        self.ctx = api.Context(block.row_end, block.elems, self.n_rows, n_cols, flags, device)
+        # grid (nx, ny, nz): the device keeps the image in Morton order, as a
+        # whole-matrix context of that geometry does
+        self.ctx = api.Context(block.row_end, block.elems, self.n_rows, n_cols, flags, device, grid)
         self.stream = torch.cuda.current_stream(self.device)
         self.ctx.set_stream(self.stream.cuda_stream)
         s = np.ascontiguousarray(sino_block, np.int32)
