@@ -919,7 +919,7 @@ def run_shards(a, rank, world, local_rank):
     f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     f0.record(stream)
     for _ in range(k_e2e):
-        shard.sino.copy_(sino_h, non_blocking=True)
+        shard.set_sinogram(sino_h.numpy())
         distributed.iterate(shard, x, 1, dist)
         img_h.copy_(x, non_blocking=True)
     f1.record(stream)
@@ -950,7 +950,8 @@ def run_shards(a, rank, world, local_rank):
                  "e2e": {"value": round(1e3 / e2e_ms, 3), "unit": UNIT,
                          "h2d_bytes_per_step": int(4 * (blk.end - blk.start)),
                          "d2h_bytes_per_step": int(4 * g.n_cols),
-                         "call": "distributed.iterate (pinned sinogram block in, image out)"},
+                         "call": "CudaShard.set_sinogram + distributed.iterate "
+                                 "(pinned sinogram block in, image out)"},
                  # per iteration and rank: the one-pass kernel and the update apply
                  "gpu_launches": int(2 * a.steps * world),
                  "clocks": clk},

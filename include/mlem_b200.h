@@ -294,9 +294,12 @@ int mlem_fwproj_correl_d(mlem_ctx* ctx, const float* x, const int32_t* sino, flo
  * matrix (the one-pass kernels, with the context's row visit when it is tuned
  * to MLEM_BK_FUSED, else sorted rows in chunks): the partial update of a row
  * shard (mlem_mpi/fusedmpimlem.cpp:205-225) or the numerator of calcUpdate.
- * Summation order varies from run to run (float atomics).  Not in the
- * bit-exact mode; must not run concurrently with the context's own
- * iterations. */
+ * sino NULL: the context's own sinograms (mlem_set_sinograms with n_frames
+ * frames, a power of two up to 16 so that none is padded); the sorted visits
+ * then leave out the rows whose counts are zero in every frame, as an
+ * iteration does.  Summation order varies from run to run (float atomics).
+ * Not in the bit-exact mode; must not run concurrently with the context's
+ * own iterations. */
 int mlem_fused_update_d(mlem_ctx* ctx, const float* x, const int32_t* sino, float* update,
                         uint32_t n_frames, void* stream);
 /* x[C][B] *= calcUpdate factor(A^T correl[R][B], norm)  (fused, CSC). */

@@ -561,12 +561,33 @@ int build_active_list(mlem_ctx* c, bool read_back) {
     return MLEM_OK;
 }
 
+// The subsets' sorted lists without their rows without counts (ordered
+// subsets walk them with the sorted visits); needs the main list's buffers.
+int build_subset_lists(mlem_ctx* c) {
+    c->sub_act_ready = false;
+    if (c->n_subsets < 2 || !c->sub_sorted || !c->sub_act_order || !c->act_ready || !c->act_tmp)
+        return MLEM_OK;
+    for (uint32_t k = 0; k < c->n_subsets; ++k) {
+        SparseView v = csr_view(c);
+        const uint64_t o = c->sub_off[k];
+        v.order = c->sub_sorted + o;
+        v.vrange = c->sub_sorted_ranges + o;
+        v.n = (uint32_t)(c->sub_off[k + 1] - o);
+        CK(c, active_rows_build(v, c->sino, c->Bp, c->act_flags, c->act_tmp, c->act_tmp_bytes,
+                                c->sub_act_order + o, c->sub_act_ranges + o, c->sub_act_n + k,
+                                c->sub_act_z + k, c->stream));
+    }
+    c->sub_act_ready = true;
+    return MLEM_OK;
+}
+
 // A captured iteration holds the list or the full visiting order: capture
 // again when that changes (not when the list is only rebuilt in place).
 int build_active(mlem_ctx* c, bool read_back) {
-    const bool was = c->act_ready;
-    const int s = build_active_list(c, read_back);
-    if (c->act_ready != was) c->graph_dirty = true;
+    const bool was = c->act_ready, sub_was = c->sub_act_ready;
+    int s = build_active_list(c, read_back);
+    if (s == MLEM_OK) s = build_subset_lists(c);
+    if (c->act_ready != was || c->sub_act_ready != sub_was) c->graph_dirty = true;
     return s;
 }
 
@@ -699,9 +720,16 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                 break;
             case MLEM_BK_FUSED:
                 if (c->n_subsets > 1) {
-                    // ordered subsets: a one-pass sub-iteration and its update per subset
+                    // ordered subsets: a one-pass sub-iteration and its update per
+                    // subset; the sorted visits walk each subset's rows with counts
                     for (uint32_t s = 0; s < c->n_subsets; ++s) {
-                        TRY(fused_pass(c, t, subset_view(c, t, s), st));
+                        SparseView v = subset_view(c, t, s);
+                        if (c->sub_act_ready && t.visit != MLEM_VISIT_FILE) {
+                            v.order = c->sub_act_order + c->sub_off[s];
+                            v.vrange = c->sub_act_ranges + c->sub_off[s];
+                            v.n_dev = c->sub_act_n + s;
+                        }
+                        TRY(fused_pass(c, t, v, st));
                         CK(c, apply_update_subset(c->x, c->update, c->sub_norm + (size_t)s * c->C,
                                                   c->norm, c->C, Bp, st));
                     }
@@ -1797,10 +1825,13 @@ namespace {
 
 void free_subsets(mlem_ctx* c) {
     for (void** p : {(void**)&c->sub_norm, (void**)&c->sub_file, (void**)&c->sub_file_ranges,
-                     (void**)&c->sub_sorted, (void**)&c->sub_sorted_ranges}) {
+                     (void**)&c->sub_sorted, (void**)&c->sub_sorted_ranges,
+                     (void**)&c->sub_act_order, (void**)&c->sub_act_ranges, (void**)&c->sub_act_n,
+                     (void**)&c->sub_act_z}) {
         dev_free(*p);
         *p = nullptr;
     }
+    c->sub_act_ready = false;
     c->sub_off.clear();
     c->n_subsets = 1;
     c->device_bytes -= c->sub_bytes;
@@ -1872,9 +1903,20 @@ int mlem_set_subsets(mlem_ctx* c, uint32_t n) {
         for (uint32_t r : order) list[next[r % n]++] = r;  // stable partition by subset
         s = upload_list(c, list, &c->sub_sorted, &c->sub_sorted_ranges);
         if (s != MLEM_OK) return bail(s);
+        // room for the lists without the rows without counts
+        if ((s = dev_alloc(c, &c->sub_act_order, c->R)) != MLEM_OK ||
+            (s = dev_alloc(c, &c->sub_act_ranges, c->R)) != MLEM_OK ||
+            (s = dev_alloc(c, &c->sub_act_n, n)) != MLEM_OK ||
+            (s = dev_alloc(c, &c->sub_act_z, n)) != MLEM_OK)
+            return bail(s);
     }
     c->n_subsets = n;
     c->sub_bytes = c->device_bytes - before;
+    if (c->B && c->sino) {  // sinograms already set: their lists now
+        s = build_subset_lists(c);
+        if (s == MLEM_OK) CK(c, cudaStreamSynchronize(c->stream));
+        if (s != MLEM_OK) return bail(s);
+    }
     return MLEM_OK;
 }
 
@@ -1976,9 +2018,19 @@ int mlem_fwproj_correl_d(mlem_ctx* c, const float* x, const int32_t* sino, float
 
 int mlem_fused_update_d(mlem_ctx* c, const float* x, const int32_t* sino, float* u, uint32_t B,
                         void* stream) {
-    if (!c || !x || !sino || !u || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
+    if (!c || !x || !u || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
     if (c->flags & MLEM_FLAG_EXACT)
         return fail(c, MLEM_ERR_STATE, "the one-pass method does not run in the bit-exact mode");
+    // sino NULL: the context's own sinograms, whose list of rows with counts
+    // the sorted visits walk (frames interleaved as the caller's vectors)
+    const bool own = sino == nullptr;
+    if (own) {
+        if (!c->sino || c->B != B || c->Bp != B)
+            return fail(c, MLEM_ERR_STATE,
+                        "sino NULL needs the context's own sinograms with %u frames (it has %u, "
+                        "padded to %u)", B, c->B, c->Bp);
+        sino = c->sino;
+    }
     TRY(set_device(c));
     cudaStream_t st = (cudaStream_t)stream;
     if (c->mirrored) {  // the full rows' sums in a buffer of the context, then the scatter
@@ -2038,6 +2090,11 @@ int mlem_fused_update_d(mlem_ctx* c, const float* x, const int32_t* sino, float*
     CK(c, cudaMemsetAsync(ud, 0, (size_t)c->C * B * 4, st));
     SparseView v = csr_visit(c, t);
     if (c->n_long) v.long_len = kLongRowElems;
+    if (own && c->act_ready && t.visit != MLEM_VISIT_FILE) {
+        v.order = c->act_order;
+        v.vrange = c->act_ranges;
+        v.n_dev = c->act_n;
+    }
     // a counter of its own (a cache sector from the iteration's), so that this
     // call and the context's graph never share one
     TRY(fused_pass(c, t, v, xd, sino, ud, B, c->counter + 8, st));

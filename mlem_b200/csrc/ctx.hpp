@@ -94,6 +94,14 @@ struct mlem_ctx {
     ulonglong2* sub_sorted_ranges = nullptr;
     std::vector<uint64_t> sub_off;
     size_t sub_bytes = 0;  // device bytes of the subset buffers
+    // every subset's sorted list without its rows whose counts are zero in
+    // every frame (built like act_order whenever the sinograms or the subsets
+    // change; subset s at sub_off[s], its length in sub_act_n[s])
+    uint32_t* sub_act_order = nullptr;
+    ulonglong2* sub_act_ranges = nullptr;
+    uint32_t* sub_act_n = nullptr;
+    unsigned long long* sub_act_z = nullptr;
+    bool sub_act_ready = false;
 
     // frames
     uint32_t B = 0, Bp = 0;

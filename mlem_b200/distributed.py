@@ -149,6 +149,10 @@ class CudaShard:
             raise api.MlemError(api.MLEM_ERR_INVALID, "sinogram block size differs from the rows")
         self.sino = torch.from_numpy(s).to(self.device)
         self._sumin = float(np.sum(s, dtype=np.float64))
+        if one_pass and self.n_rows:
+            # the block's counts also in the context, whose one-pass update then
+            # leaves out the rows without counts
+            self.ctx.set_sinograms(s)
         self.correl = torch.zeros(max(self.n_rows, 1), dtype=torch.float32, device=self.device)
         self.update = torch.zeros(n_cols, dtype=torch.float32, device=self.device)
 
@@ -174,11 +178,22 @@ class CudaShard:
             self.update.zero_()
         return self.update
 
+    def set_sinogram(self, sino_block) -> None:
+        """New counts for the block (host array, pinned or not)."""
+        s = np.ascontiguousarray(sino_block, np.int32)
+        if s.size != self.n_rows:
+            raise api.MlemError(api.MLEM_ERR_INVALID, "sinogram block size differs from the rows")
+        self.sino.copy_(self.torch.from_numpy(s), non_blocking=True)
+        self._sumin = float(np.sum(s, dtype=np.float64))
+        if getattr(self, "partial_update", None) is not None and self.n_rows:
+            self.ctx.set_sinograms(s)
+
     def partial_update(self, x):
         """The block's partial update A_b^T calcCorrel(s_b, A_b x) in one pass
-        over its rows (the one-pass kernels)."""
+        over its rows (the one-pass kernels), from the block's counts held by
+        the context (its rows without counts are left out)."""
         if self.n_rows:
-            self.ctx.fused_update_d(x.data_ptr(), self.sino.data_ptr(), self.update.data_ptr(), 1,
+            self.ctx.fused_update_d(x.data_ptr(), 0, self.update.data_ptr(), 1,
                                     self.stream.cuda_stream)
         else:
             self.update.zero_()

@@ -87,3 +87,33 @@ def test_nccl_driver_single_rank(golden):
         if shard is not None:
             shard.close()
         dist.destroy_process_group()
+
+
+def test_fused_update_from_the_context_sinogram(golden):
+    """mlem_fused_update_d with sino NULL takes the context's own counts and
+    leaves out the rows without counts: equal to the update from the same
+    counts passed explicitly (every row walked) up to the order of the
+    float atomics."""
+    torch = pytest.importorskip("torch")
+    from mlem_b200 import api
+
+    m, sino, iters, gold, _ = golden.case("plain_small_it10")
+    rng = np.random.default_rng(4)
+    s = np.ascontiguousarray(sino, np.int32).copy()
+    s[rng.random(m.n_rows) < 0.4] = 0
+    dev = torch.device("cuda", 0)
+    with api.Context.from_matrix(m, flags=api.FLAG_NO_CSC) as ctx:
+        ctx.set_sinograms(s)
+        x = torch.from_numpy(rng.uniform(0.5, 2.0, m.n_cols).astype(np.float32)).to(dev)
+        sd = torch.from_numpy(s).to(dev)
+        u_own = torch.zeros(m.n_cols, dtype=torch.float32, device=dev)
+        u_arg = torch.zeros_like(u_own)
+        st = torch.cuda.current_stream().cuda_stream
+        ctx.fused_update_d(x.data_ptr(), 0, u_own.data_ptr(), 1, st)
+        ctx.fused_update_d(x.data_ptr(), sd.data_ptr(), u_arg.data_ptr(), 1, st)
+        torch.cuda.synchronize()
+        assert ob.rel_l2(u_own.cpu().numpy(), u_arg.cpu().numpy()) <= 1e-6
+        want = ob.bkproj(m, ob.correl(ob.fwproj(m, x.cpu().numpy()), s))
+        assert ob.rel_l2(u_own.cpu().numpy(), want) <= 1e-5
+        with pytest.raises(api.MlemError):  # the context holds one frame
+            ctx.fused_update_d(x.data_ptr(), 0, u_own.data_ptr(), 2, st)

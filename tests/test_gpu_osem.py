@@ -148,3 +148,35 @@ def test_osem_autotune_and_rejections(ctxs, golden):
             ex.set_subsets(2)
     # switching to another method with one subset is allowed again
     ctx.set_tuning(bk_mode=api.BK_CSC, group=32, frame_tile=1)
+
+
+@pytest.mark.parametrize("visit", [api.VISIT_SORTED, api.VISIT_SORTED_CHUNKED, api.VISIT_SORTED_STAGED])
+def test_osem_skips_rows_without_counts(golden, visit):
+    """The sorted walks of every subset leave out its rows whose counts are
+    zero; the lists follow new sinograms in place (graph kept), are built
+    when subsets are set after the sinograms, and through mlem_step_host."""
+    m, sino, iters, gold, _ = golden.case("plain_small_it10")
+    rng = np.random.default_rng(21)
+    s = np.ascontiguousarray(sino, np.int32).copy()
+    dead = rng.random(m.n_rows) < 0.5
+    s[dead] = 0
+    S = 4
+    with api.Context.from_matrix(m) as ctx:
+        ctx.set_sinograms(s)
+        ctx.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=1, blocks_per_sm=4, visit=visit)
+        ctx.set_subsets(S)  # after the sinograms
+        for it in range(2):
+            ctx.init_images()
+            ctx.iterate(3)
+            want, _ = ob.osem(m, s, 3, S)
+            assert ob.rel_l2(ctx.get_images()[0], want) <= TOL, it
+            s = s.copy()  # other rows with counts: the lists are rebuilt in place
+            s[~dead] = 0
+            s[dead] = rng.poisson(30, int(dead.sum()))
+            ctx.set_sinograms(s)
+        x0 = np.full((1, m.n_cols), 0.5, np.float32)
+        x = x0.copy()
+        ctx.step_host(s, x)
+        want, _ = ob.osem(m, s, 1, S, start_image=x0[0])
+        assert ob.rel_l2(x[0], want) <= TOL
+        ctx.set_subsets(1)
