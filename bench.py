@@ -519,11 +519,10 @@ def run_ours(a, rank, world, local_rank, parallelism):
             detail["batched_phases_ms"] = [round(float(x), 4) for x in bph_ms]
 
         # --- full-size parity, GPU side (the host jobs run meanwhile) ---
+        pf = None
         if jobs is not None and jobs.error is None:
             pf = parity_gpu_side(ctx, a, tuning, frames.sinograms, fb, tb if fb is not None else None,
                                  kf, d, mpath, spaths["plain"])
-        else:
-            pf = None
 
         # --- ordered subsets: 8 interleaved row subsets, the plain sinogram ---
         if not a.no_osem:
@@ -651,6 +650,10 @@ def parity_finish(jobs, pf, n):
     """Relative L2 errors of the 60-iteration images: ours against the
     reference's seqcsr4mlem, and ours and the reference's against the FP64
     oracle of the same iterations."""
+    if jobs.error:
+        return {"iterations": n, "error": jobs.error}
+    if pf is None or "fast" not in pf:
+        return {"iterations": n, "error": "no GPU images (the GPU side did not run)"}
     try:
         ref, wait_s = jobs.collect()
     except Exception as e:
