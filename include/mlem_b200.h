@@ -310,6 +310,23 @@ int mlem_bkproj_update_d(mlem_ctx* ctx, const float* correl, float* x, uint32_t 
  * been summed (the single exchange of mlem_mpi/fusedmpimlem.cpp:227). */
 int mlem_apply_update_d(mlem_ctx* ctx, const float* update, float* x, uint32_t n_frames,
                         void* stream);
+/* The two one-pass kernels of the unrolled MLEM's backward pass (one frame,
+ * device pointers, natural voxel order; no counterpart in the reference):
+ *   mlem_ratio_rows_d:    update = A^T calcCorrel(sino, A x) as
+ *                         mlem_fused_update_d, and rows[R] = A x for the
+ *                         rows with a nonzero count (0 for the others);
+ *   mlem_adjoint_update_d: update = A^T df with
+ *                         df_r = -(A du)_r * (sino_r / rows_r) / rows_r where
+ *                         sino_r and rows_r are nonzero, else 0 -- the
+ *                         adjoint of calcCorrel and both projections.
+ * Each is one pass over the matrix; rows without counts are skipped before
+ * their elements are read.  Summation order varies from run to run.  Not in
+ * the bit-exact mode nor with MLEM_FLAG_MIRROR_KERNELS; must not run
+ * concurrently with the context's own iterations or mlem_fused_update_d. */
+int mlem_ratio_rows_d(mlem_ctx* ctx, const float* x, const int32_t* sino, float* rows,
+                      float* update, void* stream);
+int mlem_adjoint_update_d(mlem_ctx* ctx, const float* du, const int32_t* sino, const float* rows,
+                          float* update, void* stream);
 /* Device pointer of the context's column sums (float[C]). */
 int mlem_norm_d(mlem_ctx* ctx, const float** norm);
 /* Replace the column sums with norm[C] (device pointer): a row shard uses the

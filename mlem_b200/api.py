@@ -368,6 +368,18 @@ class Context:
         self._chk(core_lib().mlem_fused_update_d(self._h, x_ptr, sino_ptr, update_ptr, n_frames,
                                                  stream))
 
+    def ratio_rows_d(self, x_ptr, sino_ptr, rows_ptr, update_ptr, stream=0) -> None:
+        """update = A^T calcCorrel(sino, A x) and rows = A x (0 for rows
+        without a count) in one pass (one frame)."""
+        self._chk(core_lib().mlem_ratio_rows_d(self._h, x_ptr, sino_ptr, rows_ptr, update_ptr,
+                                               stream))
+
+    def adjoint_update_d(self, du_ptr, sino_ptr, rows_ptr, update_ptr, stream=0) -> None:
+        """update = A^T df, df = -(A du) (sino / rows) / rows where both are
+        nonzero, in one pass (one frame)."""
+        self._chk(core_lib().mlem_adjoint_update_d(self._h, du_ptr, sino_ptr, rows_ptr, update_ptr,
+                                                   stream))
+
     def bkproj_update_d(self, correl_ptr, x_ptr, n_frames=1, stream=0) -> None:
         self._chk(core_lib().mlem_bkproj_update_d(self._h, correl_ptr, x_ptr, n_frames, stream))
 

@@ -2105,6 +2105,44 @@ int mlem_fused_update_d(mlem_ctx* c, const float* x, const int32_t* sino, float*
     return MLEM_OK;
 }
 
+// The two one-pass kernels of the unrolled MLEM's backward pass (k_adjoint.cu):
+// vectors in natural voxel order, one frame, row vectors by row.
+static int backward_pass(mlem_ctx* c, int op, const float* x, const int32_t* sino, float* rows,
+                         float* u, void* stream) {
+    if (!c || !x || !sino || !rows || !u) return fail(c, MLEM_ERR_INVALID, "null argument");
+    if (c->flags & MLEM_FLAG_EXACT)
+        return fail(c, MLEM_ERR_STATE, "the one-pass method does not run in the bit-exact mode");
+    if (c->mirrored)
+        return fail(c, MLEM_ERR_STATE,
+                    "the backward-pass kernels walk full rows (not MLEM_FLAG_MIRROR_KERNELS)");
+    TRY(set_device(c));
+    cudaStream_t st = (cudaStream_t)stream;
+    const float* xd = x;
+    float* ud = u;
+    if (c->bricked) {
+        TRY(perm_scratch(c, (size_t)c->C));
+        CK(c, permute_to_device(x, c->pscratch[0], c->perm, c->C, 1, st));
+        xd = c->pscratch[0];
+        ud = c->pscratch[1];
+    }
+    CK(c, cudaMemsetAsync(ud, 0, (size_t)c->C * 4, st));
+    // the counter slot of mlem_fused_update_d: these calls, like it, must not
+    // run concurrently with the context's own iterations
+    CK(c, adjoint_pass(op, csr_view(c), xd, sino, rows, ud, c->counter + 8, c->n_sm, st));
+    if (c->bricked) CK(c, permute_to_natural(ud, u, c->perm, c->C, 1, st));
+    return MLEM_OK;
+}
+
+int mlem_ratio_rows_d(mlem_ctx* c, const float* x, const int32_t* sino, float* rows, float* update,
+                      void* stream) {
+    return backward_pass(c, kOpRatio, x, sino, rows, update, stream);
+}
+
+int mlem_adjoint_update_d(mlem_ctx* c, const float* du, const int32_t* sino, const float* rows,
+                          float* update, void* stream) {
+    return backward_pass(c, kOpAdjoint, du, sino, const_cast<float*>(rows), update, stream);
+}
+
 int mlem_bkproj_update_d(mlem_ctx* c, const float* correl, float* x, uint32_t B, void* stream) {
     if (!c || !x || !correl || B == 0) return fail(c, MLEM_ERR_INVALID, "bad argument");
     if (!c->has_csc || c->mirrored)

@@ -390,6 +390,16 @@ cudaError_t batch_staged(const BatchTable& t, const BatchItem* items, uint32_t n
 // the grid as a whole moves through one window of the order.
 // ctas_per_sm: 1, 2 or 4 resident CTAs of 1024, 512 or 256 threads (the
 // CTAs of one SM share its L1, a bigger CTA puts more neighbouring rows on it).
+// ---- backward-pass one-pass kernels (k_adjoint.cu), one frame ----------------
+// kOpRatio  : u += A^T calcCorrel(s, A x); rows[r] = (A x)_r (0 for a row
+//             without a count, which is skipped)
+// kOpAdjoint: u += A^T df, df_r = -(A x)_r (s_r / rows_r) / rows_r where s_r
+//             and rows_r are nonzero, else 0 (x is the adjoint image here)
+constexpr int kOpRatio = 0, kOpAdjoint = 1;
+cudaError_t adjoint_pass(int op, const SparseView& csr, const float* x, const int32_t* sino,
+                         float* rows, float* u, unsigned int* counter, int sm_count,
+                         cudaStream_t st);
+
 cudaError_t fused_chunked(const SparseView& csr, const float* x, uint32_t B, int frame_tile,
                           const int32_t* sino, float* u, uint32_t chunk_rows, int ctas_per_sm,
                           unsigned int* counter, int sm_count, cudaStream_t st);

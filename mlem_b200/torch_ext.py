@@ -9,8 +9,9 @@
   (omega_k = 1 is the reference iteration, mlem_seq/seqcsr4mlem.cpp:163-167)
   with gradients with respect to x0 and omega.  The backward pass keeps
   only the K images x_k (per-iteration checkpoints) and recomputes A x_k and
-  A^T(s / A x_k) from them, then propagates the adjoint with one forward and
-  one back projection per iteration.
+  A^T(s / A x_k) from them in one pass over the matrix, then propagates the
+  adjoint through calcCorrel and both projections in a second pass: two
+  passes per iteration (forward: one).
 
 Zero rules follow the reference: the correlation is 0 where the projection
 is 0 (calcCorrel), the update factor is the raw back projection where the
@@ -95,12 +96,24 @@ def norm_tensor(ctx: "api.Context", device) -> torch.Tensor:
     return torch.from_numpy(ctx.column_sums()).to(device)
 
 
-def _fused_ratio(ctx, x, sino_i, norm):
-    """calcUpdate factor of A^T (s / A x) from the one-pass kernels (one pass
-    over the matrix instead of a forward and a back projection)."""
+def _ratio_rows(ctx, x, sino_i, norm):
+    """calcUpdate factor of A^T (s / A x) and the row sums f = A x (0 for the
+    rows without a count), in one pass over the matrix (mlem_ratio_rows_d)."""
     u = torch.empty_like(x)
-    ctx.fused_update_d(x.data_ptr(), sino_i.data_ptr(), u.data_ptr(), 1, _stream())
-    return torch.where(norm != 0, u / torch.where(norm != 0, norm, torch.ones_like(norm)), u)
+    f = torch.empty(ctx.n_rows, dtype=torch.float32, device=x.device)
+    ctx.ratio_rows_d(x.data_ptr(), sino_i.data_ptr(), f.data_ptr(), u.data_ptr(), _stream())
+    r = torch.where(norm != 0, u / torch.where(norm != 0, norm, torch.ones_like(norm)), u)
+    return r, f
+
+
+def _adjoint(ctx, du, sino_i, f):
+    """A^T df with df = -(A du) s / f^2 where the row has a count and f != 0:
+    the adjoint of calcCorrel and both projections, in one pass
+    (mlem_adjoint_update_d)."""
+    out = torch.empty_like(du)
+    ctx.adjoint_update_d(du.contiguous().data_ptr(), sino_i.data_ptr(), f.data_ptr(),
+                         out.data_ptr(), _stream())
+    return out
 
 
 class _UnrolledMLEM(torch.autograd.Function):
@@ -110,7 +123,7 @@ class _UnrolledMLEM(torch.autograd.Function):
         xs = [x0.detach()]
         x = x0.detach().contiguous()
         for k in range(K):
-            r = _fused_ratio(ctx, x, sino_i, norm)
+            r, _ = _ratio_rows(ctx, x, sino_i, norm)
             x = x * torch.where(r > 0, r.clamp_min(1e-38) ** omega[k], torch.zeros_like(r))
             xs.append(x)
         fctx.mctx = ctx
@@ -127,8 +140,7 @@ class _UnrolledMLEM(torch.autograd.Function):
         d_omega = torch.zeros_like(omega)
         for k in range(K - 1, -1, -1):
             xk = xs[k].contiguous()
-            f = _fw(ctx, xk)                                    # recompute from the checkpoint
-            r = _fused_ratio(ctx, xk, fctx.sino_i, norm)
+            r, f = _ratio_rows(ctx, xk, fctx.sino_i, norm)      # recomputed from the checkpoint
             pos = r > 0
             rs = torch.where(pos, r, torch.ones_like(r))
             p = torch.where(pos, rs ** omega[k], torch.zeros_like(r))  # r^w
@@ -137,14 +149,10 @@ class _UnrolledMLEM(torch.autograd.Function):
             gx = g * p                                          # direct path
             dr = torch.where(pos, g * xk * omega[k] * rs ** (omega[k] - 1), torch.zeros_like(r))
             du = torch.where(norm != 0, dr / torch.where(norm != 0, norm, torch.ones_like(norm)), dr)
-            dc = _fw(ctx, du)                                   # adjoint of A^T
-            # c = s / f where f != 0: dc/df = -s / f^2.  A row with zero counts
-            # has c = 0 whatever f is (no gradient), and f^2 is never formed:
-            # for a tiny nonzero f it underflows to 0 (0 / 0 in a zero-count row)
-            live = (f != 0) & (sino_f != 0)
-            fs = torch.where(live, f, torch.ones_like(f))
-            df = torch.where(live, -(dc * (sino_f / fs)) / fs, torch.zeros_like(f))
-            gx = gx + _bk(ctx, df)                              # adjoint of A
+            # adjoint of A^T, of calcCorrel (c = s / f where f != 0: dc/df = -s / f^2,
+            # formed as -(dc (s / f)) / f so that a tiny f never squares to 0; a row
+            # with zero counts has c = 0 whatever f is: no gradient) and of A
+            gx = gx + _adjoint(ctx, du, fctx.sino_i, f)
             g = gx
         return g, d_omega, None, None, None, None
 

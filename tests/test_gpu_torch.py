@@ -117,3 +117,37 @@ def test_unrolled_mlem_gradients_finite_with_tiny_projections(small):
     assert torch.isfinite(xK).all()
     assert torch.isfinite(xt.grad).all() and torch.isfinite(wt.grad).all()
     assert float(wt.grad.abs().sum()) > 0
+
+
+@pytest.mark.parametrize("flags", [0, api.FLAG_NATURAL_LAYOUT | api.FLAG_NO_ROW_ORDER])
+def test_backward_pass_kernels_against_the_oracle(golden, flags):
+    """mlem_ratio_rows_d and mlem_adjoint_update_d (the backward pass's two
+    one-pass kernels) against the oracle's projections, in the Morton layout
+    with sorted rows and in natural order with file-order rows."""
+    m, sino, iters, gold, _ = golden.case("plain_small_it10")
+    rng = np.random.default_rng(8)
+    s = np.ascontiguousarray(sino, np.int32).copy()
+    s[rng.random(m.n_rows) < 0.3] = 0
+    x = rng.uniform(0.5, 2.0, m.n_cols).astype(np.float32)
+    du = rng.normal(0.0, 1.0, m.n_cols).astype(np.float32)
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.current_stream().cuda_stream
+    with api.Context.from_matrix(m, flags=flags) as ctx:
+        xs, dus, sd = (torch.from_numpy(a).to(dev) for a in (x, du, s))
+        rows = torch.empty(m.n_rows, dtype=torch.float32, device=dev)
+        u = torch.empty(m.n_cols, dtype=torch.float32, device=dev)
+        ctx.ratio_rows_d(xs.data_ptr(), sd.data_ptr(), rows.data_ptr(), u.data_ptr(), st)
+        a = torch.empty_like(u)
+        ctx.adjoint_update_d(dus.data_ptr(), sd.data_ptr(), rows.data_ptr(), a.data_ptr(), st)
+        torch.cuda.synchronize()
+        f_got, u_got, a_got = rows.cpu().numpy(), u.cpu().numpy(), a.cpu().numpy()
+    f = ob.fwproj(m, x)
+    live = s != 0
+    assert ob.rel_l2(f_got[live], f[live]) <= 1e-5
+    assert not f_got[~live].any()
+    assert ob.rel_l2(u_got, ob.bkproj(m, ob.correl(f, s))) <= 1e-5
+    f64 = f.astype(np.float64)
+    dc = ob.fwproj(m, du).astype(np.float64)
+    ok = live & (f64 != 0)
+    df = np.where(ok, -(dc * (s / np.where(ok, f64, 1.0))) / np.where(ok, f64, 1.0), 0.0)
+    assert ob.rel_l2(a_got, ob.bkproj(m, df.astype(np.float32))) <= 1e-5
