@@ -49,22 +49,39 @@ __global__ void __launch_bounds__(256) k_fwproj(SparseView csr, const float* __r
                                                 float* __restrict__ c, float* __restrict__ y) {
     MLEM_WARP_LOOP_SETUP
     const uint2* el = reinterpret_cast<const uint2*>(csr.pairs);
+    // Only the correlation wanted: a row whose counts are zero in the tile's
+    // frames has calcCorrel 0 whatever its projection, so its elements are
+    // not read (the counts are loaded beside the row range).
+    const bool skip_empty = c != nullptr && y == nullptr;
     for (uint64_t base = warp * RPW; base < csr.n; base += nwarps * RPW) {
         const uint64_t v = base + lw / G;
         const bool active = v < csr.n;
         const uint64_t r = active ? row_at(csr, v) : 0;
         uint64_t b = 0, e = 0;
-        if (active) { b = csr.ptr[r]; e = csr.ptr[r + 1]; }
+        int32_t s[VW];
+#pragma unroll
+        for (int i = 0; i < VW; ++i) s[i] = 0;
+        if (active) {
+            b = csr.ptr[r];
+            e = csr.ptr[r + 1];
+            if (c) ld_counts<VW>(sino + r * B + f0 + sub * VW, s);
+        }
+        if (skip_empty) {
+            bool any = false;
+#pragma unroll
+            for (int i = 0; i < VW; ++i) any |= s[i] != 0;
+            // the group's frames are split over its FL lanes: all of them decide
+#pragma unroll
+            for (int o = 1; o < FL; o <<= 1) any |= __shfl_xor_sync(MLEM_FULL_MASK, any, o) != 0;
+            if (!any) e = b;  // an empty walk: the sum is 0, calcCorrel 0
+        }
         float acc[VW];
         row_dot<G, BT, false>(el, b, e, lane, x, B, f0 + sub * VW, acc, ps, ph);
         slot_allreduce<G, BT>(acc);
         if (active && lane < FL) {
-            const uint64_t idx = r * B + f0 + sub * VW;
             const uint64_t oidx = (csr.out_by_visit ? v : r) * B + f0 + sub * VW;
             if (y) st_vec<VW>(y + oidx, acc);
             if (c) {
-                int32_t s[VW];
-                ld_counts<VW>(sino + idx, s);
                 float o[VW];
 #pragma unroll
                 for (int i = 0; i < VW; ++i) o[i] = correl_of(s[i], acc[i]);
