@@ -151,3 +151,43 @@ def test_backward_pass_kernels_against_the_oracle(golden, flags):
     ok = live & (f64 != 0)
     df = np.where(ok, -(dc * (s / np.where(ok, f64, 1.0))) / np.where(ok, f64, 1.0), 0.0)
     assert ob.rel_l2(a_got, ob.bkproj(m, df.astype(np.float32))) <= 1e-5
+
+
+def test_backward_pass_kernels_on_an_odd_matrix():
+    """Empty rows, a row far longer than one load batch, duplicate columns,
+    zero values and odd sizes through both backward-pass kernels."""
+    from mlem_b200 import formats
+    rng = np.random.default_rng(17)
+    R, C = 777, 333
+    lens = rng.integers(0, 40, R)
+    lens[::9] = 0
+    lens[5] = 10000
+    row_end = np.cumsum(lens).astype(np.uint64)
+    el = np.zeros(int(row_end[-1]), formats.ELEM_DTYPE)
+    el["index"] = rng.integers(0, C, el.size)
+    el["value"] = rng.uniform(0.0, 1.7, el.size).astype(np.float32)
+    el["value"][::13] = 0.0
+    m = formats.Csr4(R, C, row_end, el)
+    s = rng.poisson(3.0, R).astype(np.int32)
+    x = rng.uniform(0.5, 2.0, C).astype(np.float32)
+    du = rng.normal(0.0, 1.0, C).astype(np.float32)
+    dev = torch.device("cuda", 0)
+    st = torch.cuda.current_stream().cuda_stream
+    with api.Context.from_matrix(m) as ctx:
+        xs, dus, sd = (torch.from_numpy(a).to(dev) for a in (x, du, s))
+        rows = torch.empty(R, dtype=torch.float32, device=dev)
+        u = torch.empty(C, dtype=torch.float32, device=dev)
+        a = torch.empty(C, dtype=torch.float32, device=dev)
+        ctx.ratio_rows_d(xs.data_ptr(), sd.data_ptr(), rows.data_ptr(), u.data_ptr(), st)
+        ctx.adjoint_update_d(dus.data_ptr(), sd.data_ptr(), rows.data_ptr(), a.data_ptr(), st)
+        torch.cuda.synchronize()
+        f_got, u_got, a_got = rows.cpu().numpy(), u.cpu().numpy(), a.cpu().numpy()
+    f = ob.fwproj(m, x)
+    live = s != 0
+    assert ob.rel_l2(f_got[live], f[live]) <= 1e-5
+    assert ob.rel_l2(u_got, ob.bkproj(m, ob.correl(f, s))) <= 1e-5
+    f64 = f.astype(np.float64)
+    dc = ob.fwproj(m, du).astype(np.float64)
+    ok = live & (f64 != 0)
+    df = np.where(ok, -(dc * (s / np.where(ok, f64, 1.0))) / np.where(ok, f64, 1.0), 0.0)
+    assert ob.rel_l2(a_got, ob.bkproj(m, df.astype(np.float32))) <= 1e-5
