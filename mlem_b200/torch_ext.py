@@ -11,7 +11,8 @@
   only the K images x_k (per-iteration checkpoints) and recomputes A x_k and
   A^T(s / A x_k) from them in one pass over the matrix, then propagates the
   adjoint through calcCorrel and both projections in a second pass: two
-  passes per iteration (forward: one).
+  passes per iteration (forward: one).  A context with
+  MLEM_FLAG_MIRROR_KERNELS runs the same arithmetic as separate projections.
 
 Zero rules follow the reference: the correlation is 0 where the projection
 is 0 (calcCorrel), the update factor is the raw back projection where the
@@ -96,12 +97,24 @@ def norm_tensor(ctx: "api.Context", device) -> torch.Tensor:
     return torch.from_numpy(ctx.column_sums()).to(device)
 
 
+def _mirrored(ctx) -> bool:
+    """A context with MLEM_FLAG_MIRROR_KERNELS applies the mirrors inside its
+    projection kernels; the one-pass backward kernels walk full rows only."""
+    return bool(ctx.info.flags & api.FLAG_MIRROR_KERNELS)
+
+
 def _ratio_rows(ctx, x, sino_i, norm):
     """calcUpdate factor of A^T (s / A x) and the row sums f = A x (0 for the
-    rows without a count), in one pass over the matrix (mlem_ratio_rows_d)."""
+    rows without a count), in one pass over the matrix (mlem_ratio_rows_d).
+    A mirrored context takes the fused update and a separate forward
+    projection instead (f is then A x on every row)."""
     u = torch.empty_like(x)
-    f = torch.empty(ctx.n_rows, dtype=torch.float32, device=x.device)
-    ctx.ratio_rows_d(x.data_ptr(), sino_i.data_ptr(), f.data_ptr(), u.data_ptr(), _stream())
+    if _mirrored(ctx):
+        ctx.fused_update_d(x.data_ptr(), sino_i.data_ptr(), u.data_ptr(), 1, _stream())
+        f = _fw(ctx, x)
+    else:
+        f = torch.empty(ctx.n_rows, dtype=torch.float32, device=x.device)
+        ctx.ratio_rows_d(x.data_ptr(), sino_i.data_ptr(), f.data_ptr(), u.data_ptr(), _stream())
     r = torch.where(norm != 0, u / torch.where(norm != 0, norm, torch.ones_like(norm)), u)
     return r, f
 
@@ -109,10 +122,17 @@ def _ratio_rows(ctx, x, sino_i, norm):
 def _adjoint(ctx, du, sino_i, f):
     """A^T df with df = -(A du) s / f^2 where the row has a count and f != 0:
     the adjoint of calcCorrel and both projections, in one pass
-    (mlem_adjoint_update_d)."""
+    (mlem_adjoint_update_d; a mirrored context: a forward and a back
+    projection with df formed between them)."""
+    du = du.contiguous()
+    if _mirrored(ctx):
+        dc = _fw(ctx, du)
+        live = (sino_i != 0) & (f != 0)
+        fs = torch.where(live, f, torch.ones_like(f))
+        df = torch.where(live, -(dc * (sino_i.to(torch.float32) / fs)) / fs, torch.zeros_like(f))
+        return _bk(ctx, df)
     out = torch.empty_like(du)
-    ctx.adjoint_update_d(du.contiguous().data_ptr(), sino_i.data_ptr(), f.data_ptr(),
-                         out.data_ptr(), _stream())
+    ctx.adjoint_update_d(du.data_ptr(), sino_i.data_ptr(), f.data_ptr(), out.data_ptr(), _stream())
     return out
 
 
