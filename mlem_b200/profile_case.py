@@ -20,7 +20,8 @@ def main(argv=None):
     ap.add_argument("--rows", type=int, default=1 << 20)
     ap.add_argument("--count", type=int, nargs=2, default=[150, 250])
     ap.add_argument("--seed", type=int, default=1)
-    ap.add_argument("--mode", choices=["csc", "atomic", "fused", "region", "exact", "matrix-free"],
+    ap.add_argument("--mode", choices=["csc", "atomic", "fused", "region", "exact", "matrix-free",
+                                       "adjoint"],
                     default="csc")
     ap.add_argument("--group", type=int, default=32)
     ap.add_argument("--frame-tile", type=int, default=1)
@@ -36,6 +37,8 @@ def main(argv=None):
     g = synth.Geometry(nx, ny, nz, a.rows, a.count[0], a.count[1], seed=a.seed)
     if a.mode == "matrix-free":
         return matrix_free(a, g)
+    if a.mode == "adjoint":
+        return adjoint(a, g)
     flags = api.FLAG_EXACT if a.mode == "exact" else 0
     if a.natural:
         flags |= api.FLAG_NATURAL_LAYOUT
@@ -80,6 +83,38 @@ def matrix_free(a, g):
         mf.get_image()
         print(json.dumps({"mode": "matrix-free", "rays": g.n_rows, "iters": a.iters,
                           "wall_s": round(time.time() - t0, 3), **mf.info()}))
+
+
+def adjoint(a, g):
+    """The two one-pass kernels of the unrolled MLEM's backward pass
+    (mlem_ratio_rows_d, then mlem_adjoint_update_d) on the same geometry's
+    first frame, a.iters times each, with CUDA-event times."""
+    import torch
+
+    with api.Context.siddon(g, flags=api.FLAG_NO_CSC) as ctx:
+        w = synth.Workload("profile", g, 1, a.iters, 0, (3, 12), (1e6, 1e9), 9000)
+        fr = synth.make_frames(w, ctx.project_f64)
+        dev = torch.device("cuda", 0)
+        sino = torch.from_numpy(fr.sinograms[0].astype("int32")).to(dev)
+        x = torch.full((ctx.n_cols,), 1.0, device=dev)
+        du = torch.rand(ctx.n_cols, device=dev, generator=torch.Generator(dev).manual_seed(1))
+        rows = torch.empty(ctx.n_rows, device=dev)
+        u = torch.empty(ctx.n_cols, device=dev)
+        out = torch.empty(ctx.n_cols, device=dev)
+        st = torch.cuda.current_stream().cuda_stream
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ms = [0.0, 0.0]
+        for _ in range(a.iters):
+            ev[0].record()
+            ctx.ratio_rows_d(x.data_ptr(), sino.data_ptr(), rows.data_ptr(), u.data_ptr(), st)
+            ev[1].record()
+            ctx.adjoint_update_d(du.data_ptr(), sino.data_ptr(), rows.data_ptr(), out.data_ptr(), st)
+            ev[2].record()
+            torch.cuda.synchronize()
+            ms[0] = ev[0].elapsed_time(ev[1])
+            ms[1] = ev[1].elapsed_time(ev[2])
+        print(json.dumps({"mode": "adjoint", "nnz": int(ctx.nnz), "rows": g.n_rows,
+                          "ratio_rows_ms": round(ms[0], 4), "adjoint_update_ms": round(ms[1], 4)}))
 
 
 if __name__ == "__main__":
