@@ -7,12 +7,14 @@
 * `unrolled_mlem(x0, omega, sino, ctx)`: K relaxed MLEM iterations
       x_{k+1} = x_k * r_k ** omega_k,  r_k = calcUpdate factor(A^T (s / A x_k), norm)
   (omega_k = 1 is the reference iteration, mlem_seq/seqcsr4mlem.cpp:163-167)
-  with gradients with respect to x0 and omega.  The backward pass keeps
-  only the K images x_k (per-iteration checkpoints) and recomputes A x_k and
-  A^T(s / A x_k) from them in one pass over the matrix, then propagates the
-  adjoint through calcCorrel and both projections in a second pass: two
-  passes per iteration (forward: one).  A context with
-  MLEM_FLAG_MIRROR_KERNELS runs the same arithmetic as separate projections.
+  with gradients with respect to x0 and omega.  The forward pass keeps, per
+  iteration, the row sums A x_k and the update factor r_k (K x (R + C)
+  floats) when they fit `keep_bytes`; the backward pass then propagates the
+  adjoint through calcCorrel and both projections in one pass over the
+  matrix per iteration.  Otherwise it keeps only the K images x_k
+  (per-iteration checkpoints) and first recomputes A x_k and A^T(s / A x_k)
+  from them in one more pass.  A context with MLEM_FLAG_MIRROR_KERNELS runs
+  the same arithmetic as separate projections.
 
 Zero rules follow the reference: the correlation is 0 where the projection
 is 0 (calcCorrel), the update factor is the raw back projection where the
@@ -138,29 +140,41 @@ def _adjoint(ctx, du, sino_i, f):
 
 class _UnrolledMLEM(torch.autograd.Function):
     @staticmethod
-    def forward(fctx, x0, omega, sino_f, norm, ctx, sino_i):
+    def forward(fctx, x0, omega, sino_f, norm, ctx, sino_i, keep):
         K = omega.shape[0]
         xs = [x0.detach()]
+        rs, fs = [], []
         x = x0.detach().contiguous()
         for k in range(K):
-            r, _ = _ratio_rows(ctx, x, sino_i, norm)
+            r, f = _ratio_rows(ctx, x, sino_i, norm)
+            if keep:
+                rs.append(r)
+                fs.append(f)
             x = x * torch.where(r > 0, r.clamp_min(1e-38) ** omega[k], torch.zeros_like(r))
             xs.append(x)
         fctx.mctx = ctx
         fctx.sino_i = sino_i
-        fctx.save_for_backward(torch.stack(xs[:-1]), omega, sino_f, norm, x)
+        fctx.keep = keep
+        saved = [torch.stack(xs[:-1]), omega, sino_f, norm, x]
+        if keep:
+            saved += [torch.stack(rs), torch.stack(fs)]
+        fctx.save_for_backward(*saved)
         return x
 
     @staticmethod
     def backward(fctx, g):
         ctx = fctx.mctx
-        xs, omega, sino_f, norm, _ = fctx.saved_tensors
+        saved = fctx.saved_tensors
+        xs, omega, sino_f, norm = saved[:4]
         K = omega.shape[0]
         g = g.contiguous()
         d_omega = torch.zeros_like(omega)
         for k in range(K - 1, -1, -1):
             xk = xs[k].contiguous()
-            r, f = _ratio_rows(ctx, xk, fctx.sino_i, norm)      # recomputed from the checkpoint
+            if fctx.keep:  # kept by the forward pass
+                r, f = saved[5][k], saved[6][k]
+            else:  # recomputed from the checkpoint
+                r, f = _ratio_rows(ctx, xk, fctx.sino_i, norm)
             pos = r > 0
             rs = torch.where(pos, r, torch.ones_like(r))
             p = torch.where(pos, rs ** omega[k], torch.zeros_like(r))  # r^w
@@ -174,16 +188,22 @@ class _UnrolledMLEM(torch.autograd.Function):
             # with zero counts has c = 0 whatever f is: no gradient) and of A
             gx = gx + _adjoint(ctx, du, fctx.sino_i, f)
             g = gx
-        return g, d_omega, None, None, None, None
+        return g, d_omega, None, None, None, None, None
 
 
 def unrolled_mlem(x0: torch.Tensor, omega: torch.Tensor, sino: torch.Tensor,
-                  ctx: "api.Context", norm: torch.Tensor | None = None) -> torch.Tensor:
-    """K = len(omega) relaxed MLEM iterations from x0 (float32 [C] CUDA)."""
+                  ctx: "api.Context", norm: torch.Tensor | None = None,
+                  keep_bytes: int = 2 << 30) -> torch.Tensor:
+    """K = len(omega) relaxed MLEM iterations from x0 (float32 [C] CUDA).
+    The forward pass keeps each iteration's row sums and update factor for
+    the backward pass when they take at most keep_bytes (0: always
+    recompute them)."""
     _check(x0, ctx.n_cols, "x0")
     if norm is None:
         norm = norm_tensor(ctx, x0.device)
     sino_i = sino.to(device=x0.device, dtype=torch.int32).contiguous()
     sino_f = sino_i.to(torch.float32)
+    K = int(omega.shape[0])
+    keep = K * (ctx.n_rows + ctx.n_cols) * 4 <= keep_bytes
     return _UnrolledMLEM.apply(x0, omega.to(device=x0.device, dtype=torch.float32), sino_f, norm,
-                               ctx, sino_i)
+                               ctx, sino_i, keep)

@@ -55,7 +55,10 @@ def _loss64(m, sino, x0, omega, x_true):
     return float(np.mean((xk - x_true) ** 2))
 
 
-def test_unrolled_mlem_gradients_match_fp64_finite_differences(small):
+@pytest.mark.parametrize("keep_bytes", [2 << 30, 0])
+def test_unrolled_mlem_gradients_match_fp64_finite_differences(small, keep_bytes):
+    """Both ways of the backward pass: the row sums and update factors kept
+    by the forward pass, and (keep_bytes 0) recomputed from the images."""
     m, sino, ctx = small
     K = 10
     x_true = synth.phantom(32, 32, 16, 5, 0).astype(np.float64)
@@ -66,7 +69,7 @@ def test_unrolled_mlem_gradients_match_fp64_finite_differences(small):
     xt = torch.tensor(x0, device="cuda", dtype=torch.float32, requires_grad=True)
     wt = torch.tensor(omega, device="cuda", dtype=torch.float32, requires_grad=True)
     st = torch.tensor(sino, device="cuda")
-    xK = torch_ext.unrolled_mlem(xt, wt, st, ctx)
+    xK = torch_ext.unrolled_mlem(xt, wt, st, ctx, keep_bytes=keep_bytes)
     loss = torch.mean((xK.double() - torch.tensor(x_true, device="cuda")) ** 2)
     loss.backward()
     gx = xt.grad.double().cpu().numpy()
@@ -99,7 +102,8 @@ def test_unrolled_mlem_gradients_match_fp64_finite_differences(small):
     assert np.linalg.norm(w_gpu - w_fd) <= 1e-3 * np.linalg.norm(w_fd)
 
 
-def test_unrolled_mlem_gradients_finite_with_tiny_projections(small):
+@pytest.mark.parametrize("keep_bytes", [2 << 30, 0])
+def test_unrolled_mlem_gradients_finite_with_tiny_projections(small, keep_bytes):
     """Rows with zero counts whose projection is tiny but nonzero (a start
     image of 1e-25: f^2 underflows to 0 in float32) give no gradient through
     calcCorrel instead of 0 / 0."""
@@ -111,7 +115,7 @@ def test_unrolled_mlem_gradients_finite_with_tiny_projections(small):
     xt = torch.full((m.n_cols,), 1e-25, device="cuda", dtype=torch.float32, requires_grad=True)
     wt = torch.ones(K, device="cuda", dtype=torch.float32, requires_grad=True)
     x_true = torch.tensor(synth.phantom(32, 32, 16, 5, 0), device="cuda", dtype=torch.float32)
-    xK = torch_ext.unrolled_mlem(xt, wt, torch.tensor(s, device="cuda"), ctx)
+    xK = torch_ext.unrolled_mlem(xt, wt, torch.tensor(s, device="cuda"), ctx, keep_bytes=keep_bytes)
     loss = torch.mean((xK - x_true) ** 2)
     loss.backward()
     assert torch.isfinite(xK).all()
