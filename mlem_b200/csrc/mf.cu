@@ -79,6 +79,10 @@ namespace {
 
 constexpr int kMfThreads = 256;
 constexpr int kMfWarps = kMfThreads / 32;
+// Slot t of lane j sits at word j + kMfStride * t of its warp's arrays: the
+// walk's writes (one slot of every lane) and the gathers' reads (eight slots
+// of four neighbouring lanes, bank (j + 4 t) mod 32) hit 32 different banks.
+constexpr int kMfStride = 36;
 
 __device__ __forceinline__ uint32_t mf_voxel(const MfGrid& g, const uint32_t* dil, const int32_t (&i)[3]) {
     if (g.pow2) return dil[i[0]] | dil[g.n[0] + i[1]] | dil[g.n[0] + g.n[1] + i[2]];
@@ -150,8 +154,8 @@ __device__ __forceinline__ uint32_t mf_walk(MfAxis X, MfAxis Y, MfAxis Z, float 
         if (len > 0.0f) {
             if (cnt == cap) { *over = true; break; }
             if (WRITE) {
-                vox[32 * cnt] = mf_voxel3(g, dil, X.i, Y.i, Z.i);
-                lens[32 * cnt] = len;
+                vox[kMfStride * cnt] = mf_voxel3(g, dil, X.i, Y.i, Z.i);
+                lens[kMfStride * cnt] = len;
             }
             ++cnt;
         }
@@ -168,8 +172,8 @@ __device__ __forceinline__ uint32_t mf_walk(MfAxis X, MfAxis Y, MfAxis Z, float 
 }
 
 // Lane `lane` traces its 1/32 of ray r into its own slots vox[0 .. n) /
-// lens[0 .. n) (slot t of lane j at j + 32 t in the warp's arrays, so the 32
-// lanes touch 32 different banks); returns n.
+// lens[0 .. n) (slot t of lane j at j + kMfStride t in the warp's arrays);
+// returns n.
 __device__ __forceinline__ uint32_t mf_trace_lane(const MfRay& r, const MfGrid& g, const uint32_t* dil,
                                                   uint32_t* vox, float* lens, uint32_t cap, int lane,
                                                   bool* over) {
@@ -198,12 +202,17 @@ __global__ void __launch_bounds__(kMfThreads, 4) k_mf_fused(const MfRay* __restr
                                                          float* __restrict__ u,
                                                          unsigned int* __restrict__ flag) {
     extern __shared__ uint32_t smem[];
-    const size_t per_warp = (size_t)32 * cap;
+    const size_t per_warp = (size_t)kMfStride * cap;
     uint32_t* dil = smem + (size_t)kMfWarps * 2 * per_warp;
     load_dil(g, dil_g, dil);
     const int lane = threadIdx.x & 31;
-    uint32_t* vox = smem + (size_t)(threadIdx.x >> 5) * 2 * per_warp + lane;
-    float* lens = reinterpret_cast<float*>(vox + per_warp);
+    uint32_t* wvox = smem + (size_t)(threadIdx.x >> 5) * 2 * per_warp;
+    float* wlens = reinterpret_cast<float*>(wvox + per_warp);
+    // the gathers and the scatter read the slots across lanes: lane i takes
+    // slot r0 + (i & 7) of lane 4 q + (i >> 3) in step q, so one instruction
+    // covers about 32 consecutive elements of the ray (four neighbouring
+    // intervals), and its sectors are shared as in the stored walk
+    const int sub = lane & 7, grp = lane >> 3;
     const uint64_t ph = l2_evict_last();
     bool over = false;
     const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
@@ -214,23 +223,41 @@ __global__ void __launch_bounds__(kMfThreads, 4) k_mf_fused(const MfRay* __restr
         const MfRay r = rays[k];
         const int32_t s = sino[r.row];
         if (s == 0 || !(r.a1 > r.a0)) continue;  // calcCorrel 0: nothing to scatter
-        const uint32_t cnt = mf_trace_lane(r, g, dil, vox, lens, cap, lane, &over);
+        const uint32_t cnt = mf_trace_lane(r, g, dil, wvox + lane, wlens + lane, cap, lane, &over);
+        __syncwarp();  // every lane's slots are written
+        uint32_t mx = cnt;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(MLEM_FULL_MASK, mx, o));
+        uint32_t oc[8];  // the slot counts of the lanes this lane reads from
+#pragma unroll
+        for (int q = 0; q < 8; ++q) oc[q] = __shfl_sync(MLEM_FULL_MASK, cnt, 4 * q + grp);
         float acc = 0.0f;
-        uint32_t t = 0;
-        for (; t + 4 <= cnt; t += 4) {  // four gathers in flight
-            float xv[4];
+        for (uint32_t r0 = 0; r0 < mx; r0 += 8) {
+            const uint32_t t = r0 + sub;
+            float xv[8], lv[8];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) xv[j] = ld_hot(x + vox[32 * (t + j)], ph);
+            for (int q = 0; q < 8; ++q) {
+                const uint32_t w = 4 * q + grp + kMfStride * t;
+                const bool ok = t < oc[q];
+                lv[q] = ok ? wlens[w] : 0.0f;
+                xv[q] = ok ? ld_hot(x + wvox[w], ph) : 0.0f;
+            }
 #pragma unroll
-            for (int j = 0; j < 4; ++j) acc = fmaf(lens[32 * (t + j)], xv[j], acc);
+            for (int q = 0; q < 8; ++q) acc = fmaf(lv[q], xv[q], acc);
         }
-        for (; t < cnt; ++t) acc = fmaf(lens[32 * t], ld_hot(x + vox[32 * t], ph), acc);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(MLEM_FULL_MASK, acc, o);
         const float c = correl_of(s, acc);
         if (c != 0.0f)
-            for (t = 0; t < cnt; ++t) atomicAdd(u + vox[32 * t], lens[32 * t] * c);
-        __syncwarp();
+            for (uint32_t r0 = 0; r0 < mx; r0 += 8) {
+                const uint32_t t = r0 + sub;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    const uint32_t w = 4 * q + grp + kMfStride * t;
+                    if (t < oc[q]) atomicAdd(u + wvox[w], wlens[w] * c);
+                }
+            }
+        __syncwarp();  // the slots are read before the next ray's walk
     }
     if (over) atomicOr(flag, 1u);
 }
@@ -241,7 +268,7 @@ __global__ void __launch_bounds__(kMfThreads, 4) k_mf_colsum(const MfRay* __rest
                                                           uint32_t cap, float* __restrict__ norm,
                                                           unsigned int* __restrict__ flag) {
     extern __shared__ uint32_t smem[];
-    const size_t per_warp = (size_t)32 * cap;
+    const size_t per_warp = (size_t)kMfStride * cap;
     uint32_t* dil = smem + (size_t)kMfWarps * 2 * per_warp;
     load_dil(g, dil_g, dil);
     const int lane = threadIdx.x & 31;
@@ -254,7 +281,7 @@ __global__ void __launch_bounds__(kMfThreads, 4) k_mf_colsum(const MfRay* __rest
         const MfRay r = rays[k];
         if (!(r.a1 > r.a0)) continue;
         const uint32_t cnt = mf_trace_lane(r, g, dil, vox, lens, cap, lane, &over);
-        for (uint32_t t = 0; t < cnt; ++t) atomicAdd(norm + vox[32 * t], lens[32 * t]);
+        for (uint32_t t = 0; t < cnt; ++t) atomicAdd(norm + vox[kMfStride * t], lens[kMfStride * t]);
         __syncwarp();
     }
     if (over) atomicOr(flag, 1u);
@@ -388,7 +415,7 @@ MfGrid grid_of(const mlem_mf* m) {
 
 size_t mf_smem(const mlem_mf* m) {
     // per warp: 32 lanes x cap slots of a voxel and a length, then the Morton parts
-    return (size_t)kMfWarps * 2 * 32 * m->cap * 4 + (size_t)(m->grid[0] + m->grid[1] + m->grid[2]) * 4;
+    return (size_t)kMfWarps * 2 * kMfStride * m->cap * 4 + (size_t)(m->grid[0] + m->grid[1] + m->grid[2]) * 4;
 }
 
 int mf_check_flag(mlem_mf* m) {
