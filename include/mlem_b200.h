@@ -240,6 +240,19 @@ int mlem_get_images(mlem_ctx* ctx, float* images);
 /* One iteration end to end on host buffers: upload the B sinograms and the B
  * images, iterate once on the device, download the images. */
 int mlem_step_host(mlem_ctx* ctx, const int32_t* sino, float* images_inout, uint32_t n_frames);
+/* n iterations on host buffers, each with sinograms of its own: iteration k
+ * uses sinos[k] ([B][R] int32, B = the context's frame count) and, when
+ * images is non-null and images[k] non-null, writes the B images after it to
+ * images[k] ([B][C] float32).  Iteration 0 starts from the context's images
+ * (mlem_init_images, mlem_set_images or an earlier call), iteration k + 1
+ * from iteration k's, which stay on the device.  The upload of sinos[k + 1]
+ * runs on a copy stream of its own during iteration k and the download of
+ * images[k] on another during iteration k + 1; with page-locked host buffers
+ * (cudaHostAlloc, cudaHostRegister) they overlap the kernels.  Every copy has
+ * ended when the call returns.  Afterwards the context holds sinos[n - 1] as
+ * its sinograms (the initImage sums of mlem_set_sinograms are kept). */
+int mlem_stream_host(mlem_ctx* ctx, const int32_t* const* sinos, float* const* images,
+                     uint32_t n);
 
 /* Phases of one iteration, as timed by mlem_profile_phases. */
 #define MLEM_PHASE_PROJECT 0     /* forward projection + calcCorrel (or the one-pass kernel) */

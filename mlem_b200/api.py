@@ -314,6 +314,42 @@ class Context:
         self._chk(core_lib().mlem_step_host(self._h, sino_ptr, images_ptr, n_frames))
         self.n_frames = n_frames
 
+    def stream_host(self, sinos, images=None) -> None:
+        """mlem_stream_host: len(sinos) iterations, iteration k with sinograms
+        sinos[k] ([B][R] int32 arrays, B = the context's frames) and, when
+        images is given, its images written into images[k] ([B][C] float32,
+        C-contiguous; None entries skip the download)."""
+        ss = [_i32(x) for x in sinos]
+        for x in ss:
+            if x.size != self.n_frames * self.n_rows:
+                raise MlemError(MLEM_ERR_INVALID, f"sinograms of {x.size} entries, expected "
+                                f"{self.n_frames} x {self.n_rows}")
+        ims = None
+        if images is not None:
+            if len(images) != len(ss):
+                raise MlemError(MLEM_ERR_INVALID, "one image buffer (or None) per iteration")
+            for x in images:
+                if x is not None and not (isinstance(x, np.ndarray) and x.dtype == np.float32 and
+                                          x.flags.c_contiguous and x.flags.writeable and
+                                          x.size == self.n_frames * self.n_cols):
+                    raise MlemError(MLEM_ERR_INVALID,
+                                    "images must be writable C-contiguous float32 arrays of B x C")
+            ims = [None if x is None else x.ctypes.data for x in images]
+        self.stream_host_ptr([x.ctypes.data for x in ss], ims)
+
+    def stream_host_ptr(self, sino_ptrs, image_ptrs=None) -> None:
+        """mlem_stream_host on raw host pointers (e.g. pinned torch tensors):
+        one sinogram pointer per iteration, and one image pointer (or None)
+        per iteration or no image list."""
+        n = len(sino_ptrs)
+        sp = (ctypes.c_void_p * max(n, 1))(*sino_ptrs)
+        ip = None
+        if image_ptrs is not None:
+            if len(image_ptrs) != n:
+                raise MlemError(MLEM_ERR_INVALID, "one image pointer (or None) per iteration")
+            ip = ctypes.cast((ctypes.c_void_p * max(n, 1))(*image_ptrs), ctypes.c_void_p)
+        self._chk(core_lib().mlem_stream_host(self._h, ctypes.cast(sp, ctypes.c_void_p), ip, n))
+
     # -- tuning -------------------------------------------------------------------
     @staticmethod
     def _tuning_dict(t) -> dict:

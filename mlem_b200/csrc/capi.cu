@@ -1305,6 +1305,14 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->celems_vis, (void*)c->row_pos})
         dev_free(p);
     if (c->act_host) cudaFreeHost(c->act_host);
+    for (cudaStream_t q : {c->up_stream, c->down_stream})
+        if (q) { cudaStreamSynchronize(q); cudaStreamDestroy(q); }
+    for (int i = 0; i < 2; ++i) {
+        dev_free(c->sstage[i]);
+        dev_free(c->istage[i]);
+        for (cudaEvent_t ev : {c->ev_up[i], c->ev_sfree[i], c->ev_img[i], c->ev_dfree[i]})
+            if (ev) cudaEventDestroy(ev);
+    }
     if (c->own_stream) cudaStreamSynchronize(c->own_stream);
     if (c->own_stream) cudaStreamDestroy(c->own_stream);
     delete c;
@@ -1608,6 +1616,115 @@ int mlem_step_host(mlem_ctx* c, const int32_t* sino, float* images, uint32_t B) 
     CK(c, cudaGraphLaunch(c->graph, c->stream));
     TRY(download_images(c, images));
     CK(c, cudaStreamSynchronize(c->stream));
+    if (counts) {
+        c->act_rows = static_cast<uint32_t>(c->act_host[0] & 0xffffffffull);
+        c->act_nnz = c->act_host[1];
+    } else if (!c->act_ready) {
+        c->act_rows = 0;
+        c->act_nnz = 0;
+    }
+    return MLEM_OK;
+}
+
+// The copy streams, events and double-buffered staging of mlem_stream_host
+// (created on first use, sized for the current frames).
+static int ensure_streaming(mlem_ctx* c) {
+    for (cudaStream_t* q : {&c->up_stream, &c->down_stream})
+        if (!*q) CK(c, cudaStreamCreateWithFlags(q, cudaStreamNonBlocking));
+    for (int i = 0; i < 2; ++i)
+        for (cudaEvent_t* ev : {&c->ev_up[i], &c->ev_sfree[i], &c->ev_img[i], &c->ev_dfree[i]})
+            if (!*ev) CK(c, cudaEventCreateWithFlags(ev, cudaEventDisableTiming));
+    const size_t sn = (size_t)c->R * c->B, in = (size_t)c->C * c->B;
+    for (int i = 0; i < 2; ++i) {
+        if (c->sstage_n < sn) {
+            if (c->sstage[i]) { dev_free(c->sstage[i]); c->device_bytes -= c->sstage_n * 4; c->sstage[i] = nullptr; }
+            TRY(dev_alloc(c, &c->sstage[i], std::max<size_t>(sn, 1)));
+        }
+        if (c->istage_n < in) {
+            if (c->istage[i]) { dev_free(c->istage[i]); c->device_bytes -= c->istage_n * 4; c->istage[i] = nullptr; }
+            TRY(dev_alloc(c, &c->istage[i], std::max<size_t>(in, 1)));
+        }
+    }
+    c->sstage_n = std::max(c->sstage_n, sn);
+    c->istage_n = std::max(c->istage_n, in);
+    return MLEM_OK;
+}
+
+// The steps of mlem_stream_host, enqueued on the three streams.
+static int stream_steps(mlem_ctx* c, const int32_t* const* sinos, float* const* images, uint32_t n) {
+    const uint32_t B = c->B, Bp = c->Bp;
+    const size_t sbytes = (size_t)c->R * B * 4, ibytes = (size_t)c->C * B * 4;
+    CK(c, cudaMemcpyAsync(c->sstage[0], sinos[0], sbytes, cudaMemcpyHostToDevice, c->up_stream));
+    CK(c, cudaEventRecord(c->ev_up[0], c->up_stream));
+    for (uint32_t k = 0; k < n; ++k) {
+        const int cur = (int)(k & 1), nxt = cur ^ 1;
+        if (k + 1 < n) {  // the next sinograms, once iteration k - 1 has copied that buffer out
+            CK(c, cudaStreamWaitEvent(c->up_stream, c->ev_sfree[nxt], 0));
+            CK(c, cudaMemcpyAsync(c->sstage[nxt], sinos[k + 1], sbytes, cudaMemcpyHostToDevice,
+                                  c->up_stream));
+            CK(c, cudaEventRecord(c->ev_up[nxt], c->up_stream));
+        }
+        CK(c, cudaStreamWaitEvent(c->stream, c->ev_up[cur], 0));
+        if (Bp == 1)
+            CK(c, cudaMemcpyAsync(c->sino, c->sstage[cur], sbytes, cudaMemcpyDeviceToDevice, c->stream));
+        else
+            CK(c, interleave_i32(c->sstage[cur], c->sino, c->R, B, Bp, c->stream));
+        CK(c, cudaEventRecord(c->ev_sfree[cur], c->stream));
+        TRY(build_active(c, false));
+        ++c->sino_gen;
+        if (c->graph_dirty || !c->graph || c->graph_iters != 1) {
+            TRY(ensure_history(c, 1));
+            TRY(capture(c, 1));
+        }
+        CK(c, cudaGraphLaunch(c->graph, c->stream));
+        if (images && images[k]) {  // this iteration's images, once the buffer's last download is done
+            CK(c, cudaStreamWaitEvent(c->stream, c->ev_dfree[cur], 0));
+            if (Bp == 1 && !c->bricked)
+                CK(c, cudaMemcpyAsync(c->istage[cur], c->x, ibytes, cudaMemcpyDeviceToDevice, c->stream));
+            else
+                CK(c, deinterleave_f32(c->x, c->istage[cur], c->C, B, Bp, c->bricked ? c->perm : nullptr,
+                                       c->stream));
+            CK(c, cudaEventRecord(c->ev_img[cur], c->stream));
+            CK(c, cudaStreamWaitEvent(c->down_stream, c->ev_img[cur], 0));
+            CK(c, cudaMemcpyAsync(images[k], c->istage[cur], ibytes, cudaMemcpyDeviceToHost,
+                                  c->down_stream));
+            CK(c, cudaEventRecord(c->ev_dfree[cur], c->down_stream));
+        }
+    }
+    return MLEM_OK;
+}
+
+int mlem_stream_host(mlem_ctx* c, const int32_t* const* sinos, float* const* images, uint32_t n) {
+    if (!c) return fail(nullptr, MLEM_ERR_INVALID, "null context");
+    if (n == 0) return MLEM_OK;
+    if (!sinos) return fail(c, MLEM_ERR_INVALID, "null argument");
+    for (uint32_t k = 0; k < n; ++k)
+        if (!sinos[k]) return fail(c, MLEM_ERR_INVALID, "sinograms of iteration %u: null", k);
+    if (!c->B) return fail(c, MLEM_ERR_STATE, "mlem_set_sinograms must come first");
+    if (!c->images_ready) return fail(c, MLEM_ERR_STATE, "images not initialised");
+    TRY(set_device(c));
+    TRY(ensure_streaming(c));
+    if (c->tuning.bk_mode == MLEM_BK_REGION && !(c->flags & MLEM_FLAG_EXACT))
+        TRY(ensure_region(c, c->tuning.frame_tile));
+    if (c->act_ready && !c->act_host &&
+        cudaHostAlloc(reinterpret_cast<void**>(&c->act_host), 16, cudaHostAllocDefault) != cudaSuccess) {
+        cudaGetLastError();
+        c->act_host = nullptr;
+    }
+    int s = stream_steps(c, sinos, images, n);
+    const bool counts = s == MLEM_OK && c->act_ready && c->act_host;
+    if (counts &&
+        (cudaMemcpyAsync(c->act_host, c->act_n, 4, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||
+         cudaMemcpyAsync(c->act_host + 1, c->act_z, 8, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess))
+        s = fail(c, MLEM_ERR_CUDA, "row counts: %s", cudaGetErrorString(cudaGetLastError()));
+    // every copy that names a caller buffer ends before the call returns, failed or not
+    cudaError_t e = cudaSuccess;
+    for (cudaStream_t q : {c->up_stream, c->stream, c->down_stream}) {
+        const cudaError_t eq = cudaStreamSynchronize(q);
+        if (e == cudaSuccess) e = eq;
+    }
+    if (s != MLEM_OK) return s;
+    if (e != cudaSuccess) return fail(c, MLEM_ERR_CUDA, "streamed iterations: %s", cudaGetErrorString(e));
     if (counts) {
         c->act_rows = static_cast<uint32_t>(c->act_host[0] & 0xffffffffull);
         c->act_nnz = c->act_host[1];

@@ -112,6 +112,14 @@ struct mlem_ctx {
     float* update = nullptr;
     void* stage = nullptr;  // staging for frame-major <-> interleaved copies
     size_t stage_bytes = 0;
+    // mlem_stream_host: an upload and a download stream, double-buffered
+    // staging of the sinograms and images, and the events between the streams
+    cudaStream_t up_stream = nullptr, down_stream = nullptr;
+    int32_t* sstage[2] = {nullptr, nullptr};
+    float* istage[2] = {nullptr, nullptr};
+    size_t sstage_n = 0, istage_n = 0;  // elements of each buffer
+    cudaEvent_t ev_up[2] = {nullptr, nullptr}, ev_sfree[2] = {nullptr, nullptr};
+    cudaEvent_t ev_img[2] = {nullptr, nullptr}, ev_dfree[2] = {nullptr, nullptr};
     bool images_ready = false;
 
     // statistics history

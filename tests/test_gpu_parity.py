@@ -209,6 +209,66 @@ def test_step_host_matches_iterate(ctxs):
     assert x.tobytes() == ctx.get_images().tobytes()
 
 
+def test_stream_host_matches_step_host(ctxs):
+    """mlem_stream_host with one sinogram per iteration equals the same
+    iterations through mlem_step_host, bit for bit with the deterministic CSC
+    method (the image stays on the device between the streamed iterations)."""
+    ctx, m, sino, iters, gold = ctxs["tiny_it10"]
+    rng = np.random.default_rng(31)
+    sinos = [rng.permutation(sino).astype(np.int32) for _ in range(6)]
+    ctx.set_sinograms(sino)
+    ctx.set_tuning(bk_mode=api.BK_CSC, group=32, frame_tile=1, blocks_per_sm=8)
+    init = ctx.init_images()
+    x = np.full((1, m.n_cols), init[0], np.float32)
+    want = []
+    for s in sinos:
+        ctx.step_host(s, x)
+        want.append(x.copy())
+    ctx.set_sinograms(sino)
+    ctx.init_images()
+    got = [np.zeros((1, m.n_cols), np.float32) for _ in sinos]
+    got[2] = None  # no download for iteration 2
+    ctx.stream_host(sinos, got)
+    for k, g in enumerate(got):
+        if g is not None:
+            assert g.tobytes() == want[k].tobytes(), k
+    assert ctx.get_images().tobytes() == want[-1].tobytes()
+    ctx._refresh()
+    assert ctx.info.rows_with_counts == int((sinos[-1] != 0).sum())
+
+
+@pytest.mark.parametrize("flags", [0, api.FLAG_NATURAL_LAYOUT])
+@pytest.mark.parametrize("frames", [1, 3])
+def test_stream_host_against_oracle(golden, flags, frames):
+    """Streamed iterations on the one-pass method, each with other sinograms,
+    against the oracle's MLEM step by step, in both voxel layouts and with one
+    and three frames (padded to four); images=None downloads nothing."""
+    m, sino, _, _, _ = golden.case("plain_small_it10")
+    rng = np.random.default_rng(32 + frames)
+    n = 5
+    sinos = [np.stack([rng.permutation(sino) for _ in range(frames)]).astype(np.int32)
+             for _ in range(n)]
+    with api.Context.from_matrix(m, flags=flags) as ctx:
+        ctx.set_sinograms(sinos[0])
+        ctx.set_tuning(bk_mode=api.BK_FUSED, group=32, frame_tile=1, blocks_per_sm=4,
+                       visit=api.VISIT_SORTED_CHUNKED)
+        x = ctx.init_images()
+        cur = np.repeat(np.asarray(x, np.float32)[:, None], m.n_cols, axis=1)
+        got = [np.zeros((frames, m.n_cols), np.float32) for _ in range(n)]
+        ctx.stream_host(sinos, got)
+        for k in range(n):
+            for b in range(frames):
+                want, _ = ob.mlem(m, sinos[k][b], 1, start_image=cur[b])
+                assert ob.rel_l2(got[k][b], want) <= TOL_MLEM, (k, b)
+            cur = got[k]
+        ctx.stream_host(sinos[:2])  # no images: the context's own advance
+        assert ctx.get_images().shape == (frames, m.n_cols)
+        with pytest.raises(api.MlemError):
+            ctx.stream_host([sinos[0][:, :-1]])  # wrong size
+        with pytest.raises(api.MlemError):
+            ctx.stream_host(sinos[:2], [got[0]])  # one buffer per iteration
+
+
 def test_device_generator_matches_host_generator():
     g = synth.Geometry(32, 32, 16, 20000, 20, 80, seed=9)
     hm = synth.host_matrix(g)
