@@ -700,6 +700,14 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                 if (by_visit) {
                     fw.out_by_visit = true;
                     bk.pairs = reinterpret_cast<const uint4*>(c->celems_vis);
+                    if (c->act_ready && c->row_pos) {
+                        // walk only the rows with counts; the others keep calcCorrel 0
+                        fw.order = c->act_order;
+                        fw.vrange = c->act_ranges;
+                        fw.n_dev = c->act_n;
+                        fw.out_pos = c->row_pos;
+                        CK(c, cudaMemsetAsync(c->correl, 0, (size_t)c->R * Bp * 4, st));
+                    }
                 }
                 for (uint32_t f0 = 0; f0 < Bp; f0 += T)
                     CK(c, fwproj(fw, c->x, Bp, f0, c->sino, c->correl, nullptr, cfg, st));
@@ -805,8 +813,10 @@ namespace mlem {
 void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* bytes,
                      int* launches, bool active_rows) {
     const double C = c->C, B = c->B;
-    // the one-pass sorted walk visits only the rows with counts
-    const bool act = active_rows && c->act_ready && bk_mode == MLEM_BK_FUSED &&
+    // the one-pass sorted walk, and the CSC method's forward pass over the CSC
+    // in visiting order, visit only the rows with counts
+    const bool csc_act = bk_mode == MLEM_BK_CSC && c->row_pos && csc_by_visit(c, c->tuning);
+    const bool act = active_rows && c->act_ready && (bk_mode == MLEM_BK_FUSED || csc_act) &&
                      c->n_subsets == 1 && !(c->flags & MLEM_FLAG_EXACT);
     const double R = act ? (double)c->act_rows : (double)c->R;
     const double Z = act ? (double)c->act_nnz : (double)c->Z;
@@ -814,7 +824,7 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
     const int mode = exact ? MLEM_BK_CSC : bk_mode;
     const double tiles = exact ? 1.0 : (double)(c->Bp / (uint32_t)frame_tile);
     const double csr_pass = 8.0 * (R + 1) + 8.0 * Z;
-    const double csc_pass = 8.0 * (C + 1) + 8.0 * Z;
+    const double csc_pass = 8.0 * (C + 1) + 8.0 * (double)c->Z;  // every column, every element
     for (int p = 0; p < MLEM_N_PHASES; ++p) { bytes[p] = 0.0; launches[p] = 0; }
     const int nt = (int)tiles;
     if (mode == MLEM_BK_REGION) {
@@ -860,6 +870,7 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
         if (!exact && c->n_long) launches[0] += 2;  // the long-row kernels
     } else {
         bytes[0] = tiles * csr_pass + B * (4.0 * C + 4.0 * R + 4.0 * R);  // x, sino, correl
+        if (act && csc_act) bytes[0] += B * 4.0 * (double)c->R;  // the correlations zeroed
         launches[0] = exact ? 1 : nt;
     }
     if (mode == MLEM_BK_CSC) {

@@ -53,17 +53,26 @@ __global__ void __launch_bounds__(256) k_fwproj(SparseView csr, const float* __r
     // frames has calcCorrel 0 whatever its projection, so its elements are
     // not read (the counts are loaded beside the row range).
     const bool skip_empty = c != nullptr && y == nullptr;
-    for (uint64_t base = warp * RPW; base < csr.n; base += nwarps * RPW) {
+    // the visiting positions: a device-built list (the rows with counts) or all n
+    const uint64_t nv = visit_count(csr);
+    for (uint64_t base = warp * RPW; base < nv; base += nwarps * RPW) {
         const uint64_t v = base + lw / G;
-        const bool active = v < csr.n;
-        const uint64_t r = active ? row_at(csr, v) : 0;
-        uint64_t b = 0, e = 0;
+        const bool active = v < nv;
+        uint64_t r = 0, b = 0, e = 0;
         int32_t s[VW];
 #pragma unroll
         for (int i = 0; i < VW; ++i) s[i] = 0;
         if (active) {
-            b = csr.ptr[r];
-            e = csr.ptr[r + 1];
+            if (csr.vrange) {  // a sorted visit: the row's range in one load
+                const ulonglong2 q = csr.vrange[v];
+                r = csr.order[v];
+                b = q.x;
+                e = q.y;
+            } else {
+                r = row_at(csr, v);
+                b = csr.ptr[r];
+                e = csr.ptr[r + 1];
+            }
             if (c) ld_counts<VW>(sino + r * B + f0 + sub * VW, s);
         }
         if (skip_empty) {
@@ -79,7 +88,8 @@ __global__ void __launch_bounds__(256) k_fwproj(SparseView csr, const float* __r
         row_dot<G, BT, false>(el, b, e, lane, x, B, f0 + sub * VW, acc, ps, ph);
         slot_allreduce<G, BT>(acc);
         if (active && lane < FL) {
-            const uint64_t oidx = (csr.out_by_visit ? v : r) * B + f0 + sub * VW;
+            const uint64_t pos = csr.out_pos ? (uint64_t)csr.out_pos[r] : v;
+            const uint64_t oidx = (csr.out_by_visit ? pos : r) * B + f0 + sub * VW;
             if (y) st_vec<VW>(y + oidx, acc);
             if (c) {
                 float o[VW];

@@ -40,6 +40,9 @@ struct SparseView {
     // visiting position instead of its row index -- the layout the CSC in
     // visiting order (mlem_ctx::celems_vis) gathers from.
     bool out_by_visit = false;
+    // k_fwproj only, with out_by_visit and a device-built list (n_dev): the
+    // position of row r in the full visiting order is out_pos[r].
+    const uint32_t* out_pos = nullptr;
 };
 
 // Row index of visiting position v.
