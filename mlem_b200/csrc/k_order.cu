@@ -12,6 +12,8 @@
 // order of the scatter atomics, which is unordered anyway.
 #include <cub/device/device_radix_sort.cuh>
 #include <cub/device/device_select.cuh>
+#include <thrust/iterator/counting_iterator.h>
+#include <thrust/iterator/transform_iterator.h>
 
 #include <algorithm>
 
@@ -58,23 +60,37 @@ __global__ void k_row_ranges(SparseView csr, const uint32_t* __restrict__ order,
     }
 }
 
-// flags[k] = row order[k] has a nonzero count in some frame; *z += the
-// elements of those rows (one atomic per warp).
-__global__ void k_active_flags(const uint32_t* __restrict__ order,
-                               const ulonglong2* __restrict__ vrange, uint32_t n,
-                               const int32_t* __restrict__ sino, uint32_t Bp,
-                               uint8_t* __restrict__ flags, unsigned long long* __restrict__ z) {
-    unsigned long long mine = 0;
-    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n;
-         k += (uint64_t)gridDim.x * blockDim.x) {
+// Whether the row at visiting position k has a count in some frame (the
+// selection flag, computed as the select reads it).
+struct HasCount {
+    const uint32_t* order;
+    const int32_t* sino;
+    uint32_t Bp;
+    __host__ __device__ __forceinline__ uint8_t operator()(uint32_t k) const {
         const int32_t* s = sino + (size_t)order[k] * Bp;
         bool any = false;
         for (uint32_t f = 0; f < Bp; ++f) any |= (s[f] != 0);
-        flags[k] = any ? 1 : 0;
-        if (any) {
-            const ulonglong2 q = vrange[k];
-            mine += q.y - q.x;
-        }
+        return any ? 1 : 0;
+    }
+};
+using PosIt = thrust::counting_iterator<uint32_t>;
+using FlagIt = thrust::transform_iterator<HasCount, PosIt, uint8_t>;
+
+// The selected visiting positions (in act_order) become the rows and their
+// ranges, in place; *z += their elements (one atomic per warp).
+__global__ void k_active_gather(const uint32_t* __restrict__ order,
+                                const ulonglong2* __restrict__ vrange,
+                                const uint32_t* __restrict__ n_act, uint32_t* __restrict__ act_order,
+                                ulonglong2* __restrict__ act_ranges, unsigned long long* __restrict__ z) {
+    const uint64_t n = *n_act;
+    unsigned long long mine = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n;
+         i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t k = act_order[i];
+        const ulonglong2 q = vrange[k];
+        act_order[i] = order[k];
+        act_ranges[i] = q;
+        mine += q.y - q.x;
     }
     for (int o = 16; o > 0; o >>= 1) mine += __shfl_xor_sync(MLEM_FULL_MASK, mine, o);
     if ((threadIdx.x & 31) == 0 && mine) atomicAdd(z, mine);
@@ -83,34 +99,32 @@ __global__ void k_active_flags(const uint32_t* __restrict__ order,
 }  // namespace
 
 size_t active_rows_tmp_bytes(uint32_t n) {
-    size_t a = 0, b = 0;
-    cub::DeviceSelect::Flagged(nullptr, a, static_cast<const uint32_t*>(nullptr),
-                               static_cast<const uint8_t*>(nullptr), static_cast<uint32_t*>(nullptr),
-                               static_cast<uint32_t*>(nullptr), (int)n);
-    cub::DeviceSelect::Flagged(nullptr, b, static_cast<const ulonglong2*>(nullptr),
-                               static_cast<const uint8_t*>(nullptr), static_cast<ulonglong2*>(nullptr),
-                               static_cast<uint32_t*>(nullptr), (int)n);
-    return std::max<size_t>(std::max(a, b), 16);
+    size_t a = 0;
+    cub::DeviceSelect::Flagged(nullptr, a, PosIt(0), FlagIt(PosIt(0), HasCount{nullptr, nullptr, 1}),
+                               static_cast<uint32_t*>(nullptr), static_cast<uint32_t*>(nullptr),
+                               (int)n);
+    return std::max<size_t>(a, 16);
 }
 
+// Two passes: the select of the visiting positions whose rows have counts
+// (flags computed on the fly from the order and the sinograms), then the
+// gather of those rows and ranges; the list keeps the visiting order.
 cudaError_t active_rows_build(const SparseView& csr, const int32_t* sino, uint32_t Bp,
                               uint8_t* flags, void* tmp, size_t tmp_bytes, uint32_t* act_order,
                               ulonglong2* act_ranges, uint32_t* act_n, unsigned long long* act_z,
                               cudaStream_t st) {
+    (void)flags;
     if (!csr.order || !csr.vrange || csr.n > 0x7fffffffu || Bp == 0) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(act_z, 0, sizeof(unsigned long long), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(act_n, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess || csr.n == 0) return e;
-    const int grid = (int)std::min<uint64_t>((csr.n + 255) / 256, 148ull * 16);
-    k_active_flags<<<grid, 256, 0, st>>>(csr.order, csr.vrange, csr.n, sino, Bp, flags, act_z);
-    e = cudaGetLastError();
     size_t tb = tmp_bytes;
-    if (e == cudaSuccess)
-        e = cub::DeviceSelect::Flagged(tmp, tb, csr.order, flags, act_order, act_n, (int)csr.n, st);
-    tb = tmp_bytes;
-    if (e == cudaSuccess)
-        e = cub::DeviceSelect::Flagged(tmp, tb, csr.vrange, flags, act_ranges, act_n, (int)csr.n, st);
-    return e;
+    e = cub::DeviceSelect::Flagged(tmp, tb, PosIt(0), FlagIt(PosIt(0), HasCount{csr.order, sino, Bp}),
+                                   act_order, act_n, (int)csr.n, st);
+    if (e != cudaSuccess) return e;
+    const int grid = (int)std::min<uint64_t>((csr.n + 255) / 256, 148ull * 16);
+    k_active_gather<<<grid, 256, 0, st>>>(csr.order, csr.vrange, act_n, act_order, act_ranges, act_z);
+    return cudaGetLastError();
 }
 
 cudaError_t row_ranges_build(const SparseView& csr, const uint32_t* order, ulonglong2* vrange,
