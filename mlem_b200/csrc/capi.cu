@@ -535,7 +535,6 @@ int build_active_list(mlem_ctx* c, bool read_back) {
         int s = MLEM_OK;
         if (!c->act_order) s = dev_alloc(c, &c->act_order, c->R);
         if (s == MLEM_OK && !c->act_ranges) s = dev_alloc(c, &c->act_ranges, c->R);
-        if (s == MLEM_OK && !c->act_flags) s = dev_alloc(c, &c->act_flags, c->R);
         if (s == MLEM_OK && !c->act_n) s = dev_alloc(c, &c->act_n, 1);
         if (s == MLEM_OK && !c->act_z) s = dev_alloc(c, &c->act_z, 1);
         if (s == MLEM_OK) s = dev_alloc(c, &c->act_tmp, tb);
@@ -545,7 +544,7 @@ int build_active_list(mlem_ctx* c, bool read_back) {
         }
         c->act_tmp_bytes = tb;
     }
-    CK(c, active_rows_build(csr_view(c), c->sino, c->Bp, c->act_flags, c->act_tmp,
+    CK(c, active_rows_build(csr_view(c), c->sino, c->Bp, c->act_tmp,
                             c->act_tmp_bytes, c->act_order, c->act_ranges, c->act_n, c->act_z,
                             c->stream));
     if (read_back) {
@@ -573,7 +572,7 @@ int build_subset_lists(mlem_ctx* c) {
         v.order = c->sub_sorted + o;
         v.vrange = c->sub_sorted_ranges + o;
         v.n = (uint32_t)(c->sub_off[k + 1] - o);
-        CK(c, active_rows_build(v, c->sino, c->Bp, c->act_flags, c->act_tmp, c->act_tmp_bytes,
+        CK(c, active_rows_build(v, c->sino, c->Bp, c->act_tmp, c->act_tmp_bytes,
                                 c->sub_act_order + o, c->sub_act_ranges + o, c->sub_act_n + k,
                                 c->sub_act_z + k, c->stream));
     }
@@ -1312,7 +1311,7 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->sub_file, (void*)c->sub_file_ranges, (void*)c->sub_sorted,
                     (void*)c->sub_sorted_ranges, (void*)c->mirror_lut, (void*)c->mirror_vox,
                     (void*)c->f_mirror_d, (void*)c->act_order, (void*)c->act_ranges,
-                    (void*)c->act_flags, (void*)c->act_tmp, (void*)c->act_n, (void*)c->act_z,
+                    (void*)c->act_tmp, (void*)c->act_n, (void*)c->act_z,
                     (void*)c->celems_vis, (void*)c->row_pos})
         dev_free(p);
     if (c->act_host) cudaFreeHost(c->act_host);

@@ -60,7 +60,6 @@ struct mlem_ctx {
     // act_nnz are read back by mlem_set_sinograms.
     uint32_t* act_order = nullptr;
     ulonglong2* act_ranges = nullptr;
-    uint8_t* act_flags = nullptr;
     uint8_t* act_tmp = nullptr;
     size_t act_tmp_bytes = 0;
     uint32_t* act_n = nullptr;

@@ -110,10 +110,9 @@ size_t active_rows_tmp_bytes(uint32_t n) {
 // (flags computed on the fly from the order and the sinograms), then the
 // gather of those rows and ranges; the list keeps the visiting order.
 cudaError_t active_rows_build(const SparseView& csr, const int32_t* sino, uint32_t Bp,
-                              uint8_t* flags, void* tmp, size_t tmp_bytes, uint32_t* act_order,
+                              void* tmp, size_t tmp_bytes, uint32_t* act_order,
                               ulonglong2* act_ranges, uint32_t* act_n, unsigned long long* act_z,
                               cudaStream_t st) {
-    (void)flags;
     if (!csr.order || !csr.vrange || csr.n > 0x7fffffffu || Bp == 0) return cudaErrorInvalidValue;
     cudaError_t e = cudaMemsetAsync(act_z, 0, sizeof(unsigned long long), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(act_n, 0, sizeof(uint32_t), st);

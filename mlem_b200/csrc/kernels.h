@@ -251,11 +251,11 @@ cudaError_t row_ranges_build(const SparseView& csr, const uint32_t* order, ulong
 // rows whose counts are zero in all Bp frames of sino ([R][Bp]): their
 // calcCorrel is 0 in every frame, so they add nothing to the update and their
 // forward sums are never used.  Writes act_order / act_ranges (csr.n
-// capacity), *act_n = rows kept, *act_z = their elements; flags: csr.n
-// bytes; tmp: active_rows_tmp_bytes(csr.n) bytes.
+// capacity), *act_n = rows kept, *act_z = their elements; tmp:
+// active_rows_tmp_bytes(csr.n) bytes.  The list keeps the visiting order.
 size_t active_rows_tmp_bytes(uint32_t n);
 cudaError_t active_rows_build(const SparseView& csr, const int32_t* sino, uint32_t Bp,
-                              uint8_t* flags, void* tmp, size_t tmp_bytes, uint32_t* act_order,
+                              void* tmp, size_t tmp_bytes, uint32_t* act_order,
                               ulonglong2* act_ranges, uint32_t* act_n, unsigned long long* act_z,
                               cudaStream_t st);
 
