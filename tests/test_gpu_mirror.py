@@ -56,6 +56,32 @@ def test_column_sums_and_mlem(sym, grid, flags):
         assert ob.rel_l2(ctx.get_images()[0], want) <= TOL
 
 
+def test_host_step_and_streamed_iterations():
+    """mlem_step_host and mlem_stream_host on a mirrored context (the
+    sinogram per iteration indexes the full matrix's rows): each iteration
+    against the oracle's on the expanded matrix."""
+    m = sym_matrix(7, seed=91, grid=(8, 8, 4))
+    full = ob.expand_symmetries(m)
+    B = 2
+    sinos = [_frames(m, B, 100 + k) for k in range(4)]
+    with api.Context.symmetric(m, flags=MK) as ctx:
+        ctx.set_sinograms(sinos[0])
+        init = ctx.init_images()
+        cur = np.repeat(np.asarray(init, np.float32)[:, None], m.n_cols, axis=1)
+        got = [np.zeros((B, m.n_cols), np.float32) for _ in sinos]
+        ctx.stream_host(sinos, got)
+        for k, s in enumerate(sinos):
+            for b in range(B):
+                want, _ = ob.mlem(full, s[b], 1, start_image=cur[b])
+                assert ob.rel_l2(got[k][b], want) <= TOL, (k, b)
+            cur = got[k]
+        x = cur.copy()
+        ctx.step_host(sinos[0], x)
+        for b in range(B):
+            want, _ = ob.mlem(full, sinos[0][b], 1, start_image=cur[b])
+            assert ob.rel_l2(x[b], want) <= TOL, b
+
+
 @pytest.mark.parametrize("B,tile", [(3, 1), (3, 4), (8, 2), (16, 16), (12, 8)])
 @pytest.mark.parametrize("visit", [api.VISIT_FILE, api.VISIT_SORTED])
 def test_frames_tiles_visits(B, tile, visit):
