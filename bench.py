@@ -513,9 +513,16 @@ def run_ours(a, rank, world, local_rank, parallelism):
             if not a.no_parity_full:
                 jobs = ParityJobs(d, mpath, spaths, a.parity_iters, host_threads())
 
+        # --- what the L2 serves to random addresses (the one-pass walk's bound) ---
+        l2 = api.measure_l2_rates(torch.cuda.current_device())
+        head["l2_rates"] = {k: round(v / 1e9, 1) for k, v in l2.items()}
+        head["l2_rates"]["unit"] = "G/s"
+
         # --- batched: 16 sinograms in one pass over the matrix per iteration ---
         if fb is not None:
             ctx.set_sinograms(fb.sinograms)
+            ctx._refresh()
+            visited16 = int(ctx.info.nnz_with_counts)
             ctx.init_images()
             tb = ctx.autotune()
             ctx.init_images()
@@ -535,6 +542,9 @@ def run_ours(a, rank, world, local_rank, parallelism):
                 "hbm_gbs": round(float(bph_bytes.sum()) / (bms / 1e3) / 1e9, 1),
                 "method": f"{api.BK_NAMES[tb['bk_mode']]}/{api.VISIT_NAMES[tb['visit']]}"
                           f"/tile{tb['frame_tile']}",
+                # one 64-byte row reduction per visited element at 16 frames, at the
+                # measured rate of random 64-byte row reductions
+                "reduction_floor_ms": round(visited16 / l2["red_64B_rows_per_s"] * 1e3, 3),
             }
             detail["batched_phases_ms"] = [round(float(x), 4) for x in bph_ms]
 

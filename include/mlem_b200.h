@@ -267,6 +267,14 @@ int mlem_stream_host(mlem_ctx* ctx, const int32_t* const* sinos, float* const* i
  * offset and vector entry counted once per pass); launches[p]: kernels per
  * iteration.  Changes the images like mlem_iterate. */
 int mlem_profile_phases(mlem_ctx* ctx, int n_iter, double* ms, double* bytes, int* launches);
+/* The rates the L2 serves to random addresses on `device`, measured with
+ * four small kernels over a 64 MB scratch array (allocated and freed here):
+ * rates[0] float gathers of 4 bytes per second, rates[1] gathers of 64-byte
+ * rows (16 floats) per second, rates[2] float reductions (red.global.add) of
+ * 4 bytes per second, rates[3] reductions of 64-byte rows per second.  The
+ * one-pass iteration gathers and reduces at such addresses; its measured
+ * bound.  No counterpart in the reference. */
+int mlem_measure_l2_rates(int device, double* rates);
 
 /* ---- tuning --------------------------------------------------------------- */
 int mlem_get_tuning(const mlem_ctx* ctx, mlem_tuning* out);

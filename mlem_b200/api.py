@@ -674,6 +674,16 @@ class MatrixFree:
         return {"device_bytes": int(b.value), "lane_capacity": int(cap.value)}
 
 
+def measure_l2_rates(device: int = 0) -> dict:
+    """mlem_measure_l2_rates: what the L2 serves to random addresses, per
+    second -- float gathers of 4 bytes and of 64-byte rows, float reductions
+    of 4 bytes and of 64-byte rows (the rates that bound the one-pass walk)."""
+    r = np.zeros(4, np.float64)
+    _raise(core_lib().mlem_measure_l2_rates(device, _p(r)))
+    return {"gather_4B_per_s": float(r[0]), "gather_64B_rows_per_s": float(r[1]),
+            "red_4B_per_s": float(r[2]), "red_64B_rows_per_s": float(r[3])}
+
+
 NOALLOC_MAX_VOXELS = 1048576
 
 

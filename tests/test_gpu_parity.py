@@ -600,3 +600,13 @@ def test_rows_without_counts_are_skipped(golden, visit, bps):
         for b in range(B):
             want, _ = ob.mlem(m, zero[b], 1, start_image=x0[b])
             assert x[b].tobytes() == want.tobytes()
+
+
+def test_measure_l2_rates():
+    """mlem_measure_l2_rates: four positive rates; float reductions to random
+    addresses run slower than gathers of the same width (the bound of the
+    one-pass walk)."""
+    r = api.measure_l2_rates(0)
+    assert all(v > 0 for v in r.values())
+    assert r["red_4B_per_s"] < r["gather_4B_per_s"]
+    assert r["red_64B_rows_per_s"] < r["gather_64B_rows_per_s"]
