@@ -483,6 +483,28 @@ def run_ours(a, rank, world, local_rank, parallelism):
     }
     tail = {}
 
+    # --- the deterministic method (the CSC back projection, over the CSC in visiting
+    # order with the sorted visit; the CLI's default), autotuned among the
+    # deterministic methods and timed like the headline, then the fast tuning back ---
+    if a.mode == "auto":
+        td = ctx.autotune(deterministic_only=True)
+        ctx.init_images()
+        ctx.iterate(a.warmup, stats=False)
+        kd = max(10, a.steps // 4)
+        barrier()
+        e0.record(stream)
+        ctx.iterate(kd)
+        e1.record(stream)
+        barrier()
+        dms = e0.elapsed_time(e1) / kd
+        head["deterministic"] = {
+            "method": f"{api.BK_NAMES[td['bk_mode']]}/{api.VISIT_NAMES[td['visit']]}",
+            "ms_per_iteration": round(dms, 4), "iterations_per_s": round(world * 1e3 / dms, 3),
+            "two_pass_formula_frac": round(tp / (dms / 1e3) / 1e9 / peak, 4)}
+        ctx.set_tuning(bk_mode=tuning["bk_mode"], group=tuning["group"],
+                       frame_tile=tuning["frame_tile"], blocks_per_sm=tuning["blocks_per_sm"],
+                       visit=tuning["visit"])
+
     host_legs = rank == 0 and world == 1 and not a.no_cpu_baseline
     wb = synth.WORKLOADS["batched-b16"]
     fb = synth.make_frames(wb, ctx.project_f64) if not a.no_batched else None
