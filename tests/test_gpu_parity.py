@@ -180,12 +180,13 @@ def test_csc_in_visiting_order_skips_rows_without_counts(golden, tile):
             assert ob.rel_l2(x[b], want) <= TOL_MLEM, b
 
 
-@pytest.mark.parametrize("group,tile", [(32, 1), (16, 4), (8, 16)])
+@pytest.mark.parametrize("group,tile", [(32, 1), (16, 4), (8, 16), (32, 2)])
 def test_csc_in_visiting_order_with_frames(golden, group, tile):
     m, sino, iters, gold, _ = golden.case("tiny_it10")
     rng = np.random.default_rng(7 * tile)
     B = 16
     sinos = np.stack([rng.permutation(sino) if b else sino for b in range(B)]).astype(np.int32)
+    sinos[3, ::3] = 0  # rows without counts in some frames
     with api.Context.from_matrix(m) as ctx:
         ctx.set_sinograms(sinos)
         ctx.set_tuning(bk_mode=api.BK_CSC, group=group, frame_tile=tile, blocks_per_sm=8,
