@@ -111,7 +111,17 @@ typedef struct {
  * (another Z x 8 bytes + R x 4): the forward pass stores the correlations
  * by that position and the back projection gathers neighbouring rays.  It
  * stays deterministic (each column summed in ascending position); with
- * MLEM_VISIT_FILE the CSC lists rows ascending, as calcBkProj adds them. */
+ * MLEM_VISIT_FILE the CSC lists rows ascending, as calcBkProj adds them.
+ * With sinograms set, that CSC is also copied cut to the rays with a count in
+ * some frame (another Z x 8 bytes + C x 4 + R / 8, made only while 2 GiB of
+ * the device stay free beside it), and the back projection walks those
+ * entries only, leaving out terms that are +0.  mlem_set_sinograms refills
+ * the copy, as does selecting the method; mlem_step_host and
+ * mlem_stream_host, one iteration per sinogram, walk the whole CSC in
+ * visiting order instead (the copy takes about as long as the back
+ * projection saves in six iterations).  Either way the sums are a fixed
+ * function of the matrix, the sinograms and the entry point, the same from
+ * run to run. */
 typedef struct {
     int bk_mode;        /* MLEM_BK_CSC, MLEM_BK_ATOMIC, MLEM_BK_FUSED or MLEM_BK_REGION */
     int group;          /* lanes per row/column: 4, 8, 16 or 32 */

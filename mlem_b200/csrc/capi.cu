@@ -223,6 +223,65 @@ int ensure_region(mlem_ctx* c, int frame_tile) {
     return MLEM_OK;
 }
 
+size_t keep_words(const mlem_ctx* c) { return ((size_t)c->R + 31) / 32 + 1; }
+
+void free_csc_act(mlem_ctx* c) {
+    if (c->csc_act) { dev_free(c->csc_act); c->device_bytes -= (c->Z + 2) * 8; }
+    if (c->csc_act_len) { dev_free(c->csc_act_len); c->device_bytes -= (size_t)std::max<uint32_t>(c->C, 1) * 4; }
+    if (c->pos_keep) { dev_free(c->pos_keep); c->device_bytes -= keep_words(c) * 4; }
+    c->csc_act = nullptr;
+    c->csc_act_len = nullptr;
+    c->pos_keep = nullptr;
+    c->csc_act_ready = false;
+}
+
+void free_csc_vis(mlem_ctx* c) {
+    free_csc_act(c);
+    if (c->celems_vis) { dev_free(c->celems_vis); c->device_bytes -= (c->Z + 2) * 8; }
+    if (c->row_pos) { dev_free(c->row_pos); c->device_bytes -= (size_t)std::max<uint32_t>(c->R, 1) * 4; }
+    c->celems_vis = nullptr;
+    c->row_pos = nullptr;
+}
+
+bool csc_by_visit(const mlem_ctx* c, const mlem_tuning& t);
+
+// The CSC in visiting order cut to the rays with counts, for the CSC method's
+// back projection under tuning t (its other entries meet calcCorrel 0 in
+// every frame), from the current list of rows with counts.  The copy is made
+// only when the device keeps 2 GiB free beside it; without it the back
+// projection walks every entry of celems_vis.
+int build_csc_act(mlem_ctx* c, const mlem_tuning& t) {
+    c->csc_act_ready = false;
+    if (!csc_by_visit(c, t) || !c->celems_vis || !c->row_pos || !c->act_ready || !c->sino ||
+        c->Bp == 0)
+        return MLEM_OK;
+    if (!c->csc_act) {
+        const size_t need = (c->Z + 2) * 8 + (size_t)std::max<uint32_t>(c->C, 1) * 4 +
+                            keep_words(c) * 4;
+        size_t free_b = 0, total_b = 0;
+        if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+            cudaGetLastError();
+            return MLEM_OK;
+        }
+        if (free_b < need + (2ull << 30)) return MLEM_OK;
+        int s = dev_alloc(c, &c->csc_act, c->Z + 2);
+        if (s == MLEM_OK) s = dev_alloc(c, &c->csc_act_len, std::max<uint32_t>(c->C, 1));
+        if (s == MLEM_OK) s = dev_alloc(c, &c->pos_keep, keep_words(c));
+        if (s != MLEM_OK) {  // no room: every entry stays in the walk
+            free_csc_act(c);
+            c->err.clear();
+            return MLEM_OK;
+        }
+        CK(c, cudaMemsetAsync(c->csc_act + c->Z, 0, 2 * sizeof(uint2), c->stream));
+    }
+    SparseView vis = csc_view(c);
+    vis.pairs = reinterpret_cast<const uint4*>(c->celems_vis);
+    CK(c, csc_active_build(csr_view(c), c->sino, c->Bp, vis, c->pos_keep, c->csc_act,
+                           c->csc_act_len, c->stream));
+    c->csc_act_ready = true;
+    return MLEM_OK;
+}
+
 // The CSC in visiting order (mlem_ctx::celems_vis), built once on first use:
 // the transpose keyed by every row's visiting position.  Deterministic like
 // the CSC: a column's entries are summed in ascending visiting position.
@@ -255,10 +314,7 @@ int ensure_csc_vis(mlem_ctx* c) {
     if (col_ptr) { dev_free(col_ptr); c->device_bytes -= ((size_t)c->C + 1) * 8; }
     if (scratch) { dev_free(scratch); c->device_bytes -= sb; }
     if (s != MLEM_OK) {
-        if (c->celems_vis) { dev_free(c->celems_vis); c->device_bytes -= (c->Z + 2) * 8; }
-        if (c->row_pos) { dev_free(c->row_pos); c->device_bytes -= (size_t)std::max<uint32_t>(c->R, 1) * 4; }
-        c->celems_vis = nullptr;
-        c->row_pos = nullptr;
+        free_csc_vis(c);
         return s;
     }
     c->graph_dirty = true;
@@ -523,9 +579,12 @@ int download_images(mlem_ctx* c, float* host) {
 // are zero in every frame (active_rows_build), rebuilt whenever the
 // sinograms change.  Contexts without a row order and the bit-exact mode
 // keep every row; so does a context with no room for the list.  read_back:
-// wait for the list and record its size (mlem_info.rows_with_counts).
-int build_active_list(mlem_ctx* c, bool read_back) {
+// wait for the list and record its size (mlem_info.rows_with_counts).  cut:
+// also refill the CSC method's copy cut to the rays with counts (made where
+// several iterations follow the sinograms; dropped otherwise).
+int build_active_list(mlem_ctx* c, bool read_back, bool cut) {
     c->act_ready = false;
+    c->csc_act_ready = false;
     // the mirrored kernels walk stored rows, whose counts are the mirrored rows'
     if (!c->row_order || (c->flags & MLEM_FLAG_EXACT) || c->mirrored || c->R == 0 ||
         c->R > 0x7fffffffu)
@@ -557,7 +616,7 @@ int build_active_list(mlem_ctx* c, bool read_back) {
         c->act_nnz = z;
     }
     c->act_ready = true;
-    return MLEM_OK;
+    return cut ? build_csc_act(c, c->tuning) : MLEM_OK;
 }
 
 // The subsets' sorted lists without their rows without counts (ordered
@@ -582,11 +641,12 @@ int build_subset_lists(mlem_ctx* c) {
 
 // A captured iteration holds the list or the full visiting order: capture
 // again when that changes (not when the list is only rebuilt in place).
-int build_active(mlem_ctx* c, bool read_back) {
-    const bool was = c->act_ready, sub_was = c->sub_act_ready;
-    int s = build_active_list(c, read_back);
+int build_active(mlem_ctx* c, bool read_back, bool cut) {
+    const bool was = c->act_ready, sub_was = c->sub_act_ready, csc_was = c->csc_act_ready;
+    int s = build_active_list(c, read_back, cut);
     if (s == MLEM_OK) s = build_subset_lists(c);
-    if (c->act_ready != was || c->sub_act_ready != sub_was) c->graph_dirty = true;
+    if (c->act_ready != was || c->sub_act_ready != sub_was || c->csc_act_ready != csc_was)
+        c->graph_dirty = true;
     return s;
 }
 
@@ -706,6 +766,10 @@ int enqueue_iteration(mlem_ctx* c, const mlem_tuning& t, bool stats,
                         fw.n_dev = c->act_n;
                         fw.out_pos = c->row_pos;
                         CK(c, cudaMemsetAsync(c->correl, 0, (size_t)c->R * Bp * 4, st));
+                        if (c->csc_act_ready) {  // and only the entries of those rows
+                            bk.pairs = reinterpret_cast<const uint4*>(c->csc_act);
+                            bk.len = c->csc_act_len;
+                        }
                     }
                 }
                 for (uint32_t f0 = 0; f0 < Bp; f0 += T)
@@ -823,7 +887,10 @@ void phase_bytes_for(const mlem_ctx* c, int bk_mode, int frame_tile, double* byt
     const int mode = exact ? MLEM_BK_CSC : bk_mode;
     const double tiles = exact ? 1.0 : (double)(c->Bp / (uint32_t)frame_tile);
     const double csr_pass = 8.0 * (R + 1) + 8.0 * Z;
-    const double csc_pass = 8.0 * (C + 1) + 8.0 * (double)c->Z;  // every column, every element
+    // every column; every element, or those of the rows with counts (csc_act)
+    const double csc_pass = act && csc_act && c->csc_act_ready
+                                ? 8.0 * (C + 1) + 4.0 * C + 8.0 * (double)c->act_nnz
+                                : 8.0 * (C + 1) + 8.0 * (double)c->Z;
     for (int p = 0; p < MLEM_N_PHASES; ++p) { bytes[p] = 0.0; launches[p] = 0; }
     const int nt = (int)tiles;
     if (mode == MLEM_BK_REGION) {
@@ -1312,7 +1379,8 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->sub_sorted_ranges, (void*)c->mirror_lut, (void*)c->mirror_vox,
                     (void*)c->f_mirror_d, (void*)c->act_order, (void*)c->act_ranges,
                     (void*)c->act_tmp, (void*)c->act_n, (void*)c->act_z,
-                    (void*)c->celems_vis, (void*)c->row_pos})
+                    (void*)c->celems_vis, (void*)c->row_pos, (void*)c->csc_act,
+                    (void*)c->csc_act_len, (void*)c->pos_keep})
         dev_free(p);
     if (c->act_host) cudaFreeHost(c->act_host);
     for (cudaStream_t q : {c->up_stream, c->down_stream})
@@ -1521,7 +1589,7 @@ int mlem_set_sinograms(mlem_ctx* c, const int32_t* sino, uint32_t B) {
         c->sumin[b] = s;
     }
     TRY(upload_frames<int32_t>(c, sino, c->sino, c->R));
-    TRY(build_active(c, true));
+    TRY(build_active(c, true, true));
     ++c->sino_gen;
     CK(c, cudaStreamSynchronize(c->stream));
     c->images_ready = false;
@@ -1601,7 +1669,7 @@ int mlem_step_host(mlem_ctx* c, const int32_t* sino, float* images, uint32_t B) 
     TRY(set_device(c));
     if (c->B != B) TRY(alloc_frames(c, B));
     TRY(upload_frames<int32_t>(c, sino, c->sino, c->R));
-    TRY(build_active(c, false));
+    TRY(build_active(c, false, false));
     ++c->sino_gen;
     // the list's row and element counts for mlem_get_info: copied with the
     // step, read after its final synchronisation
@@ -1680,7 +1748,7 @@ static int stream_steps(mlem_ctx* c, const int32_t* const* sinos, float* const* 
         else
             CK(c, interleave_i32(c->sstage[cur], c->sino, c->R, B, Bp, c->stream));
         CK(c, cudaEventRecord(c->ev_sfree[cur], c->stream));
-        TRY(build_active(c, false));
+        TRY(build_active(c, false, false));
         ++c->sino_gen;
         if (c->graph_dirty || !c->graph || c->graph_iters != 1) {
             TRY(ensure_history(c, 1));
@@ -1837,6 +1905,10 @@ int mlem_set_tuning(mlem_ctx* c, const mlem_tuning* t) {
     if (csc_by_visit(c, n)) {
         TRY(set_device(c));
         TRY(ensure_csc_vis(c));
+        if (!c->csc_act_ready) {
+            TRY(build_csc_act(c, n));
+            CK(c, cudaStreamSynchronize(c->stream));
+        }
     }
     c->tuning = n;
     c->graph_dirty = true;
@@ -1911,8 +1983,10 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
                                      : visit == MLEM_VISIT_SORTED_STAGED ? (bps == 8 ? 3 : bps)
                                                                          : bps;
                     mlem_tuning t{mode, group, tile, ctas, visit, 0.0};
+                    // the cut copy of the CSC in visiting order, as the method runs
+                    int s = c->csc_act_ready ? MLEM_OK : build_csc_act(c, t);
                     // warm-up once, then time two iterations
-                    int s = enqueue_iteration(c, t, false);
+                    if (s == MLEM_OK) s = enqueue_iteration(c, t, false);
                     if (s != MLEM_OK) { c->tuning = orig; return s; }
                     CK(c, cudaEventRecord(e0, c->stream));
                     for (int i = 0; i < 2; ++i) TRY(enqueue_iteration(c, t, false));
@@ -1933,13 +2007,8 @@ int mlem_autotune(mlem_ctx* c, int deterministic_only, mlem_tuning* best_out) {
     cudaFree(saved);
     c->device_bytes -= xb;
     if (best.bk_mode == MLEM_BK_REGION) TRY(ensure_region(c, best.frame_tile));
-    if (!csc_by_visit(c, best) && c->celems_vis) {  // tried, not chosen: give the memory back
-        dev_free(c->celems_vis);
-        dev_free(c->row_pos);
-        c->device_bytes -= (c->Z + 2) * 8 + (size_t)std::max<uint32_t>(c->R, 1) * 4;
-        c->celems_vis = nullptr;
-        c->row_pos = nullptr;
-    }
+    if (!csc_by_visit(c, best) && c->celems_vis)  // tried, not chosen: give the memory back
+        free_csc_vis(c);
     c->tuning = best;
     c->graph_dirty = true;
     if (best_out) *best_out = best;

@@ -34,6 +34,15 @@ struct mlem_ctx {
     // column's gathers fall on neighbouring, nearly coincident rays.
     uint2* celems_vis = nullptr;
     uint32_t* row_pos = nullptr;  // visiting position of every row
+    // celems_vis cut to the rays with counts (csc_active_build), refilled by
+    // mlem_set_sinograms: each column's kept entries at its offset,
+    // csc_act_len[col] of them; pos_keep: one bit per visiting position.  The
+    // CSC method's back projection walks it while csc_act_ready (the
+    // one-iteration host steps clear that); made only where it fits.
+    uint2* csc_act = nullptr;
+    uint32_t* csc_act_len = nullptr;
+    uint32_t* pos_keep = nullptr;
+    bool csc_act_ready = false;
     uint32_t max_col_len = 0, max_row_len = 0;
     float* norm = nullptr;       // column sums, device voxel order
     float* norm_nat = nullptr;   // column sums, natural voxel order

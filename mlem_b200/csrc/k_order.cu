@@ -96,7 +96,77 @@ __global__ void k_active_gather(const uint32_t* __restrict__ order,
     if ((threadIdx.x & 31) == 0 && mine) atomicAdd(z, mine);
 }
 
+// Bit k & 31 of keep[k >> 5]: whether the ray at visiting position k has a
+// count in some frame (one ballot per 32 positions; whole warps, so the
+// grid stride stays a multiple of 32).
+__global__ void k_pos_keep(HasCount has, uint32_t n, uint32_t* __restrict__ keep) {
+    const uint64_t n32 = ((uint64_t)n + 31) & ~31ull;
+    for (uint64_t k = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; k < n32;
+         k += (uint64_t)gridDim.x * blockDim.x) {
+        const bool f = k < n && has((uint32_t)k);
+        const unsigned w = __ballot_sync(MLEM_FULL_MASK, f);
+        if ((threadIdx.x & 31) == 0) keep[k >> 5] = w;
+    }
+}
+
+// A warp per column: the column's entries whose rays are kept, in their order,
+// from the start of the column's span; len[col] = their number.  Each step
+// takes kSteps batches of 32 entries, their loads and flag gathers in flight
+// together.
+__global__ void __launch_bounds__(256) k_csc_active(const uint64_t* __restrict__ ptr,
+                                                    const uint2* __restrict__ src, uint32_t C,
+                                                    const uint32_t* __restrict__ keep,
+                                                    uint2* __restrict__ dst,
+                                                    uint32_t* __restrict__ len) {
+    constexpr int kSteps = 4;
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const uint64_t warp = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    const uint64_t ps = l2_evict_first();
+    for (uint64_t col = warp; col < C; col += nwarps) {
+        const uint64_t b = ptr[col], e = ptr[col + 1];
+        uint32_t n = 0;
+        for (uint64_t k0 = b; k0 < e; k0 += 32 * kSteps) {
+            uint2 q[kSteps];
+            bool f[kSteps];
+#pragma unroll
+            for (int u = 0; u < kSteps; ++u) {
+                const uint64_t k = k0 + 32 * u + lane;
+                q[u] = k < e ? ld_stream2(src + k, ps) : make_uint2(0u, 0u);
+            }
+#pragma unroll
+            for (int u = 0; u < kSteps; ++u)
+                f[u] = k0 + 32 * u + lane < e && ((keep[q[u].x >> 5] >> (q[u].x & 31)) & 1u);
+#pragma unroll
+            for (int u = 0; u < kSteps; ++u) {
+                const unsigned m = __ballot_sync(MLEM_FULL_MASK, f[u]);
+                if (f[u]) dst[b + n + __popc(m & below)] = q[u];
+                n += __popc(m);
+            }
+        }
+        if (lane == 0) len[col] = n;
+    }
+}
+
 }  // namespace
+
+cudaError_t csc_active_build(const SparseView& csr, const int32_t* sino, uint32_t Bp,
+                             const SparseView& csc_vis, uint32_t* keep, uint2* dst, uint32_t* len,
+                             cudaStream_t st) {
+    if (!csr.order || Bp == 0) return cudaErrorInvalidValue;
+    if (csr.n) {  // blocks of 256 threads: whole warps for the ballot
+        const int grid = (int)std::min<uint64_t>((csr.n + 255) / 256, 148ull * 16);
+        k_pos_keep<<<grid, 256, 0, st>>>(HasCount{csr.order, sino, Bp}, csr.n, keep);
+        const cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    if (csc_vis.n == 0) return cudaSuccess;
+    const int grid = (int)std::min<uint64_t>(((uint64_t)csc_vis.n + 7) / 8, 148ull * 16);
+    k_csc_active<<<grid, 256, 0, st>>>(csc_vis.ptr, reinterpret_cast<const uint2*>(csc_vis.pairs),
+                                       csc_vis.n, keep, dst, len);
+    return cudaGetLastError();
+}
 
 size_t active_rows_tmp_bytes(uint32_t n) {
     size_t a = 0;

@@ -115,7 +115,7 @@ __global__ void __launch_bounds__(256) k_bkproj_csc(SparseView csc, const float*
         const uint64_t col = base + lw / G;
         const bool active = col < csc.n;
         uint64_t b = 0, e = 0;
-        if (active) { b = csc.ptr[col]; e = csc.ptr[col + 1]; }
+        if (active) span_of(csc, col, b, e);
         float acc[VW];
         row_dot<G, BT, false>(el, b, e, lane, c, B, f0 + sub * VW, acc, ps, ph);
         slot_allreduce<G, BT>(acc);
@@ -155,7 +155,8 @@ __global__ void __launch_bounds__(256) k_bkproj_csc_pipe(SparseView csc, const f
     const uint64_t n = csc.n;
     uint64_t col = warp;
     if (col >= n) return;
-    uint64_t k0 = csc.ptr[col], e = csc.ptr[col + 1];
+    uint64_t k0 = 0, e = 0;
+    span_of(csc, col, k0, e);
     uint2 q[kBatch];
 #pragma unroll
     for (int t = 0; t < kBatch; ++t) {
@@ -169,10 +170,7 @@ __global__ void __launch_bounds__(256) k_bkproj_csc_pipe(SparseView csc, const f
         if (nk0 >= e) {
             ncol = col + nwarps;
             nk0 = ne = 0;
-            if (ncol < n) {
-                nk0 = csc.ptr[ncol];
-                ne = csc.ptr[ncol + 1];
-            }
+            if (ncol < n) span_of(csc, ncol, nk0, ne);
         }
         uint2 qn[kBatch];
 #pragma unroll

@@ -43,7 +43,17 @@ struct SparseView {
     // k_fwproj only, with out_by_visit and a device-built list (n_dev): the
     // position of row r in the full visiting order is out_pos[r].
     const uint32_t* out_pos = nullptr;
+    // CSC kernels (k_bkproj_csc, k_bkproj_csc_pipe) only, when non-null:
+    // column col holds len[col] entries from ptr[col] (the rest of its span
+    // is unused), the layout csc_active_build writes.
+    const uint32_t* len = nullptr;
 };
+
+// Entry range of column (or row) i: [ptr[i], ptr[i + 1]), or len[i] entries from ptr[i].
+__device__ __forceinline__ void span_of(const SparseView& s, uint64_t i, uint64_t& b, uint64_t& e) {
+    b = s.ptr[i];
+    e = s.len ? b + s.len[i] : s.ptr[i + 1];
+}
 
 // Row index of visiting position v.
 __host__ __device__ inline uint64_t row_at(const SparseView& s, uint64_t v) {
@@ -258,6 +268,17 @@ cudaError_t active_rows_build(const SparseView& csr, const int32_t* sino, uint32
                               void* tmp, size_t tmp_bytes, uint32_t* act_order,
                               ulonglong2* act_ranges, uint32_t* act_n, unsigned long long* act_z,
                               cudaStream_t st);
+
+// The CSC in visiting order (csc_vis: ptr[C+1], entries {visiting position,
+// value}) cut to the entries whose rays have a count in some frame: bit k & 31
+// of keep[k >> 5] ((csr.n + 31) / 32 words) flags visiting position k
+// (csr.order, as active_rows_build decides), dst (csc_vis.nnz capacity, same
+// offsets) gets each column's kept
+// entries in their order from ptr[col], len[col] their number.  The other
+// entries meet calcCorrel 0 in every frame and add +0 to the column's sum.
+cudaError_t csc_active_build(const SparseView& csr, const int32_t* sino, uint32_t Bp,
+                             const SparseView& csc_vis, uint32_t* keep, uint2* dst, uint32_t* len,
+                             cudaStream_t st);
 
 // ---- matrix validation: every column < C and offsets non-decreasing ------
 cudaError_t validate_csr(const SparseView& csr, uint32_t C, unsigned int* bad_flag,

@@ -180,6 +180,51 @@ def test_csc_in_visiting_order_skips_rows_without_counts(golden, tile):
             assert ob.rel_l2(x[b], want) <= TOL_MLEM, b
 
 
+@pytest.mark.parametrize("group,tile", [(32, 1), (16, 1), (32, 2)])
+def test_csc_cut_copy_is_refilled_with_each_sinogram(golden, group, tile):
+    """With sinograms set, the CSC method's back projection walks a copy of
+    the CSC in visiting order cut to the rays with counts, refilled from the
+    full CSC with every set of sinograms: after sinograms with other rows at
+    zero counts, the images equal those of a fresh context, to the bit."""
+    m, sino, _, _, _ = golden.case("plain_small_it10")
+    rng = np.random.default_rng(5 + group + tile)
+    B = tile
+    first = np.stack([rng.permutation(sino) for _ in range(B)]).astype(np.int32)
+    first[:, rng.random(m.n_rows) < 0.4] = 0
+    second = np.stack([rng.permutation(sino) for _ in range(B)]).astype(np.int32)
+    second[:, rng.random(m.n_rows) < 0.3] = 0
+    second[0, ::7] = 0  # and some rows empty in one frame only
+    tuning = dict(bk_mode=api.BK_CSC, group=group, frame_tile=tile, blocks_per_sm=4,
+                  visit=api.VISIT_SORTED)
+
+    def run(ctx, s):
+        ctx.set_sinograms(s)
+        ctx.init_images()
+        ctx.iterate(5)
+        return ctx.get_images()
+
+    with api.Context.from_matrix(m) as ctx:
+        ctx.set_sinograms(first)
+        ctx._refresh()
+        before = ctx.info.device_bytes
+        ctx.set_tuning(**tuning)
+        ctx._refresh()
+        # the CSC in visiting order and its cut copy (entries, lengths, flags)
+        Z, R, C = m.nnz, m.n_rows, m.n_cols
+        assert ctx.info.device_bytes - before == 2 * (Z + 2) * 8 + 4 * R + 4 * C + \
+            4 * ((R + 31) // 32 + 1)
+        run(ctx, first)
+        again = run(ctx, second)
+    with api.Context.from_matrix(m) as ctx:
+        ctx.set_sinograms(second)
+        ctx.set_tuning(**tuning)
+        fresh = run(ctx, second)
+    assert again.tobytes() == fresh.tobytes()
+    for b in range(B):
+        want, _ = ob.mlem(m, second[b], 5)
+        assert ob.rel_l2(fresh[b], want) <= TOL_MLEM, b
+
+
 @pytest.mark.parametrize("group,tile", [(32, 1), (16, 4), (8, 16), (32, 2)])
 def test_csc_in_visiting_order_with_frames(golden, group, tile):
     m, sino, iters, gold, _ = golden.case("tiny_it10")
@@ -247,15 +292,20 @@ def test_step_host_matches_iterate(ctxs):
     assert x.tobytes() == ctx.get_images().tobytes()
 
 
-def test_stream_host_matches_step_host(ctxs):
+@pytest.mark.parametrize("visit", [api.VISIT_FILE, api.VISIT_SORTED])
+def test_stream_host_matches_step_host(ctxs, visit):
     """mlem_stream_host with one sinogram per iteration equals the same
     iterations through mlem_step_host, bit for bit with the deterministic CSC
-    method (the image stays on the device between the streamed iterations)."""
+    method (the image stays on the device between the streamed iterations).
+    With the sorted visit both walk the whole CSC in visiting order: its copy
+    cut to the rays with counts is made by mlem_set_sinograms only."""
     ctx, m, sino, iters, gold = ctxs["tiny_it10"]
     rng = np.random.default_rng(31)
     sinos = [rng.permutation(sino).astype(np.int32) for _ in range(6)]
+    for s in sinos[::2]:
+        s[rng.random(m.n_rows) < 0.3] = 0
     ctx.set_sinograms(sino)
-    ctx.set_tuning(bk_mode=api.BK_CSC, group=32, frame_tile=1, blocks_per_sm=8)
+    ctx.set_tuning(bk_mode=api.BK_CSC, group=32, frame_tile=1, blocks_per_sm=8, visit=visit)
     init = ctx.init_images()
     x = np.full((1, m.n_cols), init[0], np.float32)
     want = []
@@ -273,6 +323,16 @@ def test_stream_host_matches_step_host(ctxs):
     assert ctx.get_images().tobytes() == want[-1].tobytes()
     ctx._refresh()
     assert ctx.info.rows_with_counts == int((sinos[-1] != 0).sum())
+    if visit == api.VISIT_SORTED:
+        # the same iterations after mlem_set_sinograms (the cut copy): other
+        # rounding, the same images within the tolerance
+        x = want[0]
+        for k, s in enumerate(sinos[1:], 1):
+            ctx.set_sinograms(s)
+            ctx.set_images(x)
+            ctx.iterate(1)
+            x = ctx.get_images()
+            assert ob.rel_l2(x[0], want[k][0]) <= TOL_PROJ, k
 
 
 @pytest.mark.parametrize("flags", [0, api.FLAG_NATURAL_LAYOUT])
