@@ -258,9 +258,14 @@ int mlem_step_host(mlem_ctx* ctx, const int32_t* sino, float* images_inout, uint
  * from iteration k's, which stay on the device.  The upload of sinos[k + 1]
  * runs on a copy stream of its own during iteration k and the download of
  * images[k] on another during iteration k + 1; with page-locked host buffers
- * (cudaHostAlloc, cudaHostRegister) they overlap the kernels.  Every copy has
- * ended when the call returns.  Afterwards the context holds sinos[n - 1] as
- * its sinograms (the initImage sums of mlem_set_sinograms are kept). */
+ * (cudaHostAlloc, cudaHostRegister) they overlap the kernels.  Where the
+ * iteration walks the list of rows with counts (a sorted row order, no
+ * ordered subsets, not MLEM_FLAG_EXACT or MLEM_FLAG_MIRROR_KERNELS), the copy
+ * stream also rebuilds that list for sinos[k + 1] during iteration k, in a
+ * second set of sinogram and list buffers (R x Bp x 4 + R x 20 bytes, made on
+ * first use) with a captured iteration of its own.  Every copy has ended when
+ * the call returns.  Afterwards the context holds sinos[n - 1] as its
+ * sinograms (the initImage sums of mlem_set_sinograms are kept). */
 int mlem_stream_host(mlem_ctx* ctx, const int32_t* const* sinos, float* const* images,
                      uint32_t n);
 

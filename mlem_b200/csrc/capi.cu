@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <utility>
 #include <chrono>
 #include <cstdarg>
 #include <cstdio>
@@ -510,8 +511,12 @@ int ensure_stage(mlem_ctx* c, size_t bytes) {
 
 void free_frames(mlem_ctx* c) {
     for (void* p : {(void*)c->sino, (void*)c->x, (void*)c->correl, (void*)c->update,
-                    (void*)c->stats_scratch, (void*)c->inits_dev, (void*)c->f_long})
+                    (void*)c->stats_scratch, (void*)c->inits_dev, (void*)c->f_long,
+                    (void*)c->sino_alt})
         dev_free(p);
+    if (c->graph_alt) cudaGraphExecDestroy(c->graph_alt);
+    c->graph_alt = nullptr;
+    c->sino_alt = nullptr;
     c->sino = nullptr; c->x = nullptr; c->correl = nullptr; c->update = nullptr;
     c->stats_scratch = nullptr; c->inits_dev = nullptr; c->f_long = nullptr;
     c->B = c->Bp = 0;
@@ -986,15 +991,18 @@ int ensure_history(mlem_ctx* c, int n) {
 
 namespace {
 
+// Drops the iteration graph and the streaming steps' second one (any new
+// capture of the first invalidates the second).
 void drop_graph(mlem_ctx* c) {
     if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->graph_alt) cudaGraphExecDestroy(c->graph_alt);
     c->graph = nullptr;
+    c->graph_alt = nullptr;
     c->graph_iters = 0;
 }
 
-// Capture `n` iterations (slot reset + n x (iteration + statistics)) as one graph.
-int capture(mlem_ctx* c, int n) {
-    drop_graph(c);
+// Capture `n` iterations (slot reset + n x (iteration + statistics)) into *out.
+int capture_into(mlem_ctx* c, int n, cudaGraphExec_t* out) {
     CK(c, cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     int s = MLEM_OK;
     cudaError_t e = cudaMemsetAsync(c->stats_slot, 0, sizeof(unsigned int), c->stream);
@@ -1004,9 +1012,18 @@ int capture(mlem_ctx* c, int n) {
     cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
     if (s != MLEM_OK) { if (g) cudaGraphDestroy(g); return s; }
     if (e2 != cudaSuccess) return fail(c, MLEM_ERR_CUDA, "end capture: %s", cudaGetErrorString(e2));
-    e2 = cudaGraphInstantiate(&c->graph, g, 0);
+    e2 = cudaGraphInstantiate(out, g, 0);
     cudaGraphDestroy(g);
-    if (e2 != cudaSuccess) return fail(c, MLEM_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e2));
+    if (e2 != cudaSuccess) {
+        *out = nullptr;
+        return fail(c, MLEM_ERR_CUDA, "instantiate: %s", cudaGetErrorString(e2));
+    }
+    return MLEM_OK;
+}
+
+int capture(mlem_ctx* c, int n) {
+    drop_graph(c);
+    TRY(capture_into(c, n, &c->graph));
     c->graph_iters = n;
     c->graph_dirty = false;
     return MLEM_OK;
@@ -1380,7 +1397,8 @@ void mlem_destroy(mlem_ctx* c) {
                     (void*)c->f_mirror_d, (void*)c->act_order, (void*)c->act_ranges,
                     (void*)c->act_tmp, (void*)c->act_n, (void*)c->act_z,
                     (void*)c->celems_vis, (void*)c->row_pos, (void*)c->csc_act,
-                    (void*)c->csc_act_len, (void*)c->pos_keep})
+                    (void*)c->csc_act_len, (void*)c->pos_keep, (void*)c->act_order_alt,
+                    (void*)c->act_ranges_alt, (void*)c->act_n_alt, (void*)c->act_z_alt})
         dev_free(p);
     if (c->act_host) cudaFreeHost(c->act_host);
     for (cudaStream_t q : {c->up_stream, c->down_stream})
@@ -1772,6 +1790,121 @@ static int stream_steps(mlem_ctx* c, const int32_t* const* sinos, float* const* 
     return MLEM_OK;
 }
 
+// The per-sinogram buffers the iteration graph reads: the sinogram and the
+// list of rows with counts.
+struct SinoSet {
+    int32_t* sino;
+    uint32_t* order;
+    ulonglong2* ranges;
+    uint32_t* n;
+    unsigned long long* z;
+};
+
+static void swap_sets(mlem_ctx* c) {
+    std::swap(c->sino, c->sino_alt);
+    std::swap(c->act_order, c->act_order_alt);
+    std::swap(c->act_ranges, c->act_ranges_alt);
+    std::swap(c->act_n, c->act_n_alt);
+    std::swap(c->act_z, c->act_z_alt);
+}
+
+// The overlapped steps run where the iteration walks the list of rows with
+// counts (built for the current sinograms) and no subsets.
+static bool stream_overlap_ok(const mlem_ctx* c) {
+    return c->act_ready && c->act_tmp && c->n_subsets == 1 && !c->mirrored &&
+           !(c->flags & MLEM_FLAG_EXACT);
+}
+
+static int ensure_stream_alt(mlem_ctx* c) {
+    if (!c->sino_alt) {
+        TRY(dev_alloc(c, &c->sino_alt, std::max<size_t>((size_t)c->R * c->Bp, 1)));
+        CK(c, cudaMemsetAsync(c->sino_alt, 0, (size_t)c->R * c->Bp * 4, c->stream));  // pad frames
+        if (c->graph_alt) { cudaGraphExecDestroy(c->graph_alt); c->graph_alt = nullptr; }
+    }
+    if (!c->act_order_alt) {
+        TRY(dev_alloc(c, &c->act_order_alt, std::max<uint32_t>(c->R, 1)));
+        TRY(dev_alloc(c, &c->act_ranges_alt, std::max<uint32_t>(c->R, 1)));
+        TRY(dev_alloc(c, &c->act_n_alt, 1));
+        TRY(dev_alloc(c, &c->act_z_alt, 1));
+    }
+    return MLEM_OK;
+}
+
+// mlem_stream_host's steps with two sets of per-sinogram buffers, each with
+// its own one-iteration graph: the upload of step k+1's sinograms and the
+// rebuild of their list of rows with counts run on the copy stream, into the
+// other set, while step k iterates; the compute stream only waits for its
+// set, launches its graph and copies the images out.
+static int stream_steps_overlap(mlem_ctx* c, const int32_t* const* sinos, float* const* images,
+                                uint32_t n) {
+    const uint32_t B = c->B, Bp = c->Bp;
+    const size_t sbytes = (size_t)c->R * B * 4, ibytes = (size_t)c->C * B * 4;
+    TRY(ensure_stream_alt(c));
+    if (c->csc_act_ready) {  // one iteration per sinogram: the whole CSC in visiting order
+        c->csc_act_ready = false;
+        c->graph_dirty = true;
+    }
+    if (c->graph_dirty || !c->graph || c->graph_iters != 1) {
+        TRY(ensure_history(c, 1));
+        TRY(capture(c, 1));
+    }
+    if (!c->graph_alt) {
+        swap_sets(c);
+        const int s = capture_into(c, 1, &c->graph_alt);
+        swap_sets(c);
+        TRY(s);
+    }
+    const SinoSet set[2] = {{c->sino, c->act_order, c->act_ranges, c->act_n, c->act_z},
+                            {c->sino_alt, c->act_order_alt, c->act_ranges_alt, c->act_n_alt,
+                             c->act_z_alt}};
+    const cudaGraphExec_t graph[2] = {c->graph, c->graph_alt};
+    // set q takes step j's sinograms once the step two before has iterated on it
+    auto upload = [&](uint32_t j, int q) -> int {
+        CK(c, cudaStreamWaitEvent(c->up_stream, c->ev_sfree[q], 0));
+        if (Bp == 1) {
+            CK(c, cudaMemcpyAsync(set[q].sino, sinos[j], sbytes, cudaMemcpyHostToDevice,
+                                  c->up_stream));
+        } else {
+            CK(c, cudaMemcpyAsync(c->sstage[q], sinos[j], sbytes, cudaMemcpyHostToDevice,
+                                  c->up_stream));
+            CK(c, interleave_i32(c->sstage[q], set[q].sino, c->R, B, Bp, c->up_stream));
+        }
+        CK(c, active_rows_build(csr_view(c), set[q].sino, Bp, c->act_tmp, c->act_tmp_bytes,
+                                set[q].order, set[q].ranges, set[q].n, set[q].z, c->up_stream));
+        CK(c, cudaEventRecord(c->ev_up[q], c->up_stream));
+        return MLEM_OK;
+    };
+    // both sets are free once the work already on the compute stream is done
+    for (int q = 0; q < 2; ++q) CK(c, cudaEventRecord(c->ev_sfree[q], c->stream));
+    TRY(upload(0, 0));
+    for (uint32_t k = 0; k < n; ++k) {
+        const int p = (int)(k & 1);
+        if (k + 1 < n) TRY(upload(k + 1, p ^ 1));
+        CK(c, cudaStreamWaitEvent(c->stream, c->ev_up[p], 0));
+        CK(c, cudaGraphLaunch(graph[p], c->stream));
+        CK(c, cudaEventRecord(c->ev_sfree[p], c->stream));
+        ++c->sino_gen;
+        if (images && images[k]) {  // this iteration's images, once the buffer's last download is done
+            CK(c, cudaStreamWaitEvent(c->stream, c->ev_dfree[p], 0));
+            if (Bp == 1 && !c->bricked)
+                CK(c, cudaMemcpyAsync(c->istage[p], c->x, ibytes, cudaMemcpyDeviceToDevice, c->stream));
+            else
+                CK(c, deinterleave_f32(c->x, c->istage[p], c->C, B, Bp, c->bricked ? c->perm : nullptr,
+                                       c->stream));
+            CK(c, cudaEventRecord(c->ev_img[p], c->stream));
+            CK(c, cudaStreamWaitEvent(c->down_stream, c->ev_img[p], 0));
+            CK(c, cudaMemcpyAsync(images[k], c->istage[p], ibytes, cudaMemcpyDeviceToHost,
+                                  c->down_stream));
+            CK(c, cudaEventRecord(c->ev_dfree[p], c->down_stream));
+        }
+    }
+    if ((n - 1) & 1) {  // the last sinograms are in the second set: it becomes the first
+        swap_sets(c);
+        std::swap(c->graph, c->graph_alt);
+    }
+    return MLEM_OK;
+}
+
 int mlem_stream_host(mlem_ctx* c, const int32_t* const* sinos, float* const* images, uint32_t n) {
     if (!c) return fail(nullptr, MLEM_ERR_INVALID, "null context");
     if (n == 0) return MLEM_OK;
@@ -1789,7 +1922,8 @@ int mlem_stream_host(mlem_ctx* c, const int32_t* const* sinos, float* const* ima
         cudaGetLastError();
         c->act_host = nullptr;
     }
-    int s = stream_steps(c, sinos, images, n);
+    int s = stream_overlap_ok(c) ? stream_steps_overlap(c, sinos, images, n)
+                                 : stream_steps(c, sinos, images, n);
     const bool counts = s == MLEM_OK && c->act_ready && c->act_host;
     if (counts &&
         (cudaMemcpyAsync(c->act_host, c->act_n, 4, cudaMemcpyDeviceToHost, c->stream) != cudaSuccess ||

@@ -123,6 +123,16 @@ struct mlem_ctx {
     // mlem_stream_host: an upload and a download stream, double-buffered
     // staging of the sinograms and images, and the events between the streams
     cudaStream_t up_stream = nullptr, down_stream = nullptr;
+    // The second set of per-sinogram buffers of the overlapped streaming steps
+    // (mlem_stream_host with the list of rows with counts): sinogram and list,
+    // and the one-iteration graph captured over them.  The two sets trade
+    // places when a call ends on this one.
+    int32_t* sino_alt = nullptr;
+    uint32_t* act_order_alt = nullptr;
+    ulonglong2* act_ranges_alt = nullptr;
+    uint32_t* act_n_alt = nullptr;
+    unsigned long long* act_z_alt = nullptr;
+    cudaGraphExec_t graph_alt = nullptr;
     int32_t* sstage[2] = {nullptr, nullptr};
     float* istage[2] = {nullptr, nullptr};
     size_t sstage_n = 0, istage_n = 0;  // elements of each buffer

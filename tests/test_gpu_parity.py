@@ -335,6 +335,36 @@ def test_stream_host_matches_step_host(ctxs, visit):
             assert ob.rel_l2(x[0], want[k][0]) <= TOL_PROJ, k
 
 
+@pytest.mark.parametrize("n", [3, 4])
+@pytest.mark.parametrize("mode,visit", [(api.BK_CSC, api.VISIT_SORTED),
+                                        (api.BK_FUSED, api.VISIT_SORTED_CHUNKED)])
+def test_stream_host_leaves_the_last_sinograms(ctxs, n, mode, visit):
+    """mlem_stream_host uploads each step's sinograms and rebuilds their list
+    of rows with counts into one of two buffer sets while the step before
+    iterates; afterwards the context iterates on the last step's sinograms,
+    whichever set holds them (odd and even step counts)."""
+    ctx, m, sino, iters, gold = ctxs["tiny_it10"]
+    rng = np.random.default_rng(17 + n)
+    sinos = [rng.permutation(sino).astype(np.int32) for _ in range(n)]
+    for s in sinos:
+        s[rng.random(m.n_rows) < 0.3] = 0
+    ctx.set_sinograms(sino)
+    ctx.set_tuning(bk_mode=mode, group=32, frame_tile=1, blocks_per_sm=4, visit=visit)
+    init = ctx.init_images()
+    ctx.stream_host(sinos)
+    ctx.iterate(2)
+    got = ctx.get_images()
+    ctx._refresh()
+    assert ctx.info.rows_with_counts == int((sinos[-1] != 0).sum())
+    x = np.full((1, m.n_cols), init[0], np.float32)
+    for s in sinos + [sinos[-1]] * 2:
+        ctx.step_host(s, x)
+    if mode == api.BK_CSC:  # deterministic: the same sums in the same order
+        assert got.tobytes() == x.tobytes()
+    else:
+        assert ob.rel_l2(got[0], x[0]) <= TOL_PROJ
+
+
 @pytest.mark.parametrize("flags", [0, api.FLAG_NATURAL_LAYOUT])
 @pytest.mark.parametrize("frames", [1, 3])
 def test_stream_host_against_oracle(golden, flags, frames):
