@@ -559,6 +559,14 @@ def run_ours(a, rank, world, local_rank, parallelism):
         l2 = api.measure_l2_rates(torch.cuda.current_device())
         head["l2_rates"] = {k: round(v / 1e9, 1) for k, v in l2.items()}
         head["l2_rates"]["unit"] = "G/s"
+        # the dominant kernel against the L2's float-reduction rate: its reduction
+        # sector operations per launch (committed ncu capture, scaled to this
+        # workload) at the measured rate of random 4-byte reductions
+        red = committed_traffic().get(roofline["kernel"] + "_red_sectors")
+        if red and frames.sinograms.shape[0] == 1:
+            floor = red / l2["red_4B_per_s"] * 1e3
+            roofline["l2_reduction_floor_ms"] = round(floor, 4)
+            roofline["frac_of_l2_reduction_floor"] = round(floor / roofline["ms_per_launch"], 4)
 
         # --- batched: 16 sinograms in one pass over the matrix per iteration ---
         if fb is not None:
