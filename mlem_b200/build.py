@@ -105,7 +105,7 @@ def build_core(verbose=False, jobs=8):
     out = os.path.join(LIB, "libmlem_b200.so")
     if _newer(out, objs):
         _run([NVCC] + ARCH + ["-shared", "-o", out] + objs
-             + ["-cudart", "static", "-Xlinker", "-rpath,$ORIGIN", "-ccbin", CXX])
+             + ["-cudart", "static", "-lpthread", "-Xlinker", "-rpath,$ORIGIN", "-ccbin", CXX])
         if verbose:
             print("linked", out)
     return out

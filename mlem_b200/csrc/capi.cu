@@ -8,8 +8,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
-#include <utility>
+#include <atomic>
 #include <chrono>
+#include <mutex>
+#include <thread>
+#include <utility>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -1149,6 +1152,77 @@ const char* mlem_status_string(int s) {
     }
 }
 
+namespace {
+// Host-to-device copy of a large pageable array (a matrix's elements, often a
+// file mapping): host threads copy 16 MiB chunks into a ring of page-locked
+// buffers, two per thread, and each chunk goes out with its own
+// cudaMemcpyAsync as soon as it is filled, so the threads' page faults and
+// copies overlap one another and the copy engine.  Returns once the copies
+// have finished.  Small arrays, and hosts where page-locked memory cannot be
+// had, take one plain copy.
+cudaError_t upload_pageable(int device, cudaStream_t st, void* dst, const void* src, size_t bytes) {
+    constexpr size_t kChunk = size_t(16) << 20;
+    const int T = (int)std::min(8u, std::max(1u, std::thread::hardware_concurrency()));
+    auto plain = [&]() {
+        const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+        return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
+    };
+    if (bytes < 8 * kChunk || T < 2) return plain();
+    const int K = 2 * T;
+    unsigned char* ring = nullptr;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&ring), (size_t)K * kChunk, cudaHostAllocDefault) !=
+        cudaSuccess) {
+        cudaGetLastError();
+        return plain();
+    }
+    std::vector<cudaEvent_t> ev(K, nullptr);
+    cudaError_t e = cudaSuccess;
+    for (int b = 0; b < K && e == cudaSuccess; ++b)
+        e = cudaEventCreateWithFlags(&ev[b], cudaEventDisableTiming);
+    const size_t n = (bytes + kChunk - 1) / kChunk;
+    const unsigned char* from = static_cast<const unsigned char*>(src);
+    unsigned char* to = static_cast<unsigned char*>(dst);
+    std::mutex enqueue;
+    std::atomic<int> bad{0};  // the first failure's cudaError_t
+    // thread t takes chunks t, t + T, ...; its j-th chunk uses buffer t + (j & 1) T
+    auto worker = [&](int t) {
+        cudaError_t we = cudaSetDevice(device);
+        bool used[2] = {false, false};
+        for (size_t i = (size_t)t; we == cudaSuccess && i < n && !bad.load(); i += (size_t)T) {
+            const int slot = (int)((i / (size_t)T) & 1u), b = t + slot * T;
+            if (used[slot] && (we = cudaEventSynchronize(ev[b])) != cudaSuccess) break;
+            const size_t off = i * kChunk, len = std::min(kChunk, bytes - off);
+            std::memcpy(ring + (size_t)b * kChunk, from + off, len);
+            std::lock_guard<std::mutex> g(enqueue);
+            we = cudaMemcpyAsync(to + off, ring + (size_t)b * kChunk, len, cudaMemcpyHostToDevice, st);
+            if (we == cudaSuccess) we = cudaEventRecord(ev[b], st);
+            used[slot] = true;
+        }
+        if (we != cudaSuccess) {
+            int none = 0;
+            bad.compare_exchange_strong(none, (int)we);
+        }
+    };
+    if (e == cudaSuccess) {
+        std::vector<std::thread> pool;
+        int started = 0;
+        try {
+            for (; started < T; ++started) pool.emplace_back(worker, started);
+        } catch (...) {  // no more threads: the calling thread takes the rest
+        }
+        for (int t = started; t < T; ++t) worker(t);
+        for (std::thread& th : pool) th.join();
+        if (bad.load()) e = static_cast<cudaError_t>(bad.load());
+    }
+    const cudaError_t es = cudaStreamSynchronize(st);  // the ring is read until here
+    if (e == cudaSuccess) e = es;
+    for (cudaEvent_t x : ev)
+        if (x) cudaEventDestroy(x);
+    cudaFreeHost(ring);
+    return e;
+}
+}  // namespace
+
 int mlem_create(mlem_ctx** out, const uint64_t* row_end, const void* elems, uint32_t n_rows,
                 uint32_t n_cols, uint64_t nnz, uint32_t flags, int device) {
     return mlem_create_grid(out, row_end, elems, n_rows, n_cols, nnz, nullptr, flags, device);
@@ -1180,8 +1254,7 @@ int mlem_create_grid(mlem_ctx** out, const uint64_t* row_end, const void* elems,
     if (s == MLEM_OK && n_rows) {
         cudaError_t e = cudaMemcpyAsync(c->row_ptr + 1, row_end, (size_t)n_rows * 8,
                                         cudaMemcpyHostToDevice, c->stream);
-        if (e == cudaSuccess && nnz)
-            e = cudaMemcpyAsync(c->elems, elems, nnz * 8, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess && nnz) e = upload_pageable(c->device, c->stream, c->elems, elems, nnz * 8);
         if (e != cudaSuccess) s = fail(c, MLEM_ERR_CUDA, "upload: %s", cudaGetErrorString(e));
     }
     if (s == MLEM_OK) s = finish_create(c);
@@ -1260,8 +1333,7 @@ int mlem_create_symmetric(mlem_ctx** out, const uint64_t* row_end, const void* e
         cudaError_t e = cudaMemsetAsync(sptr, 0, 8, c->stream);
         if (e == cudaSuccess && n_rows)
             e = cudaMemcpyAsync(sptr + 1, row_end, (size_t)n_rows * 8, cudaMemcpyHostToDevice, c->stream);
-        if (e == cudaSuccess && nnz)
-            e = cudaMemcpyAsync(sel, elems, nnz * 8, cudaMemcpyHostToDevice, c->stream);
+        if (e == cudaSuccess && nnz) e = upload_pageable(c->device, c->stream, sel, elems, nnz * 8);
         if (e == cudaSuccess)
             e = cudaMemcpyAsync(dlut, lut.data(), lut.size() * 4, cudaMemcpyHostToDevice, c->stream);
         const SparseView stored{sptr, reinterpret_cast<const uint4*>(sel), n_rows, nnz};

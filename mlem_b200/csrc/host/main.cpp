@@ -24,7 +24,9 @@
 // MLEM_B200_EXPAND_SYMMETRY=1 (reconstruct with the full matrix of a
 // symmetry-compressed file; by default its symmetry flags are ignored, as the
 // reference's drivers ignore them; =kernels: the same reconstruction with only
-// the stored elements on the GPU and the mirrors applied in the kernels).
+// the stored elements on the GPU and the mirrors applied in the kernels),
+// MLEM_B200_TIMING=1 (the elapsed time after each phase -- matrix, sinograms,
+// tuning, iterations, output -- as "phase,<name>,<seconds>" lines on stderr).
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -118,8 +120,14 @@ int run(int argc, char** argv) {
     const int device = env_int("MLEM_B200_DEVICE", 0);
 
     auto t0 = std::chrono::steady_clock::now();
+    // MLEM_B200_TIMING=1: "phase,<name>,<seconds since the matrix load began>" on stderr
+    const bool timing = env_int("MLEM_B200_TIMING", 0) != 0;
+    auto phase = [&](const char* name) {
+        if (timing) std::cerr << "phase," << name << "," << seconds_since(t0) << std::endl;
+    };
     mlem_ctx* ctx = nullptr;
     check(mlem_create_from_file(&ctx, o.matrix.c_str(), flags, device), nullptr);
+    phase("matrix");
     struct Guard { mlem_ctx* c; ~Guard() { mlem_destroy(c); } } guard{ctx};
     mlem_info info;
     check(mlem_get_info(ctx, &info), ctx);
@@ -140,6 +148,7 @@ int run(int argc, char** argv) {
         check(mlem_vector_read(o.inputs[b].c_str(), 4, sino.data() + (size_t)b * R, R, &n), nullptr);
     }
     check(mlem_set_sinograms(ctx, sino.data(), B), ctx);
+    phase("sinograms");
 
     int first = 0;
     std::vector<float> image((size_t)C * B);
@@ -195,6 +204,7 @@ int run(int argc, char** argv) {
                       << t.frame_tile << ", row visit " << t.visit << ", " << t.ms_per_iter
                       << " ms/iteration\n";
     }
+    phase("tuning");
     if (!csv) std::cout << "Starting " << (o.iterations - first) << " MLEM iterations" << std::endl;
 
     const int chk = o.has_checkpointing ? o.checkpointing : 0;
@@ -235,9 +245,11 @@ int run(int argc, char** argv) {
             if (!csv) std::cout << "creating checkpoint " << std::endl;
         }
     }
+    phase("iterations");
     check(mlem_get_images(ctx, image.data()), ctx);
     for (uint32_t b = 0; b < B; ++b)
         check(mlem_vector_write(o.outputs[b].c_str(), image.data() + (size_t)b * C, 4, C, 0), nullptr);
+    phase("output");
     if (chk > 0) mlem_checkpoint_remove(".");
     return 0;
 }

@@ -397,6 +397,32 @@ def test_stream_host_against_oracle(golden, flags, frames):
             ctx.stream_host(sinos[:2], [got[0]])  # one buffer per iteration
 
 
+@pytest.mark.parametrize("via_file", [False, True])
+def test_large_element_upload_round_trip(tmp_path, via_file):
+    """Element arrays of 128 MiB and more go up through host threads and a
+    ring of page-locked buffers, 16 MiB per copy: the device matrix equals the
+    host arrays byte for byte (a size that is not a whole number of chunks),
+    from host arrays and from a mapped CSR4 file."""
+    rng = np.random.default_rng(3)
+    R, C = 200_003, 4096
+    row_end = np.cumsum(rng.integers(80, 120, R)).astype(np.uint64)
+    nnz = int(row_end[-1])
+    el = np.zeros(nnz, formats.ELEM_DTYPE)
+    el["index"] = rng.integers(0, C, nnz, dtype=np.uint32)
+    el["value"] = rng.random(nnz, dtype=np.float32) + 0.25
+    assert nnz * 8 > 128 << 20 and (nnz * 8) % (16 << 20)
+    if via_file:
+        path = tmp_path / "large.csr4"
+        formats.write_csr4(str(path), R, C, row_end, el)
+        ctx = api.Context.from_file(str(path), flags=api.FLAG_NO_CSC)
+    else:
+        ctx = api.Context.from_matrix(formats.Csr4(R, C, row_end, el), flags=api.FLAG_NO_CSC)
+    with ctx:
+        got_end, got_el = ctx.csr()
+        assert np.array_equal(got_end, row_end)
+        assert got_el.tobytes() == el.tobytes()
+
+
 def test_device_generator_matches_host_generator():
     g = synth.Geometry(32, 32, 16, 20000, 20, 80, seed=9)
     hm = synth.host_matrix(g)
