@@ -303,17 +303,23 @@ def run_cli(d, matrix, sino, iters, chk):
     """The command-line drop-in, as the reference's drivers are called:
     matrix input output iterations checkpointing (default method: the
     deterministic CSC back projection).  Returns the image and whether the
-    checkpoint pair was removed after the run, as mpicsr4mlem does."""
+    checkpoint pair was removed after the run, as mpicsr4mlem does, its wall
+    time and its phases (MLEM_B200_TIMING: seconds since the matrix load
+    began, at the end of each phase)."""
     import numpy as np
     out = os.path.join(d, "cli.img")
     t0 = time.time()
     p = subprocess.run([CLI, matrix, sino, out, str(iters), str(chk)], cwd=d,
-                       capture_output=True, text=True, timeout=900)
+                       capture_output=True, text=True, timeout=900,
+                       env=dict(os.environ, MLEM_B200_TIMING="1"))
     if p.returncode != 0:
         raise RuntimeError(f"mlem_b200 CLI failed: {p.stderr[-300:]}")
+    wall = time.time() - t0
     clean = not (os.path.exists(os.path.join(d, "img.chkpt"))
                  or os.path.exists(os.path.join(d, "iter.chkpt")))
-    return np.fromfile(out, np.float32), clean, time.time() - t0
+    phases = {m.group(1): round(float(m.group(2)), 3)
+              for m in re.finditer(r"^phase,(\w+),([0-9.eE+-]+)$", p.stderr, re.M)}
+    return np.fromfile(out, np.float32), clean, wall, phases
 
 
 # ---------------------------------------------------------------------------
@@ -701,7 +707,8 @@ def parity_gpu_side(ctx, a, tuning, sinograms, fb, tb, kf, d, mpath, spath):
     out["fast"] = ctx.get_images()[0]
     out["fast_method"] = f"{api.BK_NAMES[tuning['bk_mode']]}/{api.VISIT_NAMES[tuning['visit']]}"
     try:
-        out["cli"], out["cli_clean"], out["cli_wall"] = run_cli(d, mpath, spath, n, 10)
+        out["cli"], out["cli_clean"], out["cli_wall"], out["cli_phases"] = run_cli(d, mpath, spath,
+                                                                                 n, 10)
     except Exception as e:  # reported, not fatal
         out["cli_error"] = str(e)[:200]
     if fb is not None:
@@ -746,7 +753,10 @@ def parity_finish(jobs, pf, n):
     if "cli" in pf:
         p.update({"cli_chk10_vs_seq": sig(rel_l2(pf["cli"], seq)),
                   "cli_chk10_vs_f64": sig(rel_l2(pf["cli"], f64)),
-                  "cli_checkpoints_removed": pf["cli_clean"]})
+                  "cli_checkpoints_removed": pf["cli_clean"],
+                  # the command-line run end to end (process start to exit) and its phases;
+                  # the host cores run the reference's parity jobs meanwhile
+                  "cli_wall_s": round(pf["cli_wall"], 2), "cli_phases_s": pf["cli_phases"]})
     else:
         p["cli_error"] = pf.get("cli_error")
     res["plain"] = p
