@@ -28,10 +28,10 @@ using namespace mlem;
 
 namespace {
 
-__device__ __align__(256) float g_update_scratch[MLEM_NOALLOC_MAX_VOXELS];
+static __device__ __align__(256) float g_update_scratch[MLEM_NOALLOC_MAX_VOXELS];
 // bit 0: a column index >= n_cols; bit 1: a row whose offsets decrease or
 // pass the element count
-__device__ unsigned int g_bad_input;
+static __device__ unsigned int g_bad_input;
 
 constexpr unsigned int kBadColumn = 1u, kBadOffsets = 2u;
 
