@@ -33,6 +33,8 @@ METHODS = {
                      visit=api.VISIT_FILE),
     "csc/sorted": dict(bk_mode=api.BK_CSC, group=32, frame_tile=1, blocks_per_sm=8,
                        visit=api.VISIT_SORTED),
+    "region": dict(bk_mode=api.BK_REGION, group=32, frame_tile=1, blocks_per_sm=8,
+                   visit=api.VISIT_FILE),
 }
 
 
@@ -68,6 +70,20 @@ def test_full_size_methods_keep_the_counts_and_agree(full):
     ref = images["csc/file"]
     for name, img in images.items():
         assert ob.rel_l2(img, ref) <= TOL_MLEM, name
+
+
+def test_full_size_projections_are_adjoint(full):
+    """<A x, y> = <x, A^T y> for the device projections at full size (float32 kernels,
+    the inner products in float64), and A^T 1 equals the column sums."""
+    ctx, _, norm = full
+    rng = np.random.default_rng(5)
+    x = rng.random(ctx.n_cols, dtype=np.float32)
+    y = rng.random(ctx.n_rows, dtype=np.float32)
+    lhs = ctx.fwproj(x).astype(np.float64) @ y.astype(np.float64)
+    rhs = x.astype(np.float64) @ ctx.bkproj(y).astype(np.float64)
+    assert abs(lhs - rhs) <= 1e-6 * abs(rhs)
+    ones = ctx.bkproj(np.ones(ctx.n_rows, np.float32))
+    assert ob.rel_l2(ones, norm) <= 1e-6
 
 
 def test_full_size_deterministic_method_repeats_to_the_bit(full):
@@ -107,8 +123,8 @@ def test_full_size_batch_of_16_keeps_every_frames_counts(full):
 
 
 def test_full_size_streamed_steps_keep_each_steps_counts(full):
-    """mlem_stream_host at full size, a different sinogram each step (odd step count, so
-    the second buffer set ends the call): each step's image keeps that step's counts."""
+    """mlem_stream_host at full size, a different sinogram each step (four steps, so the
+    last one runs on the second buffer set): each step's image keeps that step's counts."""
     ctx, sino, norm = full
     rng = np.random.default_rng(11)
     steps = [sino[0]] + [rng.poisson(sino[0]).astype(np.int32) for _ in range(3)]
